@@ -1,0 +1,244 @@
+"""Python binding of the C ABI in include/asz_b200.h (ctypes over the in-tree libasz_b200.so).
+
+The functions mirror the reference's compressor/decompressor surface: ``compress`` takes a float32
+field, an error bound, a predictor plan and the s1_compress tunables, and returns .asz bytes;
+``decompress`` inverts it. Inputs may be NumPy arrays (host) or CUDA tensors (device pointers,
+run on the caller's current stream). There is no CPU fallback: if the CUDA library is missing or
+no GPU is present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libasz_b200.so")
+_LIB = None
+
+ASZ_FAMILY_AUTO, ASZ_FAMILY_CUBIC, ASZ_FAMILY_QUINTIC = -1, 0, 1
+
+
+class AszError(RuntimeError):
+    """A call returned a nonzero status; the message is asz_last_error()."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("pivot_eb_ratio", C.c_float), ("eb_ratio", C.c_float), ("slope_ratio", C.c_float),
+        ("block_pivot_ratio", C.c_uint64), ("max_layer_num", C.c_uint64),
+        ("full_predictor_search_layer_num", C.c_uint64), ("generate_config_sample_stride", C.c_uint64),
+        ("h1_block_sampling_num", C.c_uint64), ("stat_eb_ratio", C.c_float),
+        ("predictor_family_suffix_layers", C.c_uint64), ("predictor_family_sample_blocks", C.c_uint64),
+        ("predictor_family_sample_point_limit", C.c_uint64), ("predictor_family_sample_fraction_limit", C.c_float),
+        ("predictor_family_coarse_probe_block_pivot_ratio", C.c_uint64),
+        ("predictor_family_fine_probe_block_pivot_ratio", C.c_uint64),
+        ("predictor_family_fine_eb_threshold", C.c_float), ("default_slope_invalid_ratio_threshold", C.c_float),
+        ("default_slope_fallback", C.c_float), ("default_slope_eb_span", C.c_float),
+        ("t_precision", C.c_int32), ("t_min", C.c_float), ("t_max", C.c_float), ("t_range_set", C.c_int32),
+        ("predictor_family", C.c_int32), ("report_t_histogram", C.c_int32),
+    ]
+
+
+class Report(C.Structure):
+    _fields_ = [
+        ("data_range_s", C.c_double), ("default_slope_s", C.c_double), ("plan_s", C.c_double),
+        ("family_s", C.c_double), ("core_s", C.c_double), ("huffman_s", C.c_double), ("zstd_s", C.c_double),
+        ("h2d_s", C.c_double), ("d2h_s", C.c_double), ("total_s", C.c_double),
+        ("min_val", C.c_float), ("max_val", C.c_float), ("abs_eb", C.c_float), ("default_slope", C.c_float),
+        ("max_err", C.c_float), ("psnr", C.c_float), ("cr", C.c_float), ("br", C.c_float),
+        ("t_fallback_count", C.c_uint64), ("pre_zstd_len", C.c_uint64), ("asz_len", C.c_uint64),
+        ("layer_num", C.c_uint64), ("slope_max_invalid_ratio", C.c_float), ("slope_fallback_reason", C.c_int32),
+        ("ambiguous_decisions", C.c_uint64), ("reruns", C.c_uint64),
+        ("pivot_stride", C.c_uint32 * 3), ("block_shape", C.c_uint32 * 3), ("block_num", C.c_uint32 * 3),
+        ("quintic", C.c_int32), ("plan", C.c_char * (64 * 11 + 1)),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            if isinstance(v, bytes):
+                v = v.decode()
+            elif hasattr(v, "__len__"):
+                v = list(v)
+            out[name] = v
+        return out
+
+
+def lib():
+    """Load libasz_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is not built: run asz_b200.build.build() (make -C asz_b200/csrc)")
+    L = C.CDLL(LIB_PATH)
+    L.asz_default_params.argtypes = [C.POINTER(Params)]
+    L.asz_create.argtypes = [C.c_int]
+    L.asz_create.restype = C.c_void_p
+    L.asz_destroy.argtypes = [C.c_void_p]
+    L.asz_last_error.argtypes = [C.c_void_p]
+    L.asz_last_error.restype = C.c_char_p
+    L.asz_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.asz_compress.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_float, C.POINTER(Params),
+                               C.c_char_p, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t), C.POINTER(Report)]
+    L.asz_decompress.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.c_float,
+                                 C.POINTER(Params), C.c_void_p, C.c_int, C.POINTER(Report)]
+    L.asz_free.argtypes = [C.c_void_p]
+    L.asz_compress_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    for name, elem in (("asz_debug_qb", None), ("asz_debug_t", None), ("asz_debug_recon", None),
+                       ("asz_debug_pre_zstd", None)):
+        f = getattr(L, name)
+        f.restype = C.c_uint64
+    L.asz_debug_qb.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+    L.asz_debug_t.argtypes = [C.c_void_p, C.c_void_p]
+    L.asz_debug_recon.argtypes = [C.c_void_p, C.c_void_p]
+    L.asz_debug_pre_zstd.argtypes = [C.c_void_p, C.c_void_p]
+    _LIB = L
+    return L
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().asz_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _family_code(family):
+    if family is None or family == "auto":
+        return ASZ_FAMILY_AUTO
+    return {"cubic": ASZ_FAMILY_CUBIC, "quintic": ASZ_FAMILY_QUINTIC}[family]
+
+
+def _dims(shape):
+    if len(shape) != 3:
+        raise ValueError("fields are three-dimensional")
+    return (C.c_uint64 * 3)(*[int(s) for s in shape])
+
+
+def _is_cuda_tensor(x):
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+class Context:
+    """One CUDA context: a stream and the device buffers reused across calls."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        self._c = self._L.asz_create(int(device))
+        if not self._c:
+            raise RuntimeError(f"asz_create({device}) failed: no usable CUDA device")
+        self.device = device
+
+    def close(self):
+        if self._c:
+            self._L.asz_destroy(self._c)
+            self._c = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise AszError(rc, self._L.asz_last_error(self._c).decode())
+
+    def _use_torch_stream(self, x):
+        import torch
+        self._L.asz_set_stream(self._c, C.c_void_p(torch.cuda.current_stream(x.device).cuda_stream))
+
+    def compress(self, data, rel_eb: float, plan: str | None, family="cubic", params: Params | None = None):
+        """Compress a float32 field; returns (asz bytes, Report)."""
+        p = params if params is not None else default_params()
+        p.predictor_family = _family_code(family) if family is not None else p.predictor_family
+        out = C.POINTER(C.c_uint8)()
+        n = C.c_size_t(0)
+        rep = Report()
+        if _is_cuda_tensor(data):
+            import torch
+            if data.dtype != torch.float32 or not data.is_contiguous():
+                raise ValueError("device input must be a contiguous float32 tensor")
+            self._use_torch_stream(data)
+            rc = self._L.asz_compress(self._c, C.c_void_p(data.data_ptr()), 1, _dims(data.shape), C.c_float(rel_eb),
+                                      C.byref(p), plan.encode() if plan else None, C.byref(out), C.byref(n), C.byref(rep))
+            self._L.asz_set_stream(self._c, None)
+        else:
+            a = np.ascontiguousarray(data, dtype=np.float32)
+            rc = self._L.asz_compress(self._c, C.c_void_p(a.ctypes.data), 0, _dims(a.shape), C.c_float(rel_eb),
+                                      C.byref(p), plan.encode() if plan else None, C.byref(out), C.byref(n), C.byref(rep))
+        self._check(rc)
+        try:
+            blob = C.string_at(out, n.value)
+        finally:
+            self._L.asz_free(out)
+        return blob, rep
+
+    def decompress(self, blob: bytes, shape, rel_eb: float, params: Params | None = None, out=None):
+        """Decompress .asz bytes; returns a NumPy array, or fills the CUDA tensor `out`."""
+        p = params if params is not None else default_params()
+        rep = Report()
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        if out is not None and _is_cuda_tensor(out):
+            self._use_torch_stream(out)
+            rc = self._L.asz_decompress(self._c, buf, len(blob), _dims(shape), C.c_float(rel_eb), C.byref(p),
+                                        C.c_void_p(out.data_ptr()), 1, C.byref(rep))
+            self._L.asz_set_stream(self._c, None)
+            self._check(rc)
+            return out, rep
+        res = np.empty(tuple(int(s) for s in shape), dtype=np.float32)
+        rc = self._L.asz_decompress(self._c, buf, len(blob), _dims(shape), C.c_float(rel_eb), C.byref(p),
+                                    C.c_void_p(res.ctypes.data), 0, C.byref(rep))
+        self._check(rc)
+        return res, rep
+
+    def stats(self):
+        m, ps = C.c_double(), C.c_double()
+        self._check(self._L.asz_compress_stats(self._c, C.byref(m), C.byref(ps)))
+        return m.value, ps.value
+
+    # Internals of the last compress call (parity checks).
+    def debug_qb(self, stream: int) -> np.ndarray:
+        n = self._L.asz_debug_qb(self._c, stream, None)
+        a = np.empty(n, np.int32)
+        if n:
+            self._L.asz_debug_qb(self._c, stream, C.c_void_p(a.ctypes.data))
+        return a
+
+    def debug_t(self) -> np.ndarray:
+        n = self._L.asz_debug_t(self._c, None)
+        a = np.empty(n, np.int64)
+        if n:
+            self._L.asz_debug_t(self._c, C.c_void_p(a.ctypes.data))
+        return a
+
+    def debug_recon(self) -> np.ndarray:
+        n = self._L.asz_debug_recon(self._c, None)
+        a = np.empty(n, np.float32)
+        if n:
+            self._L.asz_debug_recon(self._c, C.c_void_p(a.ctypes.data))
+        return a
+
+    def debug_pre_zstd(self) -> bytes:
+        n = self._L.asz_debug_pre_zstd(self._c, None)
+        a = (C.c_uint8 * max(n, 1))()
+        if n:
+            self._L.asz_debug_pre_zstd(self._c, a)
+        return bytes(a)[:n]

@@ -1,0 +1,66 @@
+// Shared device helpers: the reference's floating-point steps spelled with rounding-explicit
+// intrinsics, plus the plan geometry every kernel uses.
+//
+// Every operation that the reference performs is written with a _rn intrinsic or an explicit
+// fused multiply-add, and the library is compiled with -fmad=false, so nvcc neither contracts
+// nor reassociates. The forms follow the code GCC 13.3 emits for the reference at
+// -Ofast -mfma (c_codes/CMakeLists.txt:12); each use site cites the source line it restates.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define ASZ_HD __host__ __device__ __forceinline__
+#else
+#define ASZ_HD inline
+#endif
+
+namespace asz {
+
+#ifdef __CUDACC__
+// llround(float) as expanded under -Ofast: truncate x + copysign(0.49999997f, x).
+__device__ __forceinline__ int64_t lround_f(float x) {
+    float h = copysignf(0x1.fffffep-2f, x);
+    return __float2ll_rz(__fadd_rn(x, h));
+}
+// llround(double): truncate x + copysign(0.49999999999999994, x).
+__device__ __forceinline__ int64_t lround_d(double x) {
+    double h = copysign(0x1.fffffffffffffp-2, x);
+    return __double2ll_rz(__dadd_rn(x, h));
+}
+#endif
+
+// Quintic 1D6R weights (c_codes/asz_core/asz_param.hpp:72-74): a=3/256, b=-25/256, inner=0.5-a-b.
+constexpr double kQuinticA = 3.0 / 256, kQuinticB = -25.0 / 256, kQuinticI = 0.5 - 3.0 / 256 + 25.0 / 256;
+
+// One prediction round of the plan, in global (not per-block) terms. Host-filled.
+struct RoundGeom {
+    int32_t dir;             // interpolation axis of the round
+    int32_t order;           // QB serialisation order: 0 "120", 1 "021", 2 "012"
+    uint64_t stride[3];      // lattice strides at the start of the round
+    uint64_t hs;             // stride[dir]/2
+    uint64_t dist;           // linear distance of one half stride along dir
+    uint64_t tcount[3];      // targets per axis (global lattice)
+    uint64_t targets;        // product of tcount
+    float eb;                // layer error bound (compress.tpp:194)
+    float slope;             // layer default slope (compress.tpp:195)
+    float stat_eb;           // eb * stat_eb_ratio (compress.tpp:118)
+    float neg_2_stat_eb;     // 0.5f / stat_eb (compress.tpp:120 as emitted)
+    uint32_t axis_off[3];    // offset of this round's per-block count/prefix arrays, per axis
+    uint64_t total[3];       // sum of per-block counts along each axis
+    uint64_t qb_total;       // QBs of this round (stream length)
+    uint32_t fallback_all;   // 1 when every block falls back to the default t
+};
+
+struct FieldGeom {
+    uint64_t n[3];
+    uint64_t block_shape[3];
+    uint64_t block_num[3];
+    uint64_t pivot_stride[3];
+    uint32_t layer_num;
+    int32_t quintic;
+    int32_t t_precision;
+};
+
+ASZ_HD uint64_t owner_block(uint64_t i, uint64_t shape) { return i == 0 ? 0 : (i - 1) / shape; }
+
+}  // namespace asz

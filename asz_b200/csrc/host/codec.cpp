@@ -1,0 +1,1244 @@
+// Host orchestration of the B200 compression path and the C ABI in include/asz_b200.h.
+//
+// Compress (c_codes/asz_core/compress.tpp:147-321 behind s1_compress.cpp:153-341):
+//   data range on the GPU -> default slope (GPU proxies, glibc log10f on the host) -> pivots ->
+//   per round: t selection and prediction kernels -> replay of ambiguous t decisions on the
+//   host -> histograms -> Huffman codes built on the host -> GPU encoding -> stream assembly
+//   -> libzstd level 3.
+// Decompress (c_codes/asz_core/decompress.tpp:79-208): libzstd -> header and tree parsing ->
+//   GPU Huffman decoding -> pivots -> per-round reconstruction kernels.
+//
+// Host floating point in this file restates the reference's scalar steps and is built with
+// -ffp-contract=off; glibc's log10f, log2f, cbrt and pow are called where the reference calls
+// them, so the host values are the reference's on the same machine.
+#include <cuda_runtime.h>
+#include <immintrin.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../launch.h"
+#include "../../../include/asz_b200.h"
+#include "huffman_host.h"
+#include "zstd_api.h"
+
+using namespace asz;
+
+namespace {
+
+using u64 = uint64_t;
+using clk = std::chrono::steady_clock;
+
+double secs(clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); }
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    template <class T>
+    T *as() const {
+        return (T *)p;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// llround of a float as the reference's -Ofast build computes it (see dev_common.cuh).
+int64_t host_lround_f(float x) {
+    volatile float h = std::copysign(0x1.fffffep-2f, x);
+    volatile float s = x + h;
+    return (int64_t)s;
+}
+
+struct Plan {
+    std::vector<std::string> pred;  // "cubicD_OOO"
+    std::vector<int> dir, order;
+};
+
+bool parse_plan(const char *text, Plan &plan, std::string &err) {
+    // parse_predictor_plan (s1_compress.cpp:5-28).
+    std::string t(text);
+    size_t b = 0;
+    while (b <= t.size()) {
+        size_t e = t.find(',', b);
+        std::string p = t.substr(b, e == std::string::npos ? std::string::npos : e - b);
+        bool ok = false;
+        for (int d = 0; d < 3; d++)
+            for (const char *o : {"120", "021", "012"})
+                if (p == std::string("cubic") + char('0' + d) + "_" + o) ok = true;
+        if (!ok) {
+            err = "invalid predictor in plan: " + p;
+            return false;
+        }
+        plan.pred.push_back(p);
+        plan.dir.push_back(p[5] - '0');
+        plan.order.push_back(p[9] - '0');
+        if (e == std::string::npos) break;
+        b = e + 1;
+    }
+    if (plan.pred.empty()) {
+        err = "predictor plan cannot be empty";
+        return false;
+    }
+    return true;
+}
+
+struct Geometry {
+    FieldGeom fg{};
+    std::vector<RoundGeom> rounds;
+    std::vector<u64> tab_count, tab_prefix;     // per round, per axis, per block
+    std::vector<std::vector<ClassInfo>> classes;
+    std::vector<uint32_t> cap;                  // max samples per round
+    PivotGeom pg{};
+    u64 pivots = 0, nblocks = 0;
+};
+
+}  // namespace
+
+struct asz_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string err;
+    // Device buffers.
+    DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
+        classes, axis, pre, chunks, out;
+    // Cached glibc log2f tables, keyed by sample count.
+    std::map<uint32_t, uint32_t> log2_off;
+    std::vector<float> log2_host;
+    u64 log2_dev_len = 0;
+    // Last compress call, for the debug accessors.
+    std::vector<u64> qb_off, qb_len;
+    u64 t_len = 0, n_total = 0;
+    const float *last_in = nullptr;   // device input of the last compress call
+    float last_min = 0, last_max = 0;
+    std::vector<uint8_t> pre_zstd;
+    bool have_last = false;
+};
+
+namespace {
+
+int fail(asz_ctx *c, int code, const std::string &m) {
+    c->err = m;
+    return code;
+}
+
+#define CK(call)                                                                    \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) return fail(ctx, ASZ_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int validate(asz_ctx *ctx, const asz_params &p, bool compress_side) {
+    // validate_parameters (s1_compress.cpp:49-99) and s1_decompress.cpp:112-125.
+    auto bad = [&](const char *m) { return fail(ctx, ASZ_E_ARG, m); };
+    if (!(p.pivot_eb_ratio > 0 && p.pivot_eb_ratio <= 1)) return bad("pivot_eb_ratio must be in (0,1]");
+    if (!(p.eb_ratio > 0 && p.eb_ratio <= 1)) return bad("eb_ratio must be in (0,1]");
+    if (!(p.slope_ratio > 0 && p.slope_ratio <= 1)) return bad("slope_ratio must be in (0,1]");
+    if (p.block_pivot_ratio == 0) return bad("block_pivot_ratio must be positive");
+    if (p.max_layer_num == 0 || p.max_layer_num > 63) return bad("max_layer_num must be in [1,63]");
+    if (p.full_predictor_search_layer_num == 0 || p.full_predictor_search_layer_num > 63)
+        return bad("full_predictor_search_layer_num must be in [1,63]");
+    if (p.t_precision < 16 || p.t_precision % 16 != 0) return bad("t_precision must be a positive multiple of 16");
+    if (!compress_side) return ASZ_OK;
+    if (p.generate_config_sample_stride == 0) return bad("generate_config_sample_stride must be positive");
+    if (p.h1_block_sampling_num == 0) return bad("h1_block_sampling_num must be positive");
+    if (!(p.stat_eb_ratio > 0 && p.stat_eb_ratio <= 1)) return bad("stat_eb_ratio must be in (0,1]");
+    if (p.predictor_family_suffix_layers == 0) return bad("predictor_family_suffix_layers must be positive");
+    if (p.predictor_family_sample_blocks == 0) return bad("predictor_family_sample_blocks must be positive");
+    if (p.predictor_family_sample_point_limit == 0) return bad("predictor_family_sample_point_limit must be positive");
+    if (!(p.predictor_family_sample_fraction_limit > 0 && p.predictor_family_sample_fraction_limit <= 1))
+        return bad("predictor_family_sample_fraction_limit must be in (0,1]");
+    if (p.predictor_family_coarse_probe_block_pivot_ratio == 0 || p.predictor_family_fine_probe_block_pivot_ratio == 0)
+        return bad("predictor family probe block pivot ratios must be positive");
+    if (!(p.predictor_family_fine_eb_threshold > 0 && std::isfinite(p.predictor_family_fine_eb_threshold)))
+        return bad("predictor_family_fine_eb_threshold must be positive and finite");
+    if (!(p.default_slope_invalid_ratio_threshold > 0 && p.default_slope_invalid_ratio_threshold <= 1))
+        return bad("default_slope_invalid_ratio_threshold must be in (0,1]");
+    if (!(p.default_slope_fallback > 0 && std::isfinite(p.default_slope_fallback)))
+        return bad("default_slope_fallback must be positive and finite");
+    if (!(p.default_slope_eb_span > 1 && std::isfinite(p.default_slope_eb_span)))
+        return bad("default_slope_eb_span must be greater than 1 and finite");
+    float tmin = p.t_min, tmax = p.t_max;
+    if (!(tmin >= 0 && tmin <= tmax && tmax <= 0.5)) return bad("t range must satisfy 0 <= t_min <= t_max <= 0.5");
+    float a = tmin * (float)p.t_precision, b = tmax * (float)p.t_precision;
+    if (std::fabs(a - std::round(a)) > 1e-6 || std::fabs(b - std::round(b)) > 1e-6)
+        return bad("t_min and t_max must be representable at t_precision");
+    if (tmin > 4.0f / 16 || tmax < 5.0f / 16) return bad("t range must include 4/16 and 5/16");
+    // set_t_candidates (asz_param.hpp:194-204).
+    if (p.t_precision % 32 || tmin > 1.0f / 16 || tmax < 11.0f / 32)
+        return bad("block t candidates require t_precision divisible by 32 and t range covering [1/16,11/32]");
+    return ASZ_OK;
+}
+
+int validate_dims(asz_ctx *ctx, const uint64_t dims[3], float rel_eb) {
+    if (!dims || dims[0] < 7 || dims[1] < 7 || dims[2] < 7) return fail(ctx, ASZ_E_ARG, "all three dimensions must be at least 7");
+    if (!(rel_eb > 0 && std::isfinite(rel_eb))) return fail(ctx, ASZ_E_ARG, "relative error bound must be positive and finite");
+    u64 n = 1;
+    for (int a = 0; a < 3; a++) {
+        if (n > std::numeric_limits<u64>::max() / dims[a]) return fail(ctx, ASZ_E_ARG, "data dimensions overflow the element count");
+        n *= dims[a];
+    }
+    if (n > std::numeric_limits<size_t>::max() / sizeof(float))
+        return fail(ctx, ASZ_E_ARG, "data dimensions exceed the addressable input size");
+    return ASZ_OK;
+}
+
+// Plan geometry (generate_config.tpp:52-68) and per-round tables.
+void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &p, float abs_eb, float default_slope,
+                    bool quintic, Geometry &G) {
+    FieldGeom &fg = G.fg;
+    const u64 L = plan.pred.size();
+    for (int a = 0; a < 3; a++) {
+        fg.n[a] = dims[a];
+        fg.pivot_stride[a] = 1;
+    }
+    for (u64 l = 0; l < L; l++) fg.pivot_stride[plan.dir[l]] *= 2;
+    for (int a = 0; a < 3; a++) {
+        fg.block_shape[a] = fg.pivot_stride[a] * p.block_pivot_ratio;
+        fg.block_num[a] = (fg.n[a] + fg.block_shape[a] - 1) / fg.block_shape[a];
+    }
+    fg.layer_num = (uint32_t)L;
+    fg.quintic = quintic ? 1 : 0;
+    fg.t_precision = p.t_precision;
+    G.nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
+    // Pivots (compress.tpp:162-175).
+    G.pivots = 1;
+    for (int a = 0; a < 3; a++) {
+        G.pg.cnt[a] = (fg.n[a] + fg.pivot_stride[a] - 1) / fg.pivot_stride[a];
+        G.pg.stride[a] = fg.pivot_stride[a];
+        G.pivots *= G.pg.cnt[a];
+    }
+    G.pg.n1n2 = fg.n[1] * fg.n[2];
+    G.pg.n2 = fg.n[2];
+    float pivot_eb = abs_eb * p.pivot_eb_ratio;
+    G.pg.rp = 0.5 / (double)pivot_eb;
+    G.pg.peb2 = (double)pivot_eb + (double)pivot_eb;
+
+    u64 stride[3] = {fg.pivot_stride[0], fg.pivot_stride[1], fg.pivot_stride[2]};
+    G.rounds.assign(L, RoundGeom{});
+    G.classes.assign(L, std::vector<ClassInfo>(27));
+    G.cap.assign(L, 0);
+    G.tab_count.clear();
+    G.tab_prefix.clear();
+    for (u64 l = 0; l < L; l++) {
+        RoundGeom &rg = G.rounds[l];
+        const int d = plan.dir[l];
+        rg.dir = d;
+        rg.order = plan.order[l];
+        for (int a = 0; a < 3; a++) rg.stride[a] = stride[a];
+        rg.hs = stride[d] / 2;
+        rg.dist = rg.hs;
+        for (int a = d + 1; a < 3; a++) rg.dist *= fg.n[a];
+        rg.targets = 1;
+        for (int a = 0; a < 3; a++) {
+            if (a == d) rg.tcount[a] = fg.n[a] > rg.hs ? (fg.n[a] - rg.hs + 2 * rg.hs - 1) / (2 * rg.hs) : 0;
+            else rg.tcount[a] = (fg.n[a] + stride[a] - 1) / stride[a];
+            rg.targets *= rg.tcount[a];
+        }
+        // compress.tpp:194-195, decompress.tpp:156.
+        rg.eb = (float)((double)abs_eb * std::pow((double)p.eb_ratio, (double)(L - l - 1)));
+        rg.slope = (float)((double)default_slope * std::pow((double)p.slope_ratio, (double)((int)L - (int)l - 1)));
+        rg.stat_eb = rg.eb * p.stat_eb_ratio;
+        rg.neg_2_stat_eb = 0.5f / rg.stat_eb;
+        // Per-axis box sizes (get_layer_qb_shape, asz_param.hpp:105-114).
+        rg.qb_total = 1;
+        for (int a = 0; a < 3; a++) {
+            rg.axis_off[a] = (uint32_t)G.tab_count.size();
+            u64 sum = 0;
+            for (u64 b = 0; b < fg.block_num[a]; b++) {
+                u64 lo = b * fg.block_shape[a], hi = std::min((b + 1) * fg.block_shape[a] + 1, fg.n[a]);
+                u64 start = a == d ? lo + stride[a] / 2 : (lo == 0 ? 0 : lo + stride[a]);
+                u64 c = start >= hi ? 0 : (hi - start + stride[a] - 1) / stride[a];
+                G.tab_count.push_back(c);
+                G.tab_prefix.push_back(sum);
+                sum += c;
+            }
+            rg.total[a] = sum;
+            rg.qb_total *= sum;
+        }
+        // Block classes for coefficient selection (compress.tpp:96-116, get_AB_map.tpp:9-12).
+        bool all_fb = true;
+        for (int cls = 0; cls < 27; cls++) {
+            int cc[3] = {cls / 9, (cls / 3) % 3, cls % 3};
+            u64 rep[3];
+            bool exists = true;
+            for (int a = 0; a < 3; a++) {
+                u64 nb = fg.block_num[a];
+                if (cc[a] == 0) rep[a] = 0;
+                else if (cc[a] == 2) {
+                    if (nb < 2) exists = false;
+                    rep[a] = nb - 1;
+                } else {
+                    if (nb < 3) exists = false;
+                    rep[a] = 1;
+                }
+            }
+            ClassInfo ci{1, 0, 0, 1};
+            if (!exists) {
+                G.classes[l][cls] = ci;
+                continue;
+            }
+            u64 lo[3], hi[3];
+            for (int a = 0; a < 3; a++) {
+                lo[a] = rep[a] * fg.block_shape[a];
+                hi[a] = std::min((rep[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
+            }
+            if (hi[d] <= lo[d] + 3 * stride[d]) {
+                G.classes[l][cls] = ci;
+                continue;
+            }
+            for (int a = 0; a < 3; a++)
+                if (a != d && lo[a] != 0) lo[a] += stride[a];
+            lo[d] += 3 * stride[d] / 2;
+            hi[d] -= 3 * stride[d] / 2;
+            u64 vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+            float q = (float)vol / (float)(stride[0] * stride[1] * stride[2] * p.h1_block_sampling_num);
+            u64 ss = (u64)std::cbrt((double)q);
+            if (ss == 0) ss = 1;
+            u64 n = 1;
+            for (int a = 0; a < 3; a++) {
+                u64 step = stride[a] * ss;
+                n *= hi[a] > lo[a] ? (hi[a] - lo[a] + step - 1) / step : 0;
+            }
+            ci.ss = (uint32_t)ss;
+            ci.n = (uint32_t)n;
+            ci.fallback = n == 0 ? 1 : 0;
+            if (n) all_fb = false;
+            G.cap[l] = std::max<uint32_t>(G.cap[l], (uint32_t)n);
+            G.classes[l][cls] = ci;
+        }
+        rg.fallback_all = all_fb ? 1 : 0;
+        stride[d] /= 2;
+    }
+}
+
+// glibc log2f(freq * (1/n)) for freq = 0..n (index 0 unused), cached per n.
+uint32_t log2_table(asz_ctx *ctx, uint32_t n) {
+    auto it = ctx->log2_off.find(n);
+    if (it != ctx->log2_off.end()) return it->second;
+    uint32_t off = (uint32_t)ctx->log2_host.size();
+    float nf = (float)(u64)n;
+    float r = 1.0f / nf;
+    ctx->log2_host.push_back(0.0f);
+    for (u64 f = 1; f <= n; f++) {
+        float pr = (float)f * r;
+        ctx->log2_host.push_back(log2f(pr));
+    }
+    ctx->log2_off[n] = off;
+    return off;
+}
+
+int upload_log2(asz_ctx *ctx) {
+    if (ctx->log2_dev_len == ctx->log2_host.size()) return ASZ_OK;
+    CK(ctx->log2arena.reserve(ctx->log2_host.size() * sizeof(float)));
+    if (ctx->log2arena.cap < ctx->log2_host.size() * sizeof(float)) return fail(ctx, ASZ_E_CUDA, "log2 arena");
+    CK(cudaMemcpyAsync(ctx->log2arena.p, ctx->log2_host.data(), ctx->log2_host.size() * sizeof(float),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    ctx->log2_dev_len = ctx->log2_host.size();
+    return ASZ_OK;
+}
+
+// Scratch sizes for one AB map of up to `cap` samples.
+void scratch_dims(uint32_t cap, uint32_t &bcap, uint32_t &tcap, u64 &stride) {
+    cap = std::max<uint32_t>(cap, 1);
+    bcap = (uint32_t)sched_buckets(cap);
+    tcap = 16;
+    while (tcap < 2 * cap) tcap <<= 1;
+    stride = tsel_scratch_bytes(cap, bcap, tcap);
+}
+
+// Replays one ambiguous decision with glibc log10f (compress.tpp:127-142).
+float replay_decision(const AmbiguousRecord &r, float slope) {
+    const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+    int best = 1;
+    float best_h1 = r.h1[1], best_psnr = 10.0f * log10f(r.x[1]);
+    for (int c = 0; c < 5; c++) {
+        if (cand[c] == cand[best]) continue;
+        float psnr = 10.0f * log10f(r.x[c]);
+        float s = std::fma(best_h1 - r.h1[c], slope, psnr - best_psnr);
+        if (s > 0) {
+            best = c;
+            best_h1 = r.h1[c];
+            best_psnr = psnr;
+        }
+    }
+    return cand[best];
+}
+
+}  // namespace
+
+extern "C" {
+
+void asz_default_params(asz_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->pivot_eb_ratio = 0.05f;
+    p->eb_ratio = 0.76f;
+    p->slope_ratio = 0.54f;
+    p->block_pivot_ratio = 4;
+    p->max_layer_num = 14;
+    p->full_predictor_search_layer_num = 4;
+    p->generate_config_sample_stride = 5;
+    p->h1_block_sampling_num = 256;
+    p->stat_eb_ratio = 0.2f;
+    p->predictor_family_suffix_layers = 6;
+    p->predictor_family_sample_blocks = 8;
+    p->predictor_family_sample_point_limit = 32768;
+    p->predictor_family_sample_fraction_limit = 0.02f;
+    p->predictor_family_coarse_probe_block_pivot_ratio = 3;
+    p->predictor_family_fine_probe_block_pivot_ratio = 4;
+    p->predictor_family_fine_eb_threshold = 1e-4f;
+    p->default_slope_invalid_ratio_threshold = 1;
+    p->default_slope_fallback = 1000;
+    p->default_slope_eb_span = 1.5f;
+    p->t_precision = 32;
+    p->t_min = 1.0f / 16;
+    p->t_max = 6.0f / 16;
+    p->predictor_family = ASZ_FAMILY_AUTO;
+}
+
+asz_ctx *asz_create(int device) {
+    if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+    asz_ctx *c = new asz_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    c->stream = c->own;
+    return c;
+}
+
+void asz_destroy(asz_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
+                      &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
+                      &c->out})
+        b->release();
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+}
+
+const char *asz_last_error(const asz_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+int asz_set_stream(asz_ctx *c, void *s) {
+    if (!c) return ASZ_E_ARG;
+    c->stream = s ? (cudaStream_t)s : c->own;
+    return ASZ_OK;
+}
+
+void asz_free(void *p) { std::free(p); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Compression.
+
+namespace {
+
+struct MiscLayout {  // small device words, one allocation
+    int32_t range[2];
+    unsigned long long nonfinite;
+    unsigned long long zfirst, zlast;
+    uint32_t err;
+    uint32_t fb;
+    uint32_t amb_count;
+    uint32_t changed;
+    int32_t qb_range[2 * 64];
+    float h1[3 * 64];
+    float x[3 * 64];
+    uint32_t m[3];
+    SampleBox boxes[3];
+    ProxyEval evals[64];
+};
+
+int compute_range(asz_ctx *ctx, const float *d_in, u64 N, float &mn, float &mx) {
+    MiscLayout init{};
+    init.range[0] = INT32_MAX;
+    init.range[1] = INT32_MIN;
+    init.zfirst = ~0ull;
+    init.zlast = 0;
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    CK(cudaMemcpyAsync(dm, &init, sizeof(MiscLayout), cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_range(d_in, N, dm->range, &dm->nonfinite, ctx->stream));
+    MiscLayout h;
+    CK(cudaMemcpyAsync(&h, dm, offsetof(MiscLayout, err), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h.nonfinite) return fail(ctx, ASZ_E_DATA, "input contains a nonfinite value");
+    auto tof = [](int32_t k) {
+        uint32_t b = k >= 0 ? (uint32_t)k : ((uint32_t)k ^ 0x7fffffffu);
+        float f;
+        std::memcpy(&f, &b, 4);
+        return f;
+    };
+    mn = tof(h.range[0]);
+    mx = tof(h.range[1]);
+    if (mn == 0.0f || mx == 0.0f) {
+        // minmax_element keeps the first smallest and the last largest element; with zeros of
+        // both signs present, that decides the stored sign.
+        CK(launch_zero_first_last(d_in, N, &dm->zfirst, &dm->zlast, ctx->stream));
+        unsigned long long fl[2];
+        CK(cudaMemcpyAsync(fl, &dm->zfirst, 16, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (mn == 0.0f) CK(cudaMemcpy(&mn, d_in + fl[0], 4, cudaMemcpyDeviceToHost));
+        if (mx == 0.0f) CK(cudaMemcpy(&mx, d_in + fl[1], 4, cudaMemcpyDeviceToHost));
+    }
+    return ASZ_OK;
+}
+
+// get_default_slope (c_codes/asz_core/get_default_slope.tpp:6-83).
+int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const asz_params &p, float abs_eb, float mn,
+                  float mx, const std::vector<float> &cand_t, float &slope_out, float &max_invalid_out, int &reason_out) {
+    FieldGeom fg{};
+    for (int a = 0; a < 3; a++) fg.n[a] = dims[a];
+    const float ebs[2] = {abs_eb * p.default_slope_eb_span, abs_eb / p.default_slope_eb_span};
+    const float two_stat = abs_eb * p.stat_eb_ratio;
+    const float stat_eb = two_stat * 0.5f;
+    const float neg = 1.0f / two_stat;
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    SampleBox boxes[3];
+    uint32_t cap = 1;
+    for (int d = 0; d < 3; d++) {
+        SampleBox &b = boxes[d];
+        u64 lo[3] = {0, 0, 0}, hi[3] = {dims[0], dims[1], dims[2]}, st[3] = {1, 1, 1};
+        lo[d] = 3;
+        hi[d] = dims[d] - 3;
+        st[d] = 2;
+        u64 vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+        float q = (float)vol / (float)(st[0] * st[1] * st[2] * p.h1_block_sampling_num);
+        u64 ss = (u64)std::cbrt((double)q);
+        if (ss == 0) ss = 1;
+        u64 n = 1;
+        for (int a = 0; a < 3; a++) {
+            b.lo[a] = lo[a];
+            b.hi[a] = hi[a];
+            b.step[a] = st[a] * ss;
+            n *= hi[a] > lo[a] ? (hi[a] - lo[a] + b.step[a] - 1) / b.step[a] : 0;
+        }
+        b.dist = 1;
+        for (int a = d + 1; a < 3; a++) b.dist *= dims[a];
+        b.neg_2_stat_eb = neg;
+        b.stat_eb = stat_eb;
+        b.n = (uint32_t)n;
+        b.log2_off = n ? log2_table(ctx, (uint32_t)n) : 0;
+        cap = std::max<uint32_t>(cap, (uint32_t)n);
+    }
+    const uint32_t ne = (uint32_t)(2 * cand_t.size());
+    if (ne > 64) return fail(ctx, ASZ_E_UNSUPPORTED, "too many t candidates for the default slope");
+    ProxyEval evals[64];
+    for (int i = 0; i < 2; i++)
+        for (size_t k = 0; k < cand_t.size(); k++) evals[i * cand_t.size() + k] = ProxyEval{cand_t[k], ebs[i]};
+    int rc = upload_log2(ctx);
+    if (rc) return rc;
+    uint32_t bcap, tcap;
+    u64 sstride;
+    scratch_dims(cap, bcap, tcap, sstride);
+    CK(ctx->scratch.reserve(3 * sstride));
+    CK(cudaMemcpyAsync(dm->boxes, boxes, sizeof(boxes), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dm->evals, evals, sizeof(ProxyEval) * ne, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
+    const float R = mx - mn;
+    CK(launch_slope_v0(fg, dm->boxes, dm->evals, ne, d_in, ctx->log2arena.as<float>(), R * R, ctx->scratch.as<uint8_t>(),
+                       sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, ctx->stream));
+    std::vector<float> h1(3 * ne), x(3 * ne);
+    uint32_t m[3], errw;
+    CK(cudaMemcpyAsync(h1.data(), dm->h1, 4 * 3 * ne, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(x.data(), dm->x, 4 * 3 * ne, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(m, dm->m, 12, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (errw) return fail(ctx, ASZ_E_DEVICE, "default-slope kernel reported an internal error");
+    float avg_h1[2] = {0, 0}, avg_psnr[2] = {0, 0};
+    u64 valid[2] = {0, 0};
+    for (int d = 0; d < 3; d++) {
+        if (m[d] == 0)
+            return fail(ctx, ASZ_E_DATA, "In get_default_slope, direction " + std::to_string(d) + " AB_map is empty");
+        for (int i = 0; i < 2; i++)
+            for (size_t k = 0; k < cand_t.size(); k++) {
+                size_t e = (size_t)d * ne + i * cand_t.size() + k;
+                float psnr = 10.0f * log10f(x[e]);
+                avg_h1[i] += h1[e];
+                avg_psnr[i] += psnr;
+                valid[i]++;
+            }
+    }
+    u64 total = 3 * cand_t.size();
+    float recip = 1.0f / (float)total;
+    float max_invalid = 0;
+    for (int i = 0; i < 2; i++) {
+        float inv = std::fma(-recip, (float)valid[i], 1.0f);
+        max_invalid = std::max(inv, max_invalid);
+    }
+    max_invalid_out = max_invalid;
+    reason_out = 0;
+    if (max_invalid >= p.default_slope_invalid_ratio_threshold) {
+        slope_out = p.default_slope_fallback;
+        reason_out = 1;
+        return ASZ_OK;
+    }
+    // Tolerance scale: the approximate reciprocal with one Newton step that the reference's
+    // vectorised average_h1[i]/=valid_case_num[i] uses; the differences use exact divisions.
+    __m128 v = _mm_set_ps(1.0f, 1.0f, (float)valid[1], (float)valid[0]);
+    __m128 r0 = _mm_rcp_ps(v);
+    __m128 r1 = _mm_sub_ps(_mm_add_ps(r0, r0), _mm_mul_ps(r0, _mm_mul_ps(r0, v)));
+    alignas(16) float rr[4];
+    _mm_store_ps(rr, r1);
+    float h1v0 = avg_h1[0] * rr[0], h1v1 = avg_h1[1] * rr[1];
+    float h1_0 = avg_h1[0] / (float)valid[0], h1_1 = avg_h1[1] / (float)valid[1];
+    float ps_0 = avg_psnr[0] / (float)valid[0], ps_1 = avg_psnr[1] / (float)valid[1];
+    float h1_diff = h1_1 - h1_0, psnr_diff = ps_1 - ps_0;
+    float scale = std::max(std::fabs(h1v1), std::fabs(h1v0));
+    float tol = scale > 1.0f ? scale * 0x1p-17f : 0x1p-17f;
+    if (tol >= h1_diff || 0.0f >= psnr_diff) {
+        slope_out = p.default_slope_fallback;
+        reason_out = 2;
+    } else {
+        slope_out = psnr_diff / h1_diff;
+    }
+    return ASZ_OK;
+}
+
+std::vector<float> candidate_t(const asz_params &p) {
+    std::vector<float> c;
+    int lo = (int)host_lround_f(p.t_min * (float)p.t_precision), hi = (int)host_lround_f(p.t_max * (float)p.t_precision);
+    for (int ti = lo; ti <= hi; ti++) c.push_back((float)ti / (float)p.t_precision);
+    return c;
+}
+
+struct StreamOut {
+    HuffCode code;
+    u64 count = 0;
+    u64 payload_word_off = 0;  // in the payload arena (32-bit words)
+    int64_t lo = 0, hi = -1;   // histogram range
+    u64 hist_off = 0;
+};
+
+}  // namespace
+
+extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                            const asz_params *pp, const char *plan_text, uint8_t **out, size_t *out_len, asz_report *rep) {
+    if (!ctx) return ASZ_E_ARG;
+    auto t_start = clk::now();
+    ctx->err.clear();
+    ctx->have_last = false;
+    if (!in || !out || !out_len) return fail(ctx, ASZ_E_ARG, "null argument");
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    int rc = validate(ctx, p, true);
+    if (rc) return rc;
+    rc = validate_dims(ctx, dims, rel_eb);
+    if (rc) return rc;
+    if (!plan_text) return fail(ctx, ASZ_E_UNSUPPORTED, "automatic plan search is not available; pass a predictor plan");
+    Plan plan;
+    std::string perr;
+    if (!parse_plan(plan_text, plan, perr)) return fail(ctx, ASZ_E_ARG, perr);
+    if (plan.pred.size() > 63) return fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    if (p.predictor_family == ASZ_FAMILY_AUTO)
+        return fail(ctx, ASZ_E_UNSUPPORTED, "automatic predictor-family selection is not available; pass a family");
+    const bool quintic = p.predictor_family == ASZ_FAMILY_QUINTIC;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
+    const u64 N = dims[0] * dims[1] * dims[2];
+    const u64 L = plan.pred.size();
+    cudaStream_t st = ctx->stream;
+    asz_report R{};
+
+    CK(ctx->misc.reserve(sizeof(MiscLayout)));
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    // Input.
+    const float *d_in = in;
+    auto t0 = clk::now();
+    if (!in_on_device) {
+        CK(ctx->in.reserve(N * sizeof(float)));
+        CK(cudaMemcpyAsync(ctx->in.p, in, N * sizeof(float), cudaMemcpyHostToDevice, st));
+        d_in = ctx->in.as<float>();
+    }
+    CK(cudaStreamSynchronize(st));
+    R.h2d_s = secs(t0, clk::now());
+    // Data range (s1_compress.cpp:131-138).
+    auto t_range = clk::now();
+    float mn, mx;
+    rc = compute_range(ctx, d_in, N, mn, mx);
+    if (rc) return rc;
+    R.data_range_s = secs(t_range, clk::now());
+    if (mn == mx) return fail(ctx, ASZ_E_DATA, "max_val==min_val");
+    const float abs_eb = rel_eb * (mx - mn);
+    // Default slope.
+    auto t_slope = clk::now();
+    const std::vector<float> cand = candidate_t(p);
+    float slope, max_invalid = 0;
+    int reason = 0;
+    rc = default_slope(ctx, d_in, dims, p, abs_eb, mn, mx, cand, slope, max_invalid, reason);
+    if (rc) return rc;
+    R.default_slope_s = secs(t_slope, clk::now());
+
+    auto t_core = clk::now();
+    Geometry G;
+    build_geometry(dims, plan, p, abs_eb, slope, quintic, G);
+    u64 qb_sum = G.pivots;
+    for (auto &rg : G.rounds) qb_sum += rg.qb_total;
+    if (qb_sum != N) return fail(ctx, ASZ_E_DATA, "total_qb_num!=data.size()");
+    // Buffers: reconstruction, QB streams (pivots first), per-block t.
+    std::vector<u64> qb_off(L + 1), qb_len(L + 1);
+    qb_len[0] = G.pivots;
+    for (u64 l = 0; l < L; l++) qb_len[l + 1] = G.rounds[l].qb_total;
+    u64 acc = 0;
+    for (u64 s = 0; s <= L; s++) {
+        qb_off[s] = acc;
+        acc += qb_len[s];
+    }
+    CK(ctx->rec.reserve(N * sizeof(float)));
+    CK(ctx->qb.reserve(std::max<u64>(acc, 1) * sizeof(int32_t)));
+    CK(ctx->tval.reserve(G.nblocks * sizeof(float)));
+    CK(ctx->tint.reserve(G.nblocks * L * sizeof(int64_t)));
+    CK(ctx->axis.reserve(2 * G.tab_count.size() * sizeof(u64)));
+    CK(ctx->classes.reserve(27 * L * sizeof(ClassInfo)));
+    const u64 amb_cap = 4096;
+    CK(ctx->amb.reserve(amb_cap * sizeof(AmbiguousRecord)));
+    u64 *d_tabc = ctx->axis.as<u64>();
+    u64 *d_tabp = d_tabc + G.tab_count.size();
+    CK(cudaMemcpyAsync(d_tabc, G.tab_count.data(), G.tab_count.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_tabp, G.tab_prefix.data(), G.tab_prefix.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+    for (u64 l = 0; l < L; l++)
+        for (auto &ci : G.classes[l])
+            if (ci.n) ci.log2_off = log2_table(ctx, ci.n);
+    std::vector<ClassInfo> cls_flat;
+    for (u64 l = 0; l < L; l++) cls_flat.insert(cls_flat.end(), G.classes[l].begin(), G.classes[l].end());
+    CK(cudaMemcpyAsync(ctx->classes.p, cls_flat.data(), cls_flat.size() * sizeof(ClassInfo), cudaMemcpyHostToDevice, st));
+    rc = upload_log2(ctx);
+    if (rc) return rc;
+    uint32_t capmax = 1;
+    for (u64 l = 0; l < L; l++) capmax = std::max(capmax, G.cap[l]);
+    uint32_t bcap, tcap;
+    u64 sstride;
+    scratch_dims(capmax, bcap, tcap, sstride);
+    CK(ctx->scratch.reserve(G.nblocks * sstride));
+    const float Rg = mx - mn, R2 = Rg * Rg;
+    const float t_default = 4.0f / 16;  // insufficient_sample_t (asz_param.hpp:206)
+    int32_t init_range[2] = {INT32_MAX, INT32_MIN};
+    std::vector<uint32_t> overrides;  // (block, round, t bits) settled by host replays
+    std::vector<AmbiguousRecord> ambs;
+    uint32_t fb_total = 0;
+    int reruns = 0;
+    float *d_rec = ctx->rec.as<float>();
+    int32_t *d_qb = ctx->qb.as<int32_t>();
+    float *d_tval = ctx->tval.as<float>();
+    int64_t *d_tint = ctx->tint.as<int64_t>();
+    while (true) {
+        // Error word, fallback count, ambiguity count, QB ranges.
+        CK(cudaMemsetAsync(&dm->err, 0, 3 * sizeof(uint32_t), st));
+        for (u64 s = 0; s <= L; s++)
+            CK(cudaMemcpyAsync(&dm->qb_range[2 * s], init_range, 8, cudaMemcpyHostToDevice, st));
+        if (!overrides.empty()) {
+            CK(ctx->overrides.reserve(overrides.size() * sizeof(uint32_t)));
+            CK(cudaMemcpyAsync(ctx->overrides.p, overrides.data(), overrides.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, st));
+        }
+        // Pivots (compress.tpp:162-175).
+        CK(launch_pivot_compress(G.pg, d_in, d_rec, d_qb + qb_off[0], &dm->qb_range[0], st));
+        for (u64 l = 0; l < L; l++) {
+            const RoundGeom &rg = G.rounds[l];
+            CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, ctx->classes.as<ClassInfo>() + 27 * l, d_rec, d_in,
+                              ctx->log2arena.as<float>(), R2, t_default, ctx->scratch.as<uint8_t>(), sstride, capmax, bcap,
+                              tcap, d_tval, d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap,
+                              &dm->amb_count, ctx->overrides.as<uint32_t>(), (uint32_t)(overrides.size() / 3), &dm->err, st));
+            CK(launch_round_compress(G.fg, rg, d_tabc, d_tabp, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
+                                     &dm->qb_range[2 * (l + 1)], &dm->err, st));
+        }
+        uint32_t words[3];
+        CK(cudaMemcpyAsync(words, &dm->err, sizeof(words), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (words[0]) return fail(ctx, ASZ_E_DEVICE, "round kernels reported an internal error " + std::to_string(words[0]));
+        fb_total = words[1];
+        uint32_t namb = words[2];
+        if (namb > amb_cap) return fail(ctx, ASZ_E_UNSUPPORTED, "too many ambiguous coefficient decisions");
+        if (namb == 0) break;
+        ambs.resize(namb);
+        CK(cudaMemcpy(ambs.data(), ctx->amb.p, namb * sizeof(AmbiguousRecord), cudaMemcpyDeviceToHost));
+        bool changed = false;
+        for (const AmbiguousRecord &r : ambs) {
+            float t = replay_decision(r, G.rounds[r.round].slope);
+            int32_t code = (int32_t)host_lround_f(t * (float)p.t_precision);
+            R.ambiguous_decisions++;
+            if (code != r.provisional) {
+                uint32_t bits;
+                std::memcpy(&bits, &t, 4);
+                overrides.push_back(r.block);
+                overrides.push_back(r.round);
+                overrides.push_back(bits);
+                changed = true;
+            }
+        }
+        if (!changed) break;
+        if (++reruns > 16) return fail(ctx, ASZ_E_DEVICE, "coefficient decisions did not settle");
+    }
+    R.reruns = (u64)reruns;
+    R.t_fallback_count = fb_total;
+
+    // ---- Huffman stage: t stream (int64) and L+1 QB streams (int32). ----
+    auto t_huff = clk::now();
+    const u64 nstreams = L + 2;  // index 0: t stream, 1..L+1: QB streams
+    std::vector<StreamOut> so(nstreams);
+    std::vector<int32_t> ranges(2 * (L + 1));
+    CK(cudaMemcpyAsync(ranges.data(), dm->qb_range, ranges.size() * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    so[0].count = G.nblocks * L;
+    {
+        const float tv[6] = {t_default, 1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+        for (float t : tv) {
+            int64_t c = host_lround_f(t * (float)p.t_precision);
+            lo = std::min(lo, c);
+            hi = std::max(hi, c);
+        }
+        so[0].lo = lo;
+        so[0].hi = hi;
+    }
+    for (u64 s = 0; s <= L; s++) {
+        so[s + 1].count = qb_len[s];
+        so[s + 1].lo = ranges[2 * s];
+        so[s + 1].hi = ranges[2 * s + 1];
+    }
+    u64 hist_total = 0;
+    for (auto &o : so) {
+        if (!o.count) continue;
+        u64 range = (u64)(o.hi - o.lo) + 1;
+        if (range > (1ull << 27)) return fail(ctx, ASZ_E_UNSUPPORTED, "QB range too wide for the dense histogram");
+        o.hist_off = hist_total;
+        hist_total += range;
+    }
+    CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
+    CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
+    unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
+    if (so[0].count) CK(launch_histogram<int64_t>(d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off, st));
+    for (u64 s = 0; s <= L; s++)
+        if (so[s + 1].count)
+            CK(launch_histogram<int32_t>(d_qb + qb_off[s], qb_len[s], so[s + 1].lo, (u64)(so[s + 1].hi - so[s + 1].lo) + 1,
+                                         d_hist + so[s + 1].hist_off, st));
+    std::vector<u64> hist(hist_total);
+    if (hist_total) CK(cudaMemcpyAsync(hist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // Codes (host) and payload layout.
+    u64 code_total = 0, words_total = 0, max_count = 0;
+    std::vector<u64> code_off(nstreams);
+    for (u64 s = 0; s < nstreams; s++) {
+        StreamOut &o = so[s];
+        if (!o.count) continue;
+        u64 range = (u64)(o.hi - o.lo) + 1;
+        std::vector<u64> h(hist.begin() + o.hist_off, hist.begin() + o.hist_off + range);
+        // Trim to the symbols present so the code's offset and range match the reference.
+        u64 a = 0, b = range;
+        while (a < b && h[a] == 0) a++;
+        while (b > a && h[b - 1] == 0) b--;
+        std::vector<u64> hh(h.begin() + a, h.begin() + b);
+        std::string e;
+        if (!build_code(hh, o.lo + (int64_t)a, o.lo + (int64_t)b - 1, o.count, s == 0, o.code, e)) return fail(ctx, ASZ_E_UNSUPPORTED, e);
+        o.lo += (int64_t)a;
+        code_off[s] = code_total;
+        code_total += o.code.table.size();
+        o.payload_word_off = words_total;
+        words_total += (o.code.bits + 31) / 32 + 2;
+        max_count = std::max(max_count, o.count);
+    }
+    std::vector<CodeEntry> codes(std::max<u64>(code_total, 1));
+    for (u64 s = 0; s < nstreams; s++)
+        if (so[s].count) std::copy(so[s].code.table.begin(), so[s].code.table.end(), codes.begin() + code_off[s]);
+    CK(ctx->codes.reserve(codes.size() * sizeof(CodeEntry)));
+    CK(cudaMemcpyAsync(ctx->codes.p, codes.data(), codes.size() * sizeof(CodeEntry), cudaMemcpyHostToDevice, st));
+    CK(ctx->payload.reserve(std::max<u64>(words_total, 1) * 4));
+    CK(cudaMemsetAsync(ctx->payload.p, 0, std::max<u64>(words_total, 1) * 4, st));
+    CK(ctx->bitoff.reserve(std::max<u64>(max_count, 1) * 8));
+    size_t tmp_bytes = 0;
+    CK(launch_encode<int32_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp_bytes, nullptr, st));
+    size_t tmp64 = 0;
+    CK(launch_encode<int64_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp64, nullptr, st));
+    tmp_bytes = std::max(tmp_bytes, tmp64);
+    CK(ctx->cubtmp.reserve(tmp_bytes));
+    uint32_t *d_pay = ctx->payload.as<uint32_t>();
+    CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
+    for (u64 s = 0; s < nstreams; s++) {
+        StreamOut &o = so[s];
+        if (!o.count || o.code.maxval == 1) continue;
+        size_t tb = ctx->cubtmp.cap;
+        if (s == 0)
+            CK(launch_encode<int64_t>(d_tint, o.count, o.lo, d_codes + code_off[s], ctx->bitoff.as<u64>(), ctx->cubtmp.p, tb,
+                                      d_pay + o.payload_word_off, st));
+        else
+            CK(launch_encode<int32_t>(d_qb + qb_off[s - 1], o.count, o.lo, d_codes + code_off[s], ctx->bitoff.as<u64>(),
+                                      ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
+    }
+    std::vector<uint32_t> pay(words_total);
+    auto t_d2h = clk::now();
+    if (words_total) CK(cudaMemcpyAsync(pay.data(), d_pay, words_total * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    R.d2h_s = secs(t_d2h, clk::now());
+    // Stream assembly (compress.tpp:233-291).
+    std::vector<uint8_t> &bs = ctx->pre_zstd;
+    bs.clear();
+    u64 total_len = 9 + 2 * L;
+    for (auto &o : so) total_len += 8 + (o.count ? o.code.save_size() + o.code.encode_size() : 0);
+    bs.resize(total_len);
+    uint8_t *w = bs.data();
+    std::memcpy(w, &mn, 4);
+    std::memcpy(w + 4, &mx, 4);
+    w[8] = (uint8_t)(L | 0x40 | (quintic ? 0x80 : 0));
+    w += 9;
+    for (u64 l = 0; l < L; l++) {
+        w[0] = (uint8_t)plan.pred[l][5];
+        w[1] = (uint8_t)plan.pred[l][9];
+        w += 2;
+    }
+    for (u64 s = 0; s < nstreams; s++) {
+        const StreamOut &o = so[s];
+        for (int i = 0; i < 8; i++) w[i] = (uint8_t)(o.count >> (8 * i));
+        w += 8;
+        if (!o.count) continue;
+        write_tree(o.code, w);
+        w += o.code.save_size();
+        write_len_word(o.code, w);
+        w += 8;
+        if (o.code.maxval != 1) {
+            u64 nb = (o.code.bits + 7) >> 3;
+            std::memcpy(w, (const uint8_t *)(pay.data() + o.payload_word_off), nb);
+            w += nb;
+        }
+    }
+    if ((u64)(w - bs.data()) != total_len) return fail(ctx, ASZ_E_DEVICE, "Huffman encoded size mismatch");
+    R.huffman_s = secs(t_huff, clk::now());
+    R.core_s = secs(t_core, clk::now());
+    // zstd level 3 (compress.tpp:294-299).
+    auto t_z = clk::now();
+    size_t bound = ZSTD_compressBound(bs.size());
+    uint8_t *z = (uint8_t *)std::malloc(bound ? bound : 1);
+    if (!z) return fail(ctx, ASZ_E_DATA, "out of host memory");
+    size_t zl = ZSTD_compress(z, bound, bs.data(), bs.size(), 3);
+    if (ZSTD_isError(zl)) {
+        std::free(z);
+        return fail(ctx, ASZ_E_DATA, std::string("ZSTD_compress: ") + ZSTD_getErrorName(zl));
+    }
+    R.zstd_s = secs(t_z, clk::now());
+    *out = z;
+    *out_len = zl;
+    // Report.
+    ctx->qb_off = qb_off;
+    ctx->qb_len = qb_len;
+    ctx->t_len = G.nblocks * L;
+    ctx->n_total = N;
+    ctx->last_in = d_in;
+    ctx->last_min = mn;
+    ctx->last_max = mx;
+    ctx->have_last = true;
+    if (rep) {
+        R.min_val = mn;
+        R.max_val = mx;
+        R.abs_eb = abs_eb;
+        R.default_slope = slope;
+        R.slope_max_invalid_ratio = max_invalid;
+        R.slope_fallback_reason = reason;
+        R.pre_zstd_len = bs.size();
+        R.asz_len = zl;
+        R.layer_num = L;
+        R.quintic = quintic ? 1 : 0;
+        for (int a = 0; a < 3; a++) {
+            R.pivot_stride[a] = (uint32_t)G.fg.pivot_stride[a];
+            R.block_shape[a] = (uint32_t)G.fg.block_shape[a];
+            R.block_num[a] = (uint32_t)G.fg.block_num[a];
+        }
+        std::string pl;
+        for (u64 l = 0; l < L; l++) pl += (l ? "," : "") + plan.pred[l];
+        std::snprintf(R.plan, sizeof(R.plan), "%s", pl.c_str());
+        R.cr = (float)N * sizeof(float) / (float)zl;
+        R.br = 8 * sizeof(float) / R.cr;
+        R.total_s = secs(t_start, clk::now());
+        *rep = R;
+    }
+    return ASZ_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Decompression.
+
+namespace {
+
+int gpu_decode(asz_ctx *ctx, const HuffParsed &hp, uint64_t count, const uint8_t *d_base, uint64_t base_off, void *d_out,
+               bool wide, cudaStream_t st) {
+    if (hp.single) {
+        if (hp.single_count != count) return fail(ctx, ASZ_E_DATA, "Huffman payload length does not match its value count");
+        if (wide) CK(launch_fill<int64_t>((int64_t *)d_out, count, (int64_t)hp.offset, st));
+        else CK(launch_fill<int32_t>((int32_t *)d_out, count, (int32_t)hp.offset, st));
+        return ASZ_OK;
+    }
+    // Tables.
+    const u64 lut_bytes = hp.lut.size() * sizeof(LutEntry), child_bytes = hp.child.size() * sizeof(uint32_t);
+    CK(ctx->codes.reserve(lut_bytes + child_bytes + 16));
+    CK(cudaMemcpyAsync(ctx->codes.p, hp.lut.data(), lut_bytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((uint8_t *)ctx->codes.p + lut_bytes, hp.child.data(), child_bytes, cudaMemcpyHostToDevice, st));
+    DecodeTables dt{(const LutEntry *)ctx->codes.p, (const uint32_t *)((uint8_t *)ctx->codes.p + lut_bytes), hp.lut_bits};
+    const u64 abs_off = base_off + hp.payload_off;
+    const uint8_t *aligned = d_base + (abs_off & ~3ull);
+    const u64 bit_begin = (abs_off & 3ull) * 8, bit_end = bit_begin + hp.payload_bits;
+    const u64 C = 4096;
+    const u64 nch = std::max<u64>(1, (hp.payload_bits + C - 1) / C);
+    CK(ctx->chunks.reserve(4 * nch * 8 + 64));
+    u64 *d_start = ctx->chunks.as<u64>(), *d_end = d_start + nch, *d_cnt = d_end + nch, *d_off = d_cnt + nch;
+    uint32_t *d_flag = (uint32_t *)(d_off + nch);
+    std::vector<u64> start(nch);
+    for (u64 k = 0; k < nch; k++) start[k] = bit_begin + k * C;
+    CK(cudaMemcpyAsync(d_start, start.data(), nch * 8, cudaMemcpyHostToDevice, st));
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+    for (u64 it = 0;; it++) {
+        CK(launch_decode_sync(aligned, bit_begin, bit_end, C, nch, dt, d_start, d_end, d_cnt, &dm->err, st));
+        CK(cudaMemsetAsync(d_flag, 0, 4, st));
+        CK(launch_decode_restart(nch, d_end, d_start, d_flag, st));
+        uint32_t flag;
+        CK(cudaMemcpyAsync(&flag, d_flag, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (!flag) break;
+        if (it > nch + 2) return fail(ctx, ASZ_E_DATA, "Huffman payload does not synchronise");
+    }
+    size_t tb = 0;
+    CK(launch_scan_u64(d_cnt, d_off, nch, nullptr, tb, st));
+    CK(ctx->cubtmp.reserve(tb));
+    tb = ctx->cubtmp.cap;
+    CK(launch_scan_u64(d_cnt, d_off, nch, ctx->cubtmp.p, tb, st));
+    u64 last[3];
+    CK(cudaMemcpyAsync(&last[0], d_off + nch - 1, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[1], d_cnt + nch - 1, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[2], d_end + nch - 1, 8, cudaMemcpyDeviceToHost, st));
+    uint32_t errw;
+    CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (errw) return fail(ctx, ASZ_E_DATA, "corrupt Huffman payload");
+    if (last[2] != bit_end) return fail(ctx, ASZ_E_DATA, "Huffman payload ends inside a code");
+    if (last[0] + last[1] != count)
+        return fail(ctx, ASZ_E_DATA, last[0] + last[1] < count ? "Huffman payload contains too few values"
+                                                               : "Huffman payload contains too many values");
+    if (wide)
+        CK(launch_decode_write<int64_t>(aligned, bit_begin, bit_end, C, nch, dt, hp.offset, d_start, d_off, (int64_t *)d_out,
+                                        count, &dm->err, st));
+    else
+        CK(launch_decode_write<int32_t>(aligned, bit_begin, bit_end, C, nch, dt, hp.offset, d_start, d_off, (int32_t *)d_out,
+                                        count, &dm->err, st));
+    return ASZ_OK;
+}
+
+}  // namespace
+
+extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const uint64_t dims[3], float rel_eb,
+                              const asz_params *pp, float *out, int out_on_device, asz_report *rep) {
+    if (!ctx) return ASZ_E_ARG;
+    auto t_start = clk::now();
+    ctx->err.clear();
+    if (!in || !out) return fail(ctx, ASZ_E_ARG, "null argument");
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    int rc = validate(ctx, p, false);
+    if (rc) return rc;
+    rc = validate_dims(ctx, dims, rel_eb);
+    if (rc) return rc;
+    if (len == 0) return fail(ctx, ASZ_E_DATA, "compressed input is empty");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    asz_report R{};
+    // zstd (decompress.tpp:83-86).
+    auto t_z = clk::now();
+    unsigned long long raw = ZSTD_getFrameContentSize(in, len);
+    if (raw == ZSTD_CONTENTSIZE_ERROR || raw == ZSTD_CONTENTSIZE_UNKNOWN || raw > (1ull << 40))
+        return fail(ctx, ASZ_E_DATA, "ZSTD_decompress error in decompress()");
+    std::vector<uint8_t> bs(raw + 16, 0);
+    size_t got = ZSTD_decompress(bs.data(), raw, in, len);
+    if (ZSTD_isError(got) || got != raw) return fail(ctx, ASZ_E_DATA, "ZSTD_decompress error in decompress()");
+    R.zstd_s = secs(t_z, clk::now());
+    auto t_h = clk::now();
+    // Header (decompress.tpp:89-119).
+    if (raw < 9) return fail(ctx, ASZ_E_DATA, "truncated header");
+    float mn, mx;
+    std::memcpy(&mn, bs.data(), 4);
+    std::memcpy(&mx, bs.data() + 4, 4);
+    uint8_t flags = bs[8];
+    u64 L = flags;
+    bool quintic = p.predictor_family == ASZ_FAMILY_QUINTIC;
+    if (flags & 0x40) {
+        quintic = (flags & 0x80) != 0;
+        L = flags & 0x3f;
+    }
+    u64 pos = 9;
+    if (raw - pos < 2 * L) return fail(ctx, ASZ_E_DATA, "truncated header");
+    std::string ptxt;
+    for (u64 l = 0; l < L; l++) {
+        uint8_t a = bs[pos], o = bs[pos + 1];
+        if (a < '0' || a > '2' || o < '0' || o > '2') return fail(ctx, ASZ_E_DATA, "compressed stream contains an invalid predictor");
+        ptxt += (l ? "," : "") + std::string("cubic") + (char)a + "_" + (o == '0' ? "120" : o == '1' ? "021" : "012");
+        pos += 2;
+    }
+    Plan plan;
+    std::string perr;
+    if (L == 0 || !parse_plan(ptxt.c_str(), plan, perr)) return fail(ctx, ASZ_E_DATA, "compressed stream contains no rounds");
+    auto rd64 = [&](u64 &v) {
+        if (raw - pos < 8) return false;
+        v = 0;
+        for (int i = 0; i < 8; i++) v |= (u64)bs[pos + i] << (8 * i);
+        pos += 8;
+        return true;
+    };
+    std::vector<HuffParsed> hp(L + 2);
+    std::vector<u64> counts(L + 2);
+    for (u64 s = 0; s < L + 2; s++) {
+        if (!rd64(counts[s])) return fail(ctx, ASZ_E_DATA, "truncated stream length");
+        if (!counts[s]) continue;
+        std::string e;
+        if (!parse_stream(bs.data(), raw, pos, hp[s], e)) return fail(ctx, ASZ_E_DATA, e);
+    }
+    const float abs_eb = rel_eb * (mx - mn);
+    Geometry G;
+    build_geometry(dims, plan, p, abs_eb, 0.0f, quintic, G);
+    const u64 N = dims[0] * dims[1] * dims[2];
+    if (counts[0] < G.nblocks * L) return fail(ctx, ASZ_E_DATA, "compressed stream contains too few t values");
+    if (counts[1] < G.pivots) return fail(ctx, ASZ_E_DATA, "compressed stream has too few QBs");
+    for (u64 l = 0; l < L; l++)
+        if (counts[l + 2] < G.rounds[l].qb_total) return fail(ctx, ASZ_E_DATA, "compressed stream has too few QBs");
+    // Device: stream bytes, t codes, QB streams.
+    CK(ctx->misc.reserve(sizeof(MiscLayout)));
+    CK(ctx->pre.reserve(raw + 16));
+    auto t0 = clk::now();
+    CK(cudaMemcpyAsync(ctx->pre.p, bs.data(), raw + 16, cudaMemcpyHostToDevice, st));
+    R.h2d_s += secs(t0, clk::now());
+    std::vector<u64> qoff(L + 1);
+    u64 qtot = 0;
+    for (u64 s = 0; s <= L; s++) {
+        qoff[s] = qtot;
+        qtot += counts[s + 1];
+    }
+    CK(ctx->tint.reserve(std::max<u64>(counts[0], 1) * 8));
+    CK(ctx->qb.reserve(std::max<u64>(qtot, 1) * 4));
+    if (counts[0]) {
+        rc = gpu_decode(ctx, hp[0], counts[0], ctx->pre.as<uint8_t>(), 0, ctx->tint.p, true, st);
+        if (rc) return rc;
+    }
+    for (u64 s = 0; s <= L; s++) {
+        if (!counts[s + 1]) continue;
+        rc = gpu_decode(ctx, hp[s + 1], counts[s + 1], ctx->pre.as<uint8_t>(), 0, ctx->qb.as<int32_t>() + qoff[s], false, st);
+        if (rc) return rc;
+    }
+    R.huffman_s = secs(t_h, clk::now());
+    // Reconstruction.
+    auto t_core = clk::now();
+    float *d_out = out;
+    if (!out_on_device) {
+        CK(ctx->rec.reserve(N * sizeof(float)));
+        d_out = ctx->rec.as<float>();
+    }
+    CK(ctx->axis.reserve(2 * G.tab_count.size() * sizeof(u64)));
+    u64 *d_tabc = ctx->axis.as<u64>(), *d_tabp = d_tabc + G.tab_count.size();
+    CK(cudaMemcpyAsync(d_tabc, G.tab_count.data(), G.tab_count.size() * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_tabp, G.tab_prefix.data(), G.tab_prefix.size() * 8, cudaMemcpyHostToDevice, st));
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+    CK(launch_pivot_decompress(G.pg, ctx->qb.as<int32_t>() + qoff[0], d_out, st));
+    for (u64 l = 0; l < L; l++)
+        CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_tabc, d_tabp, ctx->tint.as<int64_t>(),
+                                   ctx->qb.as<int32_t>() + qoff[l + 1], d_out, &dm->err, st));
+    uint32_t errw;
+    CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (errw) return fail(ctx, ASZ_E_DEVICE, "reconstruction kernels reported an internal error");
+    R.core_s = secs(t_core, clk::now());
+    if (!out_on_device) {
+        auto t1 = clk::now();
+        CK(cudaMemcpyAsync(out, d_out, N * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        R.d2h_s = secs(t1, clk::now());
+    }
+    if (rep) {
+        R.min_val = mn;
+        R.max_val = mx;
+        R.abs_eb = abs_eb;
+        R.layer_num = L;
+        R.quintic = quintic;
+        R.asz_len = len;
+        R.pre_zstd_len = raw;
+        R.cr = (float)N * sizeof(float) / (float)len;
+        R.br = 8 * sizeof(float) / R.cr;
+        std::snprintf(R.plan, sizeof(R.plan), "%s", ptxt.c_str());
+        for (int a = 0; a < 3; a++) {
+            R.pivot_stride[a] = (uint32_t)G.fg.pivot_stride[a];
+            R.block_shape[a] = (uint32_t)G.fg.block_shape[a];
+            R.block_num[a] = (uint32_t)G.fg.block_num[a];
+        }
+        R.total_s = secs(t_start, clk::now());
+        *rep = R;
+    }
+    return ASZ_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Debug accessors for the last asz_compress call.
+
+extern "C" uint64_t asz_debug_qb(asz_ctx *ctx, uint32_t stream, int32_t *dst) {
+    if (!ctx || !ctx->have_last || stream >= ctx->qb_len.size()) return 0;
+    if (dst) cudaMemcpy(dst, ctx->qb.as<int32_t>() + ctx->qb_off[stream], ctx->qb_len[stream] * 4, cudaMemcpyDeviceToHost);
+    return ctx->qb_len[stream];
+}
+
+extern "C" uint64_t asz_debug_t(asz_ctx *ctx, int64_t *dst) {
+    if (!ctx || !ctx->have_last) return 0;
+    if (dst) cudaMemcpy(dst, ctx->tint.p, ctx->t_len * 8, cudaMemcpyDeviceToHost);
+    return ctx->t_len;
+}
+
+extern "C" uint64_t asz_debug_recon(asz_ctx *ctx, float *dst) {
+    if (!ctx || !ctx->have_last) return 0;
+    if (dst) cudaMemcpy(dst, ctx->rec.p, ctx->n_total * 4, cudaMemcpyDeviceToHost);
+    return ctx->n_total;
+}
+
+extern "C" uint64_t asz_debug_pre_zstd(asz_ctx *ctx, uint8_t *dst) {
+    if (!ctx || !ctx->have_last) return 0;
+    if (dst) std::memcpy(dst, ctx->pre_zstd.data(), ctx->pre_zstd.size());
+    return ctx->pre_zstd.size();
+}
+
+extern "C" int asz_compress_stats(asz_ctx *ctx, double *max_err, double *psnr) {
+    if (!ctx) return ASZ_E_ARG;
+    if (!ctx->have_last) return fail(ctx, ASZ_E_ARG, "no compression on this context");
+    cudaStream_t st = ctx->stream;
+    struct {
+        unsigned int mx;
+        unsigned int pad;
+        double sse;
+    } h{}, *d = (decltype(&h))ctx->misc.as<uint8_t>();
+    CK(cudaMemsetAsync(d, 0, sizeof(h), st));
+    CK(launch_error_stats(ctx->last_in, ctx->rec.as<float>(), ctx->n_total, &d->mx, &d->sse, st));
+    CK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float m;
+    std::memcpy(&m, &h.mx, 4);
+    double mse = h.sse / (double)ctx->n_total;
+    double range = (double)ctx->last_max - (double)ctx->last_min;
+    if (max_err) *max_err = m;
+    if (psnr) *psnr = 10.0 * std::log10(range * range / mse);
+    return ASZ_OK;
+}

@@ -1,0 +1,16 @@
+// The libzstd entry points this library calls. The system provides libzstd.so.1 without its
+// development header, so the prototypes of zstd's stable public API are declared here.
+#pragma once
+#include <cstddef>
+
+extern "C" {
+size_t ZSTD_compressBound(size_t srcSize);
+size_t ZSTD_compress(void *dst, size_t dstCapacity, const void *src, size_t srcSize, int compressionLevel);
+size_t ZSTD_decompress(void *dst, size_t dstCapacity, const void *src, size_t compressedSize);
+unsigned long long ZSTD_getFrameContentSize(const void *src, size_t srcSize);
+unsigned ZSTD_isError(size_t code);
+const char *ZSTD_getErrorName(size_t code);
+}
+
+#define ZSTD_CONTENTSIZE_UNKNOWN (0ULL - 1)
+#define ZSTD_CONTENTSIZE_ERROR (0ULL - 2)

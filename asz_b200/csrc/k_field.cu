@@ -1,0 +1,330 @@
+// Field-wide kernels: data range, pivot lattice, and the per-round prediction/quantisation.
+//
+// One launch per round covers every target of the round in every block (round-major). The
+// reference walks block-major (compress.tpp:179-209), but the two orders give the same result.
+// Every target is written once, by the block that owns it: lower faces on the non-prediction
+// axes belong to the lower block (compress.tpp:59). Every stencil read hits a point finished in
+// an earlier round or a pivot.
+#include <cuda_runtime.h>
+
+#include "dev_common.cuh"
+#include "launch.h"
+
+namespace asz {
+
+// ---------------------------------------------------------------------------------------------
+// Data range (c_codes/s1_compress.cpp:128-138). std::minmax_element returns the first minimum and
+// the last maximum, which matters only for the sign of a zero extremum; the host resolves that
+// case with zero_first_last_kernel.
+
+__device__ __forceinline__ int32_t ord_key(float v) {
+    int32_t b = __float_as_int(v == 0.0f ? 0.0f : v);
+    return b >= 0 ? b : (int32_t)(0x80000000u - (uint32_t)b) - 1;
+}
+
+// out[0] = min key, out[1] = max key (ordered-int encoding), out[2] = count of non-finite values.
+__global__ void range_kernel(const float4 *__restrict__ x4, uint64_t n4, const float *__restrict__ tail, uint32_t ntail,
+                             int32_t *out, unsigned long long *nonfinite) {
+    int32_t mn = INT32_MAX, mx = INT32_MIN;
+    unsigned long long bad = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
+        float4 v = x4[i];
+        float a[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!isfinite(a[k])) {
+                bad++;
+                continue;
+            }
+            int32_t o = ord_key(a[k]);
+            mn = min(mn, o);
+            mx = max(mx, o);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < ntail) {
+        float v = tail[threadIdx.x];
+        if (!isfinite(v)) bad++;
+        else {
+            mn = min(mn, ord_key(v));
+            mx = max(mx, ord_key(v));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&out[0], mn);
+        atomicMax(&out[1], mx);
+        if (bad) atomicAdd(nonfinite, bad);
+    }
+}
+
+// First and last index of a zero (either sign), for the sign of a zero minimum or maximum.
+__global__ void zero_first_last_kernel(const float *__restrict__ x, uint64_t n, unsigned long long *first,
+                                       unsigned long long *last) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+        if (x[i] == 0.0f) {
+            atomicMin(first, (unsigned long long)i);
+            atomicMax(last, (unsigned long long)i);
+        }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pivots (compress.tpp:162-175, decompress.tpp:160-171). Stream 0 is the pivot lattice in raster
+// order. Compress: qb = llround(x * (0.5/pivot_eb)) (hoisted reciprocal, double), value
+// qb*(2*pivot_eb) in double rounded to float.
+
+__global__ void pivot_compress_kernel(PivotGeom pg, const float *__restrict__ in, float *__restrict__ rec,
+                                      int32_t *__restrict__ qb, int32_t *qb_range) {
+    const uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t k2 = k % pg.cnt[2], k1 = (k / pg.cnt[2]) % pg.cnt[1], k0 = k / (pg.cnt[1] * pg.cnt[2]);
+        uint64_t pos = k0 * pg.stride[0] * pg.n1n2 + k1 * pg.stride[1] * pg.n2 + k2 * pg.stride[2];
+        int32_t q = (int32_t)lround_d(__dmul_rn((double)in[pos], pg.rp));
+        qb[k] = q;
+        rec[pos] = __double2float_rn(__dmul_rn((double)q, pg.peb2));
+        lo = min(lo, q);
+        hi = max(hi, q);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&qb_range[0], lo);
+        atomicMax(&qb_range[1], hi);
+    }
+}
+
+__global__ void pivot_decompress_kernel(PivotGeom pg, const int32_t *__restrict__ qb, float *__restrict__ rec) {
+    const uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t k2 = k % pg.cnt[2], k1 = (k / pg.cnt[2]) % pg.cnt[1], k0 = k / (pg.cnt[1] * pg.cnt[2]);
+        uint64_t pos = k0 * pg.stride[0] * pg.n1n2 + k1 * pg.stride[1] * pg.n2 + k2 * pg.stride[2];
+        rec[pos] = __double2float_rn(__dmul_rn((double)qb[k], pg.peb2));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Prediction (compress.tpp:7-34, decompress.tpp:6-33) in the emitted form:
+//   1D6R:            (float) fma(a*s5, fma(inner*s1, b*s3)) in double
+//   left, one ref:   x-1
+//   left, two refs:  (x-1 + x1) * 0.5
+//   left, three:     (fmaf(x-1, 3, 6*x1) - x3) * 0.125
+//   right edge:      fmaf(x-1, 3, -x-3) * 0.5
+//   right second:    fmaf(x1, 3, fmaf(x-1, 6, -x-3)) * 0.125
+//   interior 1D4R:   p=(float)(s3*(0.25-t)); (float)fma(0.25+t, s1, p) in double
+__device__ __forceinline__ float predict(const float *__restrict__ c, uint64_t i, uint64_t hs, uint64_t right, uint64_t pos,
+                                         uint64_t dist, float t, bool quintic) {
+    if (quintic && i >= 5 * hs && i + 5 * hs < right) {
+        float s1 = __fadd_rn(c[pos - dist], c[pos + dist]);
+        float s3 = __fadd_rn(c[pos - 3 * dist], c[pos + 3 * dist]);
+        float s5 = __fadd_rn(c[pos - 5 * dist], c[pos + 5 * dist]);
+        double acc = __dmul_rn((double)s3, kQuinticB);
+        acc = __fma_rn((double)s1, kQuinticI, acc);
+        acc = __fma_rn((double)s5, kQuinticA, acc);
+        return __double2float_rn(acc);
+    }
+    if (i <= hs) {
+        if (i + hs >= right) return c[pos - dist];
+        if (i + 3 * hs >= right) return __fmul_rn(__fadd_rn(c[pos - dist], c[pos + dist]), 0.5f);
+        return __fmul_rn(__fsub_rn(__fmaf_rn(c[pos - dist], 3.0f, __fmul_rn(c[pos + dist], 6.0f)), c[pos + 3 * dist]), 0.125f);
+    }
+    if (i + hs >= right) return __fmul_rn(__fmaf_rn(c[pos - dist], 3.0f, -c[pos - 3 * dist]), 0.5f);
+    if (i + 3 * hs >= right)
+        return __fmul_rn(__fmaf_rn(c[pos + dist], 3.0f, __fmaf_rn(c[pos - dist], 6.0f, -c[pos - 3 * dist])), 0.125f);
+    float s3 = __fadd_rn(c[pos - 3 * dist], c[pos + 3 * dist]);
+    float s1 = __fadd_rn(c[pos - dist], c[pos + dist]);
+    double td = (double)t;
+    float p1 = __double2float_rn(__dmul_rn((double)s3, __dsub_rn(0.25, td)));
+    return __double2float_rn(__fma_rn(__dadd_rn(0.25, td), (double)s1, (double)p1));
+}
+
+// Per-axis block tables of one round: count[b] targets of block b along the axis and prefix[b]
+// (exclusive sum), laid out at RoundGeom::axis_off[a].
+struct AxisTables {
+    const uint64_t *count, *prefix;
+};
+
+struct Target {
+    uint64_t pos, i, right, qi, block;
+};
+
+// Global target k of the round -> position, owning block, stencil bound and QB index.
+__device__ __forceinline__ Target locate(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, uint64_t k) {
+    uint64_t k2 = k % rg.tcount[2], k1 = (k / rg.tcount[2]) % rg.tcount[1], k0 = k / (rg.tcount[1] * rg.tcount[2]);
+    const uint64_t kk[3] = {k0, k1, k2};
+    uint64_t ii[3], bb[3], jj[3], cc[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        ii[a] = a == rg.dir ? rg.hs + 2 * rg.hs * kk[a] : rg.stride[a] * kk[a];
+        bb[a] = owner_block(ii[a], fg.block_shape[a]);
+        uint64_t start = bb[a] * fg.block_shape[a] +
+                         (a == rg.dir ? rg.hs : (bb[a] == 0 ? 0 : rg.stride[a]));
+        jj[a] = (ii[a] - start) / rg.stride[a];
+        cc[a] = at.count[rg.axis_off[a] + bb[a]];
+    }
+    Target t;
+    t.pos = (ii[0] * fg.n[1] + ii[1]) * fg.n[2] + ii[2];
+    t.i = ii[rg.dir];
+    t.right = min((bb[rg.dir] + 1) * fg.block_shape[rg.dir] + 1, fg.n[rg.dir]);
+    // QB base of the block: per-axis prefix sums of the raster-ordered box sizes.
+    uint64_t base = at.prefix[rg.axis_off[0] + bb[0]] * rg.total[1] * rg.total[2] +
+                    cc[0] * at.prefix[rg.axis_off[1] + bb[1]] * rg.total[2] +
+                    cc[0] * cc[1] * at.prefix[rg.axis_off[2] + bb[2]];
+    // get_qb_index (asz_param.hpp:122-129).
+    uint64_t local = rg.order == 0 ? (jj[1] * cc[2] + jj[2]) * cc[0] + jj[0]
+                   : rg.order == 1 ? (jj[0] * cc[2] + jj[2]) * cc[1] + jj[1]
+                                   : (jj[0] * cc[1] + jj[1]) * cc[2] + jj[2];
+    t.qi = base + local;
+    t.block = (bb[0] * fg.block_num[1] + bb[1]) * fg.block_num[2] + bb[2];
+    return t;
+}
+
+// Compress round: quantise the residual and write the reconstruction in place.
+// compress.tpp:35-37 as emitted: axis 0 multiplies by the hoisted 0.5*(1/eb) (inlined loop),
+// axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
+__global__ void round_compress_kernel(FieldGeom fg, RoundGeom rg, const uint64_t *__restrict__ tab_count,
+                                      const uint64_t *__restrict__ tab_prefix, const float *__restrict__ tval,
+                                      const float *__restrict__ in, float *__restrict__ rec, int32_t *__restrict__ qb,
+                                      int32_t *qb_range, uint32_t *err_word) {
+    AxisTables at{tab_count, tab_prefix};
+    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), r0 = __dmul_rn(__ddiv_rn(1.0, ebd), 0.5);
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < rg.targets; k += (uint64_t)gridDim.x * blockDim.x) {
+        Target tg = locate(fg, rg, at, k);
+        if (tg.qi >= rg.qb_total) {
+            atomicOr(err_word, 4u);
+            continue;
+        }
+        float pred = predict(rec, tg.i, rg.hs, tg.right, tg.pos, rg.dist, tval[tg.block], fg.quintic != 0);
+        double pd = (double)pred;
+        double diff = __dsub_rn(pd, (double)in[tg.pos]);
+        double q = rg.dir == 0 ? __dmul_rn(diff, r0) : __ddiv_rn(__dmul_rn(diff, 0.5), ebd);
+        int32_t v = (int32_t)lround_d(q);
+        qb[tg.qi] = v;
+        rec[tg.pos] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&qb_range[0], lo);
+        atomicMax(&qb_range[1], hi);
+    }
+}
+
+// Decompress round (decompress.tpp:34): value = fma(-qb, 2eb, pred) in double, t = t_int/t_precision.
+__global__ void round_decompress_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const uint64_t *__restrict__ tab_count,
+                                        const uint64_t *__restrict__ tab_prefix, const int64_t *__restrict__ t_int,
+                                        const int32_t *__restrict__ qb, float *__restrict__ rec, uint32_t *err_word) {
+    AxisTables at{tab_count, tab_prefix};
+    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd);
+    const float tp = (float)fg.t_precision;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < rg.targets; k += (uint64_t)gridDim.x * blockDim.x) {
+        Target tg = locate(fg, rg, at, k);
+        if (tg.qi >= rg.qb_total) {
+            atomicOr(err_word, 4u);
+            continue;
+        }
+        float t = __fdiv_rn(__ll2float_rn(t_int[tg.block * fg.layer_num + l]), tp);
+        float pred = predict(rec, tg.i, rg.hs, tg.right, tg.pos, rg.dist, t, fg.quintic != 0);
+        rec[tg.pos] = __double2float_rn(__fma_rn(-(double)qb[tg.qi], eb2, (double)pred));
+    }
+}
+
+}  // namespace asz
+
+// ---------------------------------------------------------------------------------------------
+// Launchers (declared in launch.h).
+namespace asz {
+
+static unsigned grid_for(uint64_t n, unsigned threads, unsigned cap) {
+    uint64_t b = (n + threads - 1) / threads;
+    return (unsigned)(b < cap ? (b ? b : 1) : cap);
+}
+
+cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st) {
+    uint64_t n4 = ((uintptr_t)x % 16 == 0) ? n / 4 : 0;
+    uint32_t ntail = (uint32_t)(n - 4 * n4);
+    if (ntail > 1024) return cudaErrorInvalidValue;
+    range_kernel<<<grid_for(n4 ? n4 : 1, 256, 148 * 8), max(256u, ntail), 0, st>>>((const float4 *)x, n4, x + 4 * n4,
+                                                                                     ntail, out, nonfinite);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
+                                   cudaStream_t st) {
+    zero_first_last_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(x, n, first, last);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *rec, int32_t *qb, int32_t *qb_range,
+                                  cudaStream_t st) {
+    uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
+    pivot_compress_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, st>>>(pg, in, rec, qb, qb_range);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, float *rec, cudaStream_t st) {
+    uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
+    pivot_decompress_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, st>>>(pg, qb, rec);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const uint64_t *tab_count,
+                                  const uint64_t *tab_prefix, const float *tval, const float *in, float *rec, int32_t *qb,
+                                  int32_t *qb_range, uint32_t *err, cudaStream_t st) {
+    round_compress_kernel<<<grid_for(rg.targets, 256, 148 * 32), 256, 0, st>>>(fg, rg, tab_count, tab_prefix, tval, in, rec,
+                                                                                qb, qb_range, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const uint64_t *tab_count,
+                                    const uint64_t *tab_prefix, const int64_t *t_int, const int32_t *qb, float *rec,
+                                    uint32_t *err, cudaStream_t st) {
+    round_decompress_kernel<<<grid_for(rg.targets, 256, 148 * 32), 256, 0, st>>>(fg, rg, l, tab_count, tab_prefix, t_int, qb,
+                                                                                  rec, err);
+    return cudaGetLastError();
+}
+
+}  // namespace asz
+
+// ---------------------------------------------------------------------------------------------
+// Error statistics of a reconstruction: max |x - y| (as float bits, non-negative) and the sum of
+// squared differences in double.
+namespace asz {
+__global__ void error_stats_kernel(const float *__restrict__ x, const float *__restrict__ y, uint64_t n,
+                                   unsigned int *max_bits, double *sse) {
+    float mx = 0.0f;
+    double s = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        float d = fabsf(__fsub_rn(x[i], y[i]));
+        mx = fmaxf(mx, d);
+        double dd = (double)x[i] - (double)y[i];
+        s = __fma_rn(dd, dd, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(max_bits, __float_as_uint(mx));
+        atomicAdd(sse, s);
+    }
+}
+
+cudaError_t launch_error_stats(const float *x, const float *y, uint64_t n, unsigned int *max_bits, double *sse,
+                               cudaStream_t st) {
+    error_stats_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(x, y, n, max_bits, sse);
+    return cudaGetLastError();
+}
+}  // namespace asz

@@ -1,0 +1,83 @@
+// Host-callable launchers for the CUDA kernels, and the structs they share with the host.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "dev_common.cuh"
+#include "tsel.cuh"
+
+namespace asz {
+
+struct PivotGeom {
+    uint64_t cnt[3];      // pivots per axis
+    uint64_t stride[3];
+    uint64_t n1n2, n2;
+    double rp;            // 0.5 / (double)pivot_eb
+    double peb2;          // 2 * (double)pivot_eb
+};
+
+struct CodeEntry {
+    uint32_t code;
+    uint32_t len;
+};
+
+struct LutEntry {
+    uint32_t sym;   // symbol index (value - offset), or tree node when len == 0
+    uint32_t len;
+};
+
+struct DecodeTables {
+    const LutEntry *lut;
+    const uint32_t *child;
+    uint32_t lut_bits;
+};
+
+cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st);
+cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
+                                   cudaStream_t st);
+cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *rec, int32_t *qb, int32_t *qb_range,
+                                  cudaStream_t st);
+cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, float *rec, cudaStream_t st);
+cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const uint64_t *tab_count,
+                                  const uint64_t *tab_prefix, const float *tval, const float *in, float *rec, int32_t *qb,
+                                  int32_t *qb_range, uint32_t *err, cudaStream_t st);
+cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const uint64_t *tab_count,
+                                    const uint64_t *tab_prefix, const int64_t *t_int, const int32_t *qb, float *rec,
+                                    uint32_t *err, cudaStream_t st);
+
+cudaError_t launch_error_stats(const float *x, const float *y, uint64_t n, unsigned int *max_bits, double *sse,
+                               cudaStream_t st);
+
+uint64_t tsel_scratch_bytes(uint32_t cap, uint32_t bcap, uint32_t tcap);
+cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
+                           const float *orig, const float *log2arena, float R2, float t_default, uint8_t *scratch,
+                           uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap, float *tval, int64_t *t_int,
+                           uint32_t *fb_count, AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
+                           const uint32_t *overrides, uint32_t n_overrides, uint32_t *err, cudaStream_t st);
+cudaError_t launch_slope_v0(const FieldGeom &fg, const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals,
+                            const float *orig, const float *log2arena, float R2, uint8_t *scratch, uint64_t scratch_stride,
+                            uint32_t cap, uint32_t bcap, uint32_t tcap, float *h1, float *x, uint32_t *m_out, uint32_t *err,
+                            cudaStream_t st);
+
+template <class T>
+cudaError_t launch_histogram(const T *s, uint64_t n, int64_t offset, uint64_t range, unsigned long long *hist,
+                             cudaStream_t st);
+template <class T>
+cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntry *tab, uint64_t *bitoff, void *tmp,
+                          size_t &tmp_bytes, uint32_t *out, cudaStream_t st);
+cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st);
+cudaError_t launch_decode_sync(const uint8_t *payload, uint64_t bit_begin, uint64_t bit_end, uint64_t chunk_bits,
+                               uint64_t nchunks, DecodeTables dt, const uint64_t *start, uint64_t *end, uint64_t *count,
+                               uint32_t *err, cudaStream_t st);
+cudaError_t launch_decode_restart(uint64_t nchunks, const uint64_t *end, uint64_t *start, uint32_t *changed,
+                                  cudaStream_t st);
+template <class T>
+cudaError_t launch_decode_write(const uint8_t *payload, uint64_t bit_begin, uint64_t bit_end, uint64_t chunk_bits,
+                                uint64_t nchunks, DecodeTables dt, int64_t offset, const uint64_t *start, const uint64_t *off,
+                                T *out, uint64_t nout, uint32_t *err, cudaStream_t st);
+template <class T>
+cudaError_t launch_fill(T *out, uint64_t n, T v, cudaStream_t st);
+
+}  // namespace asz

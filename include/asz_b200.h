@@ -1,0 +1,144 @@
+/* asz_b200: B200-native implementation of the ASZ compression hot path behind a C ABI.
+ *
+ * The reference (ASZ) has no library boundary of its own: callers drive the CLI binaries
+ * s1_compress / s1_decompress and exchange raw float32 files and .asz streams. These entry points
+ * replace that surface one for one:
+ *
+ *   asz_compress    replaces s1_compress's main (c_codes/s1_compress.cpp:153-341): parameter
+ *                   validation (:49-99), data range (:101-140), plan preparation (:30-47) and
+ *                   param_c<float>::compress() (c_codes/asz_core/compress.tpp:147-321).
+ *   asz_decompress  replaces s1_decompress's main (c_codes/s1_decompress.cpp:5-149) and
+ *                   param_c<float>::decompress() (c_codes/asz_core/decompress.tpp:79-208).
+ *
+ * The .asz bytes are the reference's bitstream: the same header, t stream, Huffman trees and
+ * payloads, compressed by libzstd at level 3 on the host. For the same input, error bound, plan
+ * and parameters the output equals s1_compress's byte for byte when both link the same libzstd.
+ *
+ * Errors: every call returns 0 on success or a negative ASZ_E* code; asz_last_error(ctx) holds
+ * the message. The reference prints "error: <msg>" and exits 1 on the same conditions. Device
+ * faults are never raised on purpose: kernels bound every loop and report through an error word.
+ *
+ * Threading: a context owns one CUDA stream and its device buffers. Calls on one context must
+ * not overlap; separate contexts may be used from separate threads.
+ */
+#ifndef ASZ_B200_H
+#define ASZ_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASZ_OK 0
+#define ASZ_E_ARG -1      /* invalid argument (reference: std::invalid_argument) */
+#define ASZ_E_DATA -2     /* invalid input data or stream (reference: std::runtime_error) */
+#define ASZ_E_CUDA -3     /* CUDA runtime error */
+#define ASZ_E_DEVICE -4   /* a kernel reported an inconsistency through its error word */
+#define ASZ_E_UNSUPPORTED -5
+
+/* Predictor family: ASZ_FAMILY_AUTO runs the reference's selector (predictor_family.tpp). */
+#define ASZ_FAMILY_AUTO -1
+#define ASZ_FAMILY_CUBIC 0
+#define ASZ_FAMILY_QUINTIC 1
+
+/* Every tunable of s1_compress / s1_decompress (c_codes/s1_compress.cpp:163-333), with the
+ * defaults of asz::param_c (c_codes/asz_core/asz_param.hpp:147-180) from asz_default_params.
+ * The reference does not store block_pivot_ratio, eb_ratio, pivot_eb_ratio or t_precision in the
+ * .asz, so the decompressor must be given the values the compressor used. */
+typedef struct asz_params {
+    float pivot_eb_ratio;           /* --pivot-eb-ratio, default 0.05 */
+    float eb_ratio;                 /* --eb-ratio, default 0.76 */
+    float slope_ratio;              /* --slope-ratio, default 0.54 */
+    uint64_t block_pivot_ratio;     /* --block-pivot-ratio, default 4 */
+    uint64_t max_layer_num;         /* --max-layer-num, default 14 */
+    uint64_t full_predictor_search_layer_num; /* default 4 */
+    uint64_t generate_config_sample_stride;   /* default 5 */
+    uint64_t h1_block_sampling_num; /* default 256 */
+    float stat_eb_ratio;            /* default 0.2 */
+    uint64_t predictor_family_suffix_layers;  /* default 6 */
+    uint64_t predictor_family_sample_blocks;  /* default 8 */
+    uint64_t predictor_family_sample_point_limit; /* default 32768 */
+    float predictor_family_sample_fraction_limit; /* default 0.02 */
+    uint64_t predictor_family_coarse_probe_block_pivot_ratio; /* default 3 */
+    uint64_t predictor_family_fine_probe_block_pivot_ratio;   /* default 4 */
+    float predictor_family_fine_eb_threshold; /* default 1e-4 */
+    float default_slope_invalid_ratio_threshold; /* default 1 */
+    float default_slope_fallback;   /* default 1000 */
+    float default_slope_eb_span;    /* default 1.5 */
+    int32_t t_precision;            /* --t-precision, default 32 */
+    float t_min, t_max;             /* --t-min/--t-max, defaults 1/16 and 6/16 */
+    int32_t t_range_set;            /* nonzero when t_min/t_max were given (they come together) */
+    int32_t predictor_family;       /* ASZ_FAMILY_*, default AUTO */
+    int32_t report_t_histogram;     /* --report-t-histogram */
+} asz_params;
+
+/* Timings (seconds) and figures of one call, matching the reference's stdout lines. */
+typedef struct asz_report {
+    double data_range_s;      /* "Data range time" */
+    double default_slope_s;   /* "Get default slope time" */
+    double plan_s;            /* "Generate config time" (auto plans) */
+    double family_s;          /* "Predictor family selection time" */
+    double core_s;            /* "Core compression time" without zstd (GPU rounds + Huffman) */
+    double huffman_s;         /* "Huffman compression time" / "Huffman decompression time" */
+    double zstd_s;            /* "Zstd compression time" / "Zstd decompression time" */
+    double h2d_s, d2h_s;      /* host<->device copies inside the call */
+    double total_s;           /* wall time of the whole call */
+    float min_val, max_val, abs_eb, default_slope;
+    float max_err, psnr, cr, br;
+    uint64_t t_fallback_count;
+    uint64_t pre_zstd_len, asz_len;
+    uint64_t layer_num;
+    float slope_max_invalid_ratio; /* "Default slope statistics" line */
+    int32_t slope_fallback_reason; /* 0 none, 1 invalid_ratio, 2 invalid_difference */
+    uint64_t ambiguous_decisions; /* per-block t decisions re-checked on the host */
+    uint64_t reruns;              /* compressions repeated after a host re-check */
+    uint32_t pivot_stride[3], block_shape[3], block_num[3];
+    int32_t quintic;
+    char plan[64 * 11 + 1];       /* comma-separated predictor plan actually used */
+} asz_report;
+
+typedef struct asz_ctx asz_ctx;
+
+void asz_default_params(asz_params *p);
+
+/* Create a context bound to CUDA device `device`. Returns NULL on failure. */
+asz_ctx *asz_create(int device);
+void asz_destroy(asz_ctx *ctx);
+const char *asz_last_error(const asz_ctx *ctx);
+
+/* Run subsequent calls on the caller's stream (a cudaStream_t passed as a pointer); NULL
+ * restores the context's own stream. */
+int asz_set_stream(asz_ctx *ctx, void *cuda_stream);
+
+/* Compress a C-order float32 field (dims[2] fastest). `in` is a host pointer, or a device
+ * pointer when in_on_device is nonzero. `plan` is the reference's plan string
+ * ("cubic2_012,cubic1_120,..."); NULL asks for the reference's automatic plan search.
+ * On success *out receives a buffer of *out_len .asz bytes; release it with asz_free. */
+int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                 const asz_params *p, const char *plan, uint8_t **out, size_t *out_len, asz_report *rep);
+
+/* Decompress .asz bytes into `out` (prod(dims) floats; host pointer, or device pointer when
+ * out_on_device is nonzero). */
+int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const uint64_t dims[3], float rel_eb,
+                   const asz_params *p, float *out, int out_on_device, asz_report *rep);
+
+void asz_free(void *ptr);
+
+/* Error statistics of the last asz_compress call on this context, as the reference prints them
+ * after compressing (compress.tpp:307-319): max |x - x'| and PSNR in dB. The input buffer given
+ * to that call must still be valid (device input) or is the context's own copy (host input). */
+int asz_compress_stats(asz_ctx *ctx, double *max_err, double *psnr);
+
+/* Internals of the last asz_compress call on this context, for parity checks: QB stream k
+ * (0 = pivots, k = round k), per-(block, round) t codes, the in-place reconstruction and the
+ * stream before zstd. Each copies into caller memory and returns the element count; pass NULL to
+ * query the count. */
+uint64_t asz_debug_qb(asz_ctx *ctx, uint32_t stream, int32_t *dst);
+uint64_t asz_debug_t(asz_ctx *ctx, int64_t *dst);
+uint64_t asz_debug_recon(asz_ctx *ctx, float *dst);
+uint64_t asz_debug_pre_zstd(asz_ctx *ctx, uint8_t *dst);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,953 @@
+// CPU oracle: a restatement of the ASZ reference compression path, used only as a checker.
+//
+// TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+// load this library, and only to check or time against it. The product never links it.
+//
+// Scope: the plain path with a given plan and predictor family. That is the default-slope
+// proxy, the per-(block, round) coefficient choice, the 1D4R/1D6R rounds with in-place
+// reconstruction, the QB reorder, Huffman coding, stream assembly, zstd and decompression.
+//
+// Floating point. The reference is built with -Ofast -march=native -mavx2 -mfma
+// (c_codes/CMakeLists.txt:12). The operation order and FMA contraction below were read from
+// the code GCC 13.3 emits for the reference's sources, compiled here. Each fused step is an
+// explicit fma()/fmaf() and every other step is a single IEEE operation. This file is built
+// with -ffp-contract=off so the compiler adds nothing. Under -Ofast (-ffinite-math-only) GCC
+// drops the reference's `psnr==INFINITY` tests (compress.tpp:131,136;
+// get_default_slope.tpp:33), so they are absent here as well.
+//
+// Hash-table order. The proxies sum floats while iterating std::unordered_map, so their results
+// depend on libstdc++'s iteration order. The restatement uses the same containers with the same
+// hash (asz_param.hpp:22-40), key types and insertion sequence, so its order is the reference's.
+#include "asz_oracle.h"
+#include "zstd_decls.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <immintrin.h>
+#include <limits>
+#include <map>
+#include <queue>
+#include <stack>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+using std::vector;
+using u64 = uint64_t;
+using i64 = int64_t;
+using qb_t = int32_t;
+
+// asz_param.hpp:22-40: h = a*1145141919810 + b in wrapping 64-bit arithmetic.
+struct ab_hash {
+    size_t operator()(const std::tuple<i64, i64> &t) const {
+        u64 h = (u64)std::get<0>(t);
+        h = h * 1145141919810ull + (u64)std::get<1>(t);
+        return (size_t)h;
+    }
+};
+using ab_map = std::unordered_map<std::tuple<i64, i64>, u64, ab_hash>;
+
+// llround of a float as GCC expands it under -Ofast: trunc(x + copysign(0.49999997f, x)).
+static inline i64 lround_f(float x) {
+    float h = std::copysign(0x1.fffffep-2f, x);
+    float s = x + h;
+    return (i64)s;
+}
+// Same for double: trunc(x + copysign(0.49999999999999994, x)).
+static inline i64 lround_d(double x) {
+    double h = std::copysign(0x1.fffffffffffffp-2, x);
+    double s = x + h;
+    return (i64)s;
+}
+
+// Quintic 1D6R weights (asz_param.hpp:72-74).
+constexpr double QA = 3.0 / 256, QB = -25.0 / 256, QI = 0.5 - QA - QB;
+
+struct field {
+    u64 n[3];
+    u64 size() const { return n[0] * n[1] * n[2]; }
+    u64 pos(u64 i0, u64 i1, u64 i2) const { return i0 * n[1] * n[2] + i1 * n[2] + i2; }
+};
+
+// get_AB_map.tpp:7-24 (sample set and key quantisation).
+template <class LOC, class STR>
+void get_ab_map(ab_map &m, const float *d, const field &f, const LOC &loc, const STR &stride, u64 dist,
+                float neg_2_stat_eb, u64 h1num) {
+    u64 vol = (loc[0][1] - loc[0][0]) * (loc[1][1] - loc[1][0]) * (loc[2][1] - loc[2][0]);
+    float q = (float)vol / (float)(stride[0] * stride[1] * stride[2] * h1num);
+    u64 ss = (u64)std::cbrt((double)q);
+    if (ss == 0) ss = 1;
+    for (u64 i0 = loc[0][0]; i0 < loc[0][1]; i0 += stride[0] * ss)
+        for (u64 i1 = loc[1][0]; i1 < loc[1][1]; i1 += stride[1] * ss)
+            for (u64 i2 = loc[2][0]; i2 < loc[2][1]; i2 += stride[2] * ss) {
+                u64 p = f.pos(i0, i1, i2);
+                float m1 = d[p - dist], m3 = d[p - 3 * dist], p1 = d[p + dist], p3 = d[p + 3 * dist];
+                float A = (m1 + p1) - (m3 + p3);
+                float S4 = (p1 + p3) + (m1 + m3);
+                float B = (float)std::fma((double)S4, 0.25, -(double)d[p]);
+                i64 ak = lround_f(A * neg_2_stat_eb);
+                i64 bk = lround_f(B * neg_2_stat_eb);
+                m[{ak, bk}]++;
+            }
+}
+
+// get_h_psnr.tpp:6-31. Returns also the log10f argument and the float sum for callers
+// that need them.
+void get_h1_psnr(float &h1, float &psnr, const ab_map &m, float t, float abs_eb, float stat_eb,
+                 float min_val, float max_val, float *x_out = nullptr, float *mse_out = nullptr) {
+    float neg_2_eb = 0.5f / abs_eb;
+    float t2 = t + t, eb2 = abs_eb + abs_eb;
+    std::unordered_map<i64, u64> qb_map;
+    float mse = 0;
+    u64 n = 0;
+    for (const auto &[key, cnt] : m) {
+        float af = (float)std::get<0>(key), bf = (float)std::get<1>(key);
+        float err = std::fmaf(bf, 2.0f, af * t2) * stat_eb;
+        i64 qb = lround_f(err * neg_2_eb);
+        qb_map[qb] += cnt;
+        float de = std::fmaf(-(float)qb, eb2, err);
+        mse = (float)std::fma((double)cnt, (double)de * (double)de, (double)mse);
+        n += cnt;
+    }
+    float nf = (float)n;
+    h1 = 0;
+    if (!qb_map.empty()) {
+        float r = 1.0f / nf;
+        for (const auto &[qb, freq] : qb_map) {
+            float p = (float)freq * r;
+            float L = log2f(p);
+            h1 = std::fmaf(-p, L, h1);
+        }
+    }
+    float R = max_val - min_val;
+    float x = (R * R / mse) * nf;
+    psnr = 10.0f * log10f(x);
+    if (x_out) *x_out = x;
+    if (mse_out) *mse_out = mse;
+}
+
+struct params_t {
+    aszo_params p;
+    vector<float> candidate_t, block_candidate_t;
+    void init(const aszo_params &pp) {
+        p = pp;
+        candidate_t.clear();
+        int lo = (int)llround(p.t_min * p.t_precision), hi = (int)llround(p.t_max * p.t_precision);
+        for (int ti = lo; ti <= hi; ti++) candidate_t.push_back((float)ti / p.t_precision);
+        block_candidate_t = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+    }
+};
+
+// get_default_slope.tpp:6-83.
+float default_slope(const float *data, const field &f, float abs_eb, float min_val, float max_val,
+                    const params_t &P) {
+    const aszo_params &p = P.p;
+    float ebs[2] = {abs_eb * p.default_slope_eb_span, abs_eb / p.default_slope_eb_span};
+    float two_stat = abs_eb * p.stat_eb_ratio;
+    float stat_eb = two_stat * 0.5f;
+    float neg_2_stat_eb = 1.0f / two_stat;
+    float avg_h1[2] = {0, 0}, avg_psnr[2] = {0, 0};
+    u64 valid[2] = {0, 0};
+    for (int dir = 0; dir < 3; dir++) {
+        std::array<std::array<u64, 2>, 3> loc = {{{0, f.n[0]}, {0, f.n[1]}, {0, f.n[2]}}};
+        loc[dir] = {3, f.n[dir] - 3};
+        std::array<u64, 3> stride = {1, 1, 1};
+        stride[dir] = 2;
+        u64 dist = 1;
+        for (int a = dir + 1; a < 3; a++) dist *= f.n[a];
+        ab_map m;
+        get_ab_map(m, data, f, loc, stride, dist, neg_2_stat_eb, p.h1_block_sampling_num);
+        if (m.empty()) throw std::runtime_error("default slope: empty AB map");
+        for (int i = 0; i < 2; i++)
+            for (float t : P.candidate_t) {
+                float h1, psnr;
+                get_h1_psnr(h1, psnr, m, t, ebs[i], stat_eb, min_val, max_val);
+                avg_h1[i] += h1;
+                avg_psnr[i] += psnr;
+                valid[i]++;
+            }
+    }
+    u64 total = 3 * P.candidate_t.size();
+    float recip = 1.0f / (float)total;
+    float max_invalid = 0;
+    for (int i = 0; i < 2; i++) {
+        float inv = std::fmaf(-recip, (float)valid[i], 1.0f);
+        max_invalid = std::max(inv, max_invalid);
+    }
+    if (max_invalid >= p.default_slope_invalid_ratio_threshold) return p.default_slope_fallback;
+    // The tolerance scale uses the vectorised approximate reciprocal plus one Newton step that
+    // GCC emits for average_h1[i]/=valid_case_num[i]; the differences use exact divisions.
+    __m128 v = _mm_set_ps(1.0f, 1.0f, (float)valid[1], (float)valid[0]);
+    __m128 r0 = _mm_rcp_ps(v);
+    __m128 r1 = _mm_sub_ps(_mm_add_ps(r0, r0), _mm_mul_ps(r0, _mm_mul_ps(r0, v)));
+    alignas(16) float rr[4];
+    _mm_store_ps(rr, r1);
+    float h1v0 = avg_h1[0] * rr[0], h1v1 = avg_h1[1] * rr[1];
+    float h1_0 = avg_h1[0] / (float)valid[0], h1_1 = avg_h1[1] / (float)valid[1];
+    float ps_0 = avg_psnr[0] / (float)valid[0], ps_1 = avg_psnr[1] / (float)valid[1];
+    float h1_diff = h1_1 - h1_0, psnr_diff = ps_1 - ps_0;
+    float scale = std::max(std::fabs(h1v1), std::fabs(h1v0));
+    float tol = scale > 1.0f ? scale * 0x1p-17f : 0x1p-17f;
+    // Ordered compares, as emitted: a NaN difference does not select the fallback.
+    if (tol >= h1_diff || 0.0f >= psnr_diff) return p.default_slope_fallback;
+    return psnr_diff / h1_diff;
+}
+
+struct codec {
+    field f;
+    params_t P;
+    bool quintic = false;
+    vector<std::string> plan;
+    std::array<u64, 3> pivot_stride{}, block_shape{}, block_num{};
+    float min_val = 0, max_val = 0, abs_eb = 0, default_slope_v = 0;
+    const float *data = nullptr;
+    vector<float> cd;  // compressed_data (in-place reconstruction)
+    vector<vector<qb_t>> qbs;
+    vector<i64> t_int;
+    u64 t_fallback = 0;
+
+    void geometry() {  // generate_config.tpp:52-68
+        pivot_stride = {1, 1, 1};
+        for (auto &pr : plan) pivot_stride[pr[5] - '0'] *= 2;
+        for (int a = 0; a < 3; a++) {
+            block_shape[a] = pivot_stride[a] * P.p.block_pivot_ratio;
+            block_num[a] = (f.n[a] + block_shape[a] - 1) / block_shape[a];
+        }
+    }
+
+    // compress.tpp:91-144.
+    float select_t(int dir, const std::array<std::array<u64, 2>, 3> &loc, const std::array<u64, 3> &stride,
+                   float layer_eb, float slope, bool &fb) {
+        fb = false;
+        float best_t = P.p.insufficient_sample_t;
+        if (loc[dir][1] <= loc[dir][0] + 3 * stride[dir]) {
+            fb = true;
+            return best_t;
+        }
+        std::array<std::array<u64, 2>, 3> sl;
+        for (int a = 0; a < 3; a++) {
+            sl[a] = {loc[a][0], loc[a][1]};
+            if (a != dir && loc[a][0] != 0) sl[a][0] += stride[a];
+        }
+        sl[dir][0] += 3 * stride[dir] / 2;
+        sl[dir][1] -= 3 * stride[dir] / 2;
+        u64 sdist = stride[dir] / 2;
+        for (int a = dir + 1; a < 3; a++) sdist *= f.n[a];
+        float stat_eb = layer_eb * P.p.stat_eb_ratio;
+        ab_map m;
+        get_ab_map(m, cd.data(), f, sl, stride, sdist, 0.5f / stat_eb, P.p.h1_block_sampling_num);
+        if (m.empty()) {
+            fb = true;
+            return best_t;
+        }
+        float best_h1, best_psnr;
+        get_h1_psnr(best_h1, best_psnr, m, best_t, layer_eb, stat_eb, min_val, max_val);
+        for (float c : P.block_candidate_t) {
+            if (c == best_t) continue;
+            float h1, psnr;
+            get_h1_psnr(h1, psnr, m, c, layer_eb, stat_eb, min_val, max_val);
+            float s = std::fmaf(best_h1 - h1, slope, psnr - best_psnr);
+            if (s > 0) {
+                best_t = c;
+                best_h1 = h1;
+                best_psnr = psnr;
+            }
+        }
+        return best_t;
+    }
+
+    // compress.tpp:7-40 (prediction), and decompress.tpp:6-35 for the same stencils.
+    inline float predict(u64 i, u64 hs, u64 right, u64 pos, u64 dist, float t) const {
+        const float *c = cd.data();
+        if (quintic && i >= 5 * hs && i + 5 * hs < right) {
+            float s1 = c[pos - dist] + c[pos + dist];
+            float s3 = c[pos - 3 * dist] + c[pos + 3 * dist];
+            float s5 = c[pos - 5 * dist] + c[pos + 5 * dist];
+            double acc = (double)s3 * QB;
+            acc = std::fma((double)s1, QI, acc);
+            acc = std::fma((double)s5, QA, acc);
+            return (float)acc;
+        }
+        if (i <= hs) {
+            if (i + hs >= right) return c[pos - dist];
+            if (i + 3 * hs >= right) return (c[pos - dist] + c[pos + dist]) * 0.5f;
+            return (std::fmaf(c[pos - dist], 3.0f, c[pos + dist] * 6.0f) - c[pos + 3 * dist]) * 0.125f;
+        }
+        if (i + hs >= right) return std::fmaf(c[pos - dist], 3.0f, -c[pos - 3 * dist]) * 0.5f;
+        if (i + 3 * hs >= right)
+            return std::fmaf(c[pos + dist], 3.0f, std::fmaf(c[pos - dist], 6.0f, -c[pos - 3 * dist])) * 0.125f;
+        float s3 = c[pos - 3 * dist] + c[pos + 3 * dist];
+        float s1 = c[pos - dist] + c[pos + dist];
+        double td = t;
+        float p1 = (float)((double)s3 * (0.25 - td));
+        return (float)std::fma(0.25 + td, (double)s1, (double)p1);
+    }
+
+    // Target lattice and QB placement of one (block, round): compress.tpp:53-88.
+    template <class FN>
+    void for_targets(const std::array<std::array<u64, 2>, 3> &loc, const std::array<u64, 3> &stride, int dir,
+                     int order, u64 &qb_base, FN fn) {
+        std::array<u64, 3> left, shape;
+        for (int a = 0; a < 3; a++) {
+            left[a] = a == dir ? loc[a][0] + stride[a] / 2 : (loc[a][0] == 0 ? 0 : loc[a][0] + stride[a]);
+            shape[a] = left[a] >= loc[a][1] ? 0 : (loc[a][1] - left[a] + stride[a] - 1) / stride[a];
+        }
+        u64 inner = order == 0 ? shape[0] : order == 1 ? shape[1] : 1;
+        u64 dist = stride[dir] / 2;
+        for (int a = dir + 1; a < 3; a++) dist *= f.n[a];
+        u64 j0 = 0;
+        for (u64 i0 = left[0]; i0 < loc[0][1]; i0 += stride[0], j0++) {
+            u64 j1 = 0;
+            for (u64 i1 = left[1]; i1 < loc[1][1]; i1 += stride[1], j1++) {
+                u64 qi;
+                if (order == 0) qi = (j1 * shape[2] + 0) * shape[0] + j0;
+                else if (order == 1) qi = (j0 * shape[2] + 0) * shape[1] + j1;
+                else qi = (j0 * shape[1] + j1) * shape[2] + 0;
+                qi += qb_base;
+                for (u64 i2 = left[2]; i2 < loc[2][1]; i2 += stride[2], qi += inner) {
+                    u64 i = dir == 0 ? i0 : dir == 1 ? i1 : i2;
+                    fn(i, stride[dir] / 2, loc[dir][1], f.pos(i0, i1, i2), dist, qi);
+                }
+            }
+        }
+        qb_base += shape[0] * shape[1] * shape[2];
+    }
+
+    u64 layer_qb_count(const std::array<std::array<u64, 2>, 3> &loc, const std::array<u64, 3> &stride, int dir) {
+        u64 c = 1;
+        for (int a = 0; a < 3; a++) {
+            u64 left = a == dir ? loc[a][0] + stride[a] / 2 : (loc[a][0] == 0 ? 0 : loc[a][0] + stride[a]);
+            c *= left >= loc[a][1] ? 0 : (loc[a][1] - left + stride[a] - 1) / stride[a];
+        }
+        return c;
+    }
+
+    std::array<std::array<u64, 2>, 3> block_loc(u64 b0, u64 b1, u64 b2) const {
+        u64 b[3] = {b0, b1, b2};
+        std::array<std::array<u64, 2>, 3> loc;
+        for (int a = 0; a < 3; a++) loc[a] = {b[a] * block_shape[a], std::min((b[a] + 1) * block_shape[a] + 1, f.n[a])};
+        return loc;
+    }
+
+    float layer_eb(u64 L, u64 l) const {
+        return (float)((double)abs_eb * std::pow((double)P.p.eb_ratio, (double)(L - l - 1)));
+    }
+
+    // compress.tpp:147-231 (prediction part).
+    void compress_core() {
+        u64 N = f.size();
+        cd.assign(data, data + N);
+        u64 L = plan.size();
+        qbs.assign(L + 1, {});
+        t_int.clear();
+        t_fallback = 0;
+        // Pivots (compress.tpp:162-175): hoisted reciprocal 0.5/pivot_eb in double.
+        float pivot_eb = abs_eb * P.p.pivot_eb_ratio;
+        double peb = pivot_eb, rp = 0.5 / peb, peb2 = peb + peb;
+        for (u64 i0 = 0; i0 < f.n[0]; i0 += pivot_stride[0])
+            for (u64 i1 = 0; i1 < f.n[1]; i1 += pivot_stride[1])
+                for (u64 i2 = 0; i2 < f.n[2]; i2 += pivot_stride[2]) {
+                    u64 pos = f.pos(i0, i1, i2);
+                    qb_t qb = (qb_t)lround_d((double)data[pos] * rp);
+                    qbs[0].push_back(qb);
+                    cd[pos] = (float)((double)qb * peb2);
+                }
+        for (u64 l = 0; l < L; l++) {
+            u64 cnt = 0;
+            for (u64 b0 = 0; b0 < block_num[0]; b0++)
+                for (u64 b1 = 0; b1 < block_num[1]; b1++)
+                    for (u64 b2 = 0; b2 < block_num[2]; b2++) {
+                        std::array<u64, 3> stride = pivot_stride;
+                        for (u64 k = 0; k < l; k++) stride[plan[k][5] - '0'] /= 2;
+                        cnt += layer_qb_count(block_loc(b0, b1, b2), stride, plan[l][5] - '0');
+                    }
+            qbs[l + 1].assign(cnt, 0);
+        }
+        vector<u64> qb_base(L + 1, 0);
+        for (u64 b0 = 0; b0 < block_num[0]; b0++)
+            for (u64 b1 = 0; b1 < block_num[1]; b1++)
+                for (u64 b2 = 0; b2 < block_num[2]; b2++) {
+                    auto loc = block_loc(b0, b1, b2);
+                    std::array<u64, 3> stride = pivot_stride;
+                    for (u64 l = 0; l < L; l++) {
+                        int dir = plan[l][5] - '0', order = plan[l][9] - '0';
+                        float leb = layer_eb(L, l);
+                        float slope =
+                            (float)((double)default_slope_v * std::pow((double)P.p.slope_ratio, (double)((int)L - (int)l - 1)));
+                        bool fb = false;
+                        float t = select_t(dir, loc, stride, leb, slope, fb);
+                        if (fb) t_fallback++;
+                        t_int.push_back(lround_f(t * (float)P.p.t_precision));
+                        // Quantisation: direction 0 multiplies by a hoisted 0.5*(1/eb); directions 1
+                        // and 2 divide (compress.tpp:35 as emitted for block_compress_impl<false>).
+                        double ebd = leb, eb2 = ebd + ebd, r0 = (1.0 / ebd) * 0.5;
+                        vector<qb_t> &out = qbs[l + 1];
+                        for_targets(loc, stride, dir, order, qb_base[l + 1],
+                                    [&](u64 i, u64 hs, u64 right, u64 pos, u64 dist, u64 qi) {
+                                        float pred = predict(i, hs, right, pos, dist, t);
+                                        double pd = pred, diff = pd - (double)data[pos];
+                                        double q = dir == 0 ? diff * r0 : (diff * 0.5) / ebd;
+                                        qb_t qb = (qb_t)lround_d(q);
+                                        out[qi] = qb;
+                                        cd[pos] = (float)std::fma(-(double)qb, eb2, pd);
+                                    });
+                        stride[dir] /= 2;
+                    }
+                }
+    }
+
+    // decompress.tpp:79-196 (after the entropy stage).
+    void decompress_core(float *out) {
+        u64 N = f.size();
+        cd.assign(N, 0.0f);
+        u64 L = plan.size();
+        float pivot_eb = abs_eb * P.p.pivot_eb_ratio;
+        double peb2 = (double)pivot_eb + (double)pivot_eb;
+        u64 k = 0;
+        for (u64 i0 = 0; i0 < f.n[0]; i0 += pivot_stride[0])
+            for (u64 i1 = 0; i1 < f.n[1]; i1 += pivot_stride[1])
+                for (u64 i2 = 0; i2 < f.n[2]; i2 += pivot_stride[2]) {
+                    if (k >= qbs[0].size()) throw std::runtime_error("compressed stream has too few QBs");
+                    cd[f.pos(i0, i1, i2)] = (float)((double)qbs[0][k++] * peb2);
+                }
+        vector<float> lebs(L);
+        for (u64 l = 0; l < L; l++) lebs[l] = layer_eb(L, l);
+        vector<u64> qb_pos(L + 1, 0);
+        u64 tp = 0;
+        for (u64 b0 = 0; b0 < block_num[0]; b0++)
+            for (u64 b1 = 0; b1 < block_num[1]; b1++)
+                for (u64 b2 = 0; b2 < block_num[2]; b2++) {
+                    auto loc = block_loc(b0, b1, b2);
+                    std::array<u64, 3> stride = pivot_stride;
+                    for (u64 l = 0; l < L; l++) {
+                        if (tp >= t_int.size()) throw std::runtime_error("compressed stream contains too few t values");
+                        float t = (float)t_int[tp++] / (float)P.p.t_precision;
+                        int dir = plan[l][5] - '0', order = plan[l][9] - '0';
+                        double ebd = lebs[l], eb2 = ebd + ebd;
+                        const vector<qb_t> &in = qbs[l + 1];
+                        u64 need = layer_qb_count(loc, stride, dir);
+                        if (qb_pos[l + 1] > in.size() || need > in.size() - qb_pos[l + 1])
+                            throw std::runtime_error("compressed stream has too few QBs");
+                        for_targets(loc, stride, dir, order, qb_pos[l + 1],
+                                    [&](u64 i, u64 hs, u64 right, u64 pos, u64 dist, u64 qi) {
+                                        float pred = predict(i, hs, right, pos, dist, t);
+                                        cd[pos] = (float)std::fma(-(double)in[qi], eb2, (double)pred);
+                                    });
+                        stride[dir] /= 2;
+                    }
+                }
+        std::memcpy(out, cd.data(), N * sizeof(float));
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Huffman coder: huffman.hpp:17-784, restated with the same tree construction, tie-breaking,
+// code assignment, DFS serialisation and LSB-first packing.
+template <class T>
+struct huff {
+    struct node {
+        u64 c = 0;
+        int l = -1, r = -1;
+    };
+    vector<node> ht;
+    bool usemp = false;
+    T offset = 0;
+    u64 maxval = 0, n = 0;
+    unsigned mbft = 0;
+    u64 root = 0;
+    std::unordered_map<u64, std::pair<unsigned, u64>> code;  // symbol-offset -> (len, code)
+    vector<u64> freq_of;                                     // per leaf index
+    u64 bits = 0;
+
+    static void put_be64(uint8_t *b, u64 v) {
+        for (int i = 0; i < 8; i++) b[i] = (uint8_t)(v >> (56 - 8 * i));
+    }
+
+    void build(const T *s, u64 num) {
+        T mn = s[0], mx = s[0];
+        for (u64 i = 1; i < num; i++) {
+            mn = std::min(mn, s[i]);
+            mx = std::max(mx, s[i]);
+        }
+        offset = mn;
+        maxval = (u64)(T)(mx - mn + 1);
+        usemp = ((T)maxval >= (1 << 12) && num < 2 * (u64)mx) || (T)maxval >= (1 << 28);
+        std::map<u64, u64> freq;
+        for (u64 i = 0; i < num; i++) ++freq[(u64)(s[i] - offset)];
+        ht.clear();
+        freq_of.clear();
+        for (auto &kv : freq) {
+            node nd;
+            nd.c = kv.first;
+            ht.push_back(nd);
+            freq_of.push_back(kv.second);
+        }
+        n = ht.size();
+        code.clear();
+        bits = 0;
+        if (n == 1 || maxval == 1) {  // huffman.hpp:193-210
+            mbft = 1;
+            maxval = 1;
+            offset = (T)(offset + (T)ht[0].c);
+            ht[0].c = 0;
+            code[0] = {1, 0};
+            return;
+        }
+        mbft = 1;
+        while ((1ull << mbft) < maxval) ++mbft;
+        using pr = std::pair<u64, u64>;  // (node index, freq); min freq first, then min index
+        auto cmp = [](const pr &u, const pr &v) { return u.second == v.second ? u.first > v.first : u.second > v.second; };
+        std::priority_queue<pr, vector<pr>, decltype(cmp)> q(cmp);
+        for (u64 i = 0; i < ht.size(); i++) q.push({i, freq_of[i]});
+        while (q.size() > 1) {
+            pr u = q.top();
+            q.pop();
+            pr v = q.top();
+            q.pop();
+            node nd;
+            nd.l = (int)u.first;
+            nd.r = (int)v.first;
+            ht.push_back(nd);
+            q.push({ht.size() - 1, u.second + v.second});
+        }
+        root = ht.size() - 1;
+        dfs(root, 0, 0);
+        for (u64 i = 0; i < n; i++) bits += freq_of[i] * code[ht[i].c].first;
+    }
+    void dfs(u64 u, unsigned len, u64 vec) {
+        if (ht[u].l < 0) {
+            if (len > 32) throw std::runtime_error("Huffman code longer than 32 bits");
+            code[ht[u].c] = {len, vec};
+            return;
+        }
+        dfs(ht[u].l, len + 1, vec);
+        dfs(ht[u].r, len + 1, vec | (1ull << len));
+    }
+    u64 save_size() const {
+        u64 s = 1 + 8 + 8 + 8;
+        if (n > 1) s += (n * (mbft + 2) - 1 + 7) >> 3;
+        return s;
+    }
+    u64 encode_size() const { return 8 + (maxval == 1 ? 0 : (bits + 7) >> 3); }
+
+    struct bitw {
+        uint8_t *p;
+        unsigned mask = 0, idx = 0;
+        void bit(unsigned v) {
+            mask |= v << idx++;
+            if (idx == 8) {
+                *p++ = (uint8_t)mask;
+                mask = idx = 0;
+            }
+        }
+        void bits(u64 v, unsigned len) {
+            for (unsigned k = 0; k < len; k++) bit((v >> k) & 1);
+        }
+        void flush() {
+            if (idx > 0) *p++ = (uint8_t)mask;
+        }
+    };
+
+    uint8_t *save(uint8_t *c) const {  // huffman.hpp:650-691
+        *c++ = (uint8_t)((usemp << 7) | ((n == 1) << 6) | mbft);
+        u64 ob = (u64)(i64)offset;
+        for (int i = 0; i < 8; i++) *c++ = (uint8_t)(ob >> (8 * i));
+        put_be64(c, n);
+        c += 8;
+        put_be64(c, maxval);
+        c += 8;
+        if (n <= 1) return c;
+        bitw w{c};
+        std::stack<u64> st;
+        st.push(root);
+        while (!st.empty()) {
+            u64 u = st.top();
+            st.pop();
+            if (ht[u].l < 0) {
+                w.bit(1);
+                w.bits(ht[u].c, mbft);
+            } else {
+                w.bit(0);
+                st.push((u64)ht[u].r);
+                st.push((u64)ht[u].l);
+            }
+        }
+        w.flush();
+        return w.p;
+    }
+    uint8_t *encode(const T *s, u64 num, uint8_t *c) const {  // huffman.hpp:340-381
+        if (maxval == 1) {
+            put_be64(c, num ^ 0x1234abcd);
+            return c + 8;
+        }
+        uint8_t *head = c;
+        bitw w{c + 8};
+        u64 len = 0;
+        for (u64 i = 0; i < num; i++) {
+            auto &e = code.at((u64)(s[i] - offset));
+            len += e.first;
+            w.bits(e.second, e.first);
+        }
+        w.flush();
+        put_be64(head, len ^ 0x1234abcd);
+        return w.p;
+    }
+};
+
+// Huffman decoder: huffman.hpp:383-526 and 693-783. A plain tree walk (same output).
+template <class T>
+struct hdec {
+    struct node {
+        int l = -1, r = -1;
+        u64 c = 0;
+    };
+    vector<node> ht;
+    T offset = 0;
+    u64 n = 0, maxval = 0;
+    unsigned mbft = 0;
+    static u64 be64(const uint8_t *b) {
+        u64 v = 0;
+        for (int i = 0; i < 8; i++) v = (v << 8) | b[i];
+        return v;
+    }
+    const uint8_t *load(const uint8_t *b, const uint8_t *end) {
+        if (end - b < 25) throw std::runtime_error("truncated Huffman header");
+        mbft = b[0] & 0x3f;
+        b++;
+        u64 ob = 0;
+        for (int i = 0; i < 8; i++) ob |= (u64)b[i] << (8 * i);
+        b += 8;
+        offset = (T)(i64)ob;
+        n = be64(b);
+        b += 8;
+        maxval = be64(b);
+        b += 8;
+        ht.clear();
+        if (n <= 1) return b;
+        ht.push_back(node());
+        vector<int> st{0};
+        u64 i = 1;
+        auto rd = [&](u64 k) -> unsigned {
+            if ((k >> 3) >= (u64)(end - b)) throw std::runtime_error("truncated Huffman tree");
+            return (b[k >> 3] >> (k & 7)) & 1;
+        };
+        while (!st.empty()) {
+            int u = st.back();
+            if (rd(i++) == 0) {
+                ht.push_back(node());
+                int id = (int)ht.size() - 1;
+                if (ht[u].l < 0) ht[u].l = id;
+                else ht[u].r = id;
+                st.push_back(id);
+            } else {
+                u64 c = 0;
+                for (unsigned j = 0; j < mbft; j++) c |= (u64)rd(i++) << j;
+                node nd;
+                nd.c = c;
+                ht.push_back(nd);
+                int id = (int)ht.size() - 1;
+                if (ht[u].l < 0) ht[u].l = id;
+                else ht[u].r = id;
+                while (!st.empty() && ht[st.back()].r >= 0) st.pop_back();
+            }
+            if (ht.size() > 2 * n + 2) throw std::runtime_error("corrupt Huffman tree");
+        }
+        return b + ((i + 7) >> 3);
+    }
+    const uint8_t *decode(const uint8_t *b, const uint8_t *end, T *out, u64 count) {
+        if (end - b < 8) throw std::runtime_error("truncated Huffman payload");
+        if (maxval == 1 || n <= 1) {
+            u64 c = be64(b) ^ 0x1234abcd;
+            if (count && c != count) throw std::runtime_error("Huffman payload length does not match its value count");
+            for (u64 i = 0; i < count; i++) out[i] = offset;
+            return b + 8;
+        }
+        u64 len = be64(b) ^ 0x1234abcd;
+        b += 8;
+        if (((len + 7) >> 3) > (u64)(end - b)) throw std::runtime_error("truncated Huffman payload");
+        u64 o = 0;
+        int u = 0;
+        for (u64 k = 0; k < len; k++) {
+            unsigned bit = (b[k >> 3] >> (k & 7)) & 1;
+            u = bit ? ht[u].r : ht[u].l;
+            if (u < 0) throw std::runtime_error("corrupt Huffman payload");
+            if (ht[u].l < 0) {
+                if (o >= count) throw std::runtime_error("Huffman payload contains too many values");
+                out[o++] = (T)(ht[u].c + offset);
+                u = 0;
+            }
+        }
+        if (u != 0) throw std::runtime_error("Huffman payload ends inside a code");
+        if (o != count) throw std::runtime_error("Huffman payload contains too few values");
+        return b + ((len + 7) >> 3);
+    }
+};
+
+template <class T>
+void append_stream(vector<uint8_t> &bs, const vector<T> &v) {
+    u64 len = v.size();
+    for (int i = 0; i < 8; i++) bs.push_back((uint8_t)(len >> (8 * i)));
+    if (v.empty()) return;
+    huff<T> h;
+    h.build(v.data(), v.size());
+    u64 sz = h.save_size() + h.encode_size();
+    size_t off = bs.size();
+    bs.resize(off + sz);
+    uint8_t *p = h.save(bs.data() + off);
+    p = h.encode(v.data(), v.size(), p);
+    if (p != bs.data() + bs.size()) throw std::runtime_error("Huffman encoded size mismatch");
+}
+
+vector<std::string> parse_plan(const char *s) {
+    vector<std::string> out;
+    std::string t(s ? s : "");
+    size_t b = 0;
+    while (b <= t.size()) {
+        size_t e = t.find(',', b);
+        std::string pr = t.substr(b, e == std::string::npos ? std::string::npos : e - b);
+        bool ok = pr.size() == 10 && pr.compare(0, 5, "cubic") == 0 && pr[5] >= '0' && pr[5] <= '2' && pr[6] == '_' &&
+                  (pr.compare(7, 3, "120") == 0 || pr.compare(7, 3, "021") == 0 || pr.compare(7, 3, "012") == 0);
+        if (!ok) throw std::invalid_argument("invalid predictor in plan: " + pr);
+        out.push_back(pr);
+        if (e == std::string::npos) break;
+        b = e + 1;
+    }
+    return out;
+}
+
+void set_err(char *err, const char *m) {
+    if (err) snprintf(err, 256, "%s", m);
+}
+
+}  // namespace
+
+extern "C" {
+
+void aszo_default_params(aszo_params *p) {
+    p->pivot_eb_ratio = 0.05f;
+    p->eb_ratio = 0.76f;
+    p->slope_ratio = 0.54f;
+    p->block_pivot_ratio = 4;
+    p->t_precision = 32;
+    p->t_min = 1.0f / 16;
+    p->t_max = 6.0f / 16;
+    p->h1_block_sampling_num = 256;
+    p->stat_eb_ratio = 0.2f;
+    p->default_slope_invalid_ratio_threshold = 1;
+    p->default_slope_fallback = 1000;
+    p->default_slope_eb_span = 1.5f;
+    p->insufficient_sample_t = 4.0f / 16;
+}
+
+int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
+                  int quintic, aszo_result *out, char *err) {
+    try {
+        std::memset(out, 0, sizeof(*out));
+        codec C;
+        C.f = {{dims[0], dims[1], dims[2]}};
+        C.P.init(*p);
+        C.quintic = quintic != 0;
+        C.plan = parse_plan(plan);
+        if (C.plan.size() > 63) throw std::invalid_argument("predictor plan cannot contain more than 63 layers");
+        C.data = data;
+        u64 N = C.f.size();
+        auto mm = std::minmax_element(data, data + N);
+        C.min_val = *mm.first;
+        C.max_val = *mm.second;
+        if (C.min_val == C.max_val) throw std::runtime_error("max_val==min_val");
+        C.abs_eb = rel_eb * (C.max_val - C.min_val);
+        C.default_slope_v = default_slope(data, C.f, C.abs_eb, C.min_val, C.max_val, C.P);
+        C.geometry();
+        C.compress_core();
+        // Stream assembly: compress.tpp:233-291.
+        vector<uint8_t> bs;
+        uint8_t hdr[9];
+        std::memcpy(hdr, &C.min_val, 4);
+        std::memcpy(hdr + 4, &C.max_val, 4);
+        hdr[8] = (uint8_t)(C.plan.size() | 0x40 | (C.quintic ? 0x80 : 0));
+        bs.insert(bs.end(), hdr, hdr + 9);
+        for (auto &pr : C.plan) {
+            bs.push_back((uint8_t)pr[5]);
+            bs.push_back((uint8_t)pr[9]);
+        }
+        append_stream<int64_t>(bs, C.t_int);
+        for (auto &v : C.qbs) append_stream<int32_t>(bs, v);
+        size_t bound = ZSTD_compressBound(bs.size());
+        vector<uint8_t> z(bound);
+        size_t zl = ZSTD_compress(z.data(), bound, bs.data(), bs.size(), 3);
+        if (ZSTD_isError(zl)) throw std::runtime_error(ZSTD_getErrorName(zl));
+        z.resize(zl);
+        // Outputs.
+        out->layer_num = (uint32_t)C.plan.size();
+        out->qb_len = (uint64_t *)malloc(sizeof(uint64_t) * C.qbs.size());
+        out->qb = (int32_t **)malloc(sizeof(int32_t *) * C.qbs.size());
+        for (size_t i = 0; i < C.qbs.size(); i++) {
+            out->qb_len[i] = C.qbs[i].size();
+            out->qb[i] = (int32_t *)malloc(sizeof(int32_t) * std::max<size_t>(1, C.qbs[i].size()));
+            std::memcpy(out->qb[i], C.qbs[i].data(), sizeof(int32_t) * C.qbs[i].size());
+        }
+        out->t_len = C.t_int.size();
+        out->t_int = (int64_t *)malloc(sizeof(int64_t) * std::max<size_t>(1, C.t_int.size()));
+        std::memcpy(out->t_int, C.t_int.data(), sizeof(int64_t) * C.t_int.size());
+        out->recon = (float *)malloc(sizeof(float) * N);
+        std::memcpy(out->recon, C.cd.data(), sizeof(float) * N);
+        out->pre_zstd_len = bs.size();
+        out->pre_zstd = (uint8_t *)malloc(bs.size());
+        std::memcpy(out->pre_zstd, bs.data(), bs.size());
+        out->asz_len = z.size();
+        out->asz = (uint8_t *)malloc(z.size());
+        std::memcpy(out->asz, z.data(), z.size());
+        out->min_val = C.min_val;
+        out->max_val = C.max_val;
+        out->abs_eb = C.abs_eb;
+        out->default_slope = C.default_slope_v;
+        out->t_fallback_count = C.t_fallback;
+        return 0;
+    } catch (const std::exception &e) {
+        set_err(err, e.what());
+        return -1;
+    }
+}
+
+void aszo_free_result(aszo_result *r) {
+    if (r->qb) {
+        for (uint32_t i = 0; i <= r->layer_num; i++) free(r->qb[i]);
+        free(r->qb);
+    }
+    free(r->qb_len);
+    free(r->t_int);
+    free(r->recon);
+    free(r->pre_zstd);
+    free(r->asz);
+    std::memset(r, 0, sizeof(*r));
+}
+
+int aszo_decompress(const uint8_t *asz, uint64_t asz_len, const uint64_t dims[3], float rel_eb, const aszo_params *p,
+                    float *out, char *err) {
+    try {
+        unsigned long long raw = ZSTD_getFrameContentSize(asz, asz_len);
+        if (raw == 0ULL - 1 || raw == 0ULL - 2) throw std::runtime_error("not a zstd frame with a known size");
+        vector<uint8_t> bs(raw);
+        size_t got = ZSTD_decompress(bs.data(), raw, asz, asz_len);
+        if (ZSTD_isError(got) || got != raw) throw std::runtime_error("ZSTD_decompress error in decompress()");
+        const uint8_t *b = bs.data(), *end = bs.data() + bs.size();
+        if (end - b < 9) throw std::runtime_error("truncated header");
+        codec C;
+        C.f = {{dims[0], dims[1], dims[2]}};
+        C.P.init(*p);
+        std::memcpy(&C.min_val, b, 4);
+        std::memcpy(&C.max_val, b + 4, 4);
+        uint8_t fl = b[8];
+        u64 L = fl;
+        if (fl & 0x40) {
+            C.quintic = (fl & 0x80) != 0;
+            L = fl & 0x3f;
+        }
+        b += 9;
+        if ((u64)(end - b) < 2 * L) throw std::runtime_error("truncated header");
+        for (u64 i = 0; i < L; i++) {
+            if (b[0] < '0' || b[0] > '2' || b[1] < '0' || b[1] > '2')
+                throw std::runtime_error("compressed stream contains an invalid predictor");
+            std::string pr = "cubic";
+            pr += (char)b[0];
+            pr += "_";
+            pr += b[1] == '0' ? "120" : b[1] == '1' ? "021" : "012";
+            C.plan.push_back(pr);
+            b += 2;
+        }
+        auto rd64 = [&](void) {
+            if (end - b < 8) throw std::runtime_error("truncated stream length");
+            u64 v = 0;
+            for (int i = 0; i < 8; i++) v |= (u64)b[i] << (8 * i);
+            b += 8;
+            return v;
+        };
+        {
+            u64 len = rd64();
+            C.t_int.assign(len, 0);
+            if (len) {
+                hdec<int64_t> d;
+                b = d.load(b, end);
+                b = d.decode(b, end, C.t_int.data(), len);
+            }
+        }
+        C.qbs.assign(L + 1, {});
+        for (u64 i = 0; i <= L; i++) {
+            u64 len = rd64();
+            C.qbs[i].assign(len, 0);
+            if (!len) continue;
+            hdec<int32_t> d;
+            b = d.load(b, end);
+            b = d.decode(b, end, C.qbs[i].data(), len);
+        }
+        C.abs_eb = rel_eb * (C.max_val - C.min_val);
+        C.geometry();
+        C.decompress_core(out);
+        return 0;
+    } catch (const std::exception &e) {
+        set_err(err, e.what());
+        return -1;
+    }
+}
+
+float aszo_default_slope(const float *data, const uint64_t dims[3], float abs_eb, float min_val, float max_val,
+                         const aszo_params *p) {
+    params_t P;
+    P.init(*p);
+    field f{{dims[0], dims[1], dims[2]}};
+    return default_slope(data, f, abs_eb, min_val, max_val, P);
+}
+
+uint64_t aszo_huffman_encode(const void *symbols, uint64_t n, int wide, uint8_t *out) {
+    vector<uint8_t> bs;
+    if (wide) {
+        const int64_t *s = (const int64_t *)symbols;
+        append_stream<int64_t>(bs, vector<int64_t>(s, s + n));
+    } else {
+        const int32_t *s = (const int32_t *)symbols;
+        append_stream<int32_t>(bs, vector<int32_t>(s, s + n));
+    }
+    if (out) std::memcpy(out, bs.data() + 8, bs.size() - 8);
+    return bs.size() - 8;
+}
+
+uint64_t aszo_abmap_order(const int64_t *a, const int64_t *b, uint64_t n, uint64_t *order) {
+    ab_map m;
+    std::map<std::tuple<i64, i64>, u64> first;
+    for (u64 i = 0; i < n; i++) {
+        m[{a[i], b[i]}]++;
+        first.emplace(std::tuple<i64, i64>{a[i], b[i]}, i);
+    }
+    u64 k = 0;
+    for (auto &kv : m) order[k++] = first[kv.first];
+    return k;
+}
+
+uint64_t aszo_i64map_order(const int64_t *keys, uint64_t n, uint64_t *order) {
+    std::unordered_map<i64, u64> m;
+    std::map<i64, u64> first;
+    for (u64 i = 0; i < n; i++) {
+        m[keys[i]]++;
+        first.emplace(keys[i], i);
+    }
+    u64 k = 0;
+    for (auto &kv : m) order[k++] = first[kv.first];
+    return k;
+}
+
+void aszo_h1_psnr(const int64_t *a, const int64_t *b, uint64_t n, float t, float abs_eb, float stat_eb, float min_val,
+                  float max_val, float *h1, float *psnr, float *x, float *mse) {
+    ab_map m;
+    for (u64 i = 0; i < n; i++) m[{a[i], b[i]}]++;
+    get_h1_psnr(*h1, *psnr, m, t, abs_eb, stat_eb, min_val, max_val, x, mse);
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+/* C interface of the CPU oracle: a restatement of the ASZ reference compression path.
+ *
+ * TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+ * may load this library, and only as the checker. The product never links it.
+ *
+ * Every function follows the reference codec (the .tpp files and huffman.hpp under c_codes/asz_core) and the
+ * floating-point form GCC 13.3 emits for it under the reference's flags
+ * (-Ofast -march=native -mavx2 -mfma, c_codes/CMakeLists.txt:12). Each FMA, reciprocal and
+ * rounding step is spelled out, so this file builds with -ffp-contract=off.
+ */
+#ifndef ASZ_ORACLE_H
+#define ASZ_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Tunables of asz::param_c (c_codes/asz_core/asz_param.hpp:147-180). The defaults come from
+ * aszo_default_params(). Fields the reference does not store in the .asz must be the same on
+ * both sides. */
+typedef struct aszo_params {
+    float pivot_eb_ratio, eb_ratio, slope_ratio;
+    uint64_t block_pivot_ratio;
+    int32_t t_precision;
+    float t_min, t_max;
+    uint64_t h1_block_sampling_num;
+    float stat_eb_ratio;
+    float default_slope_invalid_ratio_threshold, default_slope_fallback, default_slope_eb_span;
+    float insufficient_sample_t;
+} aszo_params;
+
+void aszo_default_params(aszo_params *p);
+
+/* Result of aszo_compress. Buffers are malloc'd by the oracle; free them with aszo_free_result. */
+typedef struct aszo_result {
+    uint32_t layer_num;
+    uint64_t *qb_len;        /* layer_num+1 stream lengths */
+    int32_t **qb;            /* layer_num+1 QB streams (pivot stream first) */
+    uint64_t t_len;
+    int64_t *t_int;          /* per (block, round) t codes, block-major */
+    float *recon;            /* in-place reconstruction (compressed_data) */
+    uint8_t *pre_zstd;       /* header + t stream + QB streams, before zstd */
+    uint64_t pre_zstd_len;
+    uint8_t *asz;            /* final .asz bytes (zstd level 3) */
+    uint64_t asz_len;
+    float min_val, max_val, abs_eb, default_slope;
+    uint64_t t_fallback_count;
+} aszo_result;
+
+/* Compress with a given plan ("cubic2_012,cubic1_120,..."), quintic = force_quintic.
+ * Returns 0 or a negative error code; err (256 bytes) receives a message. */
+int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p,
+                  const char *plan, int quintic, aszo_result *out, char *err);
+void aszo_free_result(aszo_result *r);
+
+/* Decompress an .asz produced by the reference or by aszo_compress. */
+int aszo_decompress(const uint8_t *asz, uint64_t asz_len, const uint64_t dims[3], float rel_eb,
+                    const aszo_params *p, float *out, char *err);
+
+/* Default rate-distortion slope (c_codes/asz_core/get_default_slope.tpp:6-83). */
+float aszo_default_slope(const float *data, const uint64_t dims[3], float abs_eb, float min_val,
+                         float max_val, const aszo_params *p);
+
+/* Huffman-encode one stream exactly as huffman_encoder_class<T> does (save + encode), T=int32
+ * (wide=0) or int64 (wide=1). Returns the byte count; out may be NULL to query the size. */
+uint64_t aszo_huffman_encode(const void *symbols, uint64_t n, int wide, uint8_t *out);
+
+/* Order probe for the hash-table emulation: builds std::unordered_map<tuple<int64,int64>,u64>
+ * with the reference hash from keys (a[i], b[i]) in sequence and writes the iteration order
+ * as indices of first occurrence into order (length = number of distinct keys, returned). */
+uint64_t aszo_abmap_order(const int64_t *a, const int64_t *b, uint64_t n, uint64_t *order);
+/* Same for std::unordered_map<int64_t,u64> (identity hash). */
+uint64_t aszo_i64map_order(const int64_t *k, uint64_t n, uint64_t *order);
+
+/* The reference's per-group proxy evaluation (c_codes/asz_core/get_h_psnr.tpp:6-31) on a map
+ * built from the keys in sequence. Also returns the float fed to log10f (x) and the sum (mse). */
+void aszo_h1_psnr(const int64_t *a, const int64_t *b, uint64_t n, float t, float abs_eb, float stat_eb,
+                  float min_val, float max_val, float *h1, float *psnr, float *x, float *mse);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
