@@ -1,0 +1,49 @@
+// Target geometry of one round, shared by the kernels and the host-side geometry check.
+#pragma once
+#include "dev_common.cuh"
+
+namespace asz {
+
+// Per-axis block tables of one round: count[b] targets of block b along the axis and prefix[b]
+// (exclusive sum), laid out at RoundGeom::axis_off[a].
+struct AxisTables {
+    const uint64_t *count, *prefix;
+};
+
+struct Target {
+    uint64_t pos, i, right, qi, block;
+};
+
+// Global target k of the round -> position, owning block, stencil bound and QB index.
+ASZ_HD Target locate(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, uint64_t k) {
+    uint64_t k2 = k % rg.tcount[2], k1 = (k / rg.tcount[2]) % rg.tcount[1], k0 = k / (rg.tcount[1] * rg.tcount[2]);
+    const uint64_t kk[3] = {k0, k1, k2};
+    uint64_t ii[3], bb[3], jj[3], cc[3];
+    for (int a = 0; a < 3; a++) {
+        ii[a] = a == rg.dir ? rg.hs + 2 * rg.hs * kk[a] : rg.stride[a] * kk[a];
+        bb[a] = owner_block(ii[a], fg.block_shape[a]);
+        uint64_t start = bb[a] * fg.block_shape[a] +
+                         (a == rg.dir ? rg.hs : (bb[a] == 0 ? 0 : rg.stride[a]));
+        jj[a] = (ii[a] - start) / rg.stride[a];
+        cc[a] = at.count[rg.axis_off[a] + bb[a]];
+    }
+    Target t;
+    t.pos = (ii[0] * fg.n[1] + ii[1]) * fg.n[2] + ii[2];
+    t.i = ii[rg.dir];
+    const uint64_t r = (bb[rg.dir] + 1) * fg.block_shape[rg.dir] + 1;
+    t.right = r < fg.n[rg.dir] ? r : fg.n[rg.dir];
+    // QB base of the block: per-axis prefix sums of the raster-ordered box sizes.
+    uint64_t base = at.prefix[rg.axis_off[0] + bb[0]] * rg.total[1] * rg.total[2] +
+                    cc[0] * at.prefix[rg.axis_off[1] + bb[1]] * rg.total[2] +
+                    cc[0] * cc[1] * at.prefix[rg.axis_off[2] + bb[2]];
+    // get_qb_index (asz_param.hpp:122-129).
+    uint64_t local = rg.order == 0 ? (jj[1] * cc[2] + jj[2]) * cc[0] + jj[0]
+                   : rg.order == 1 ? (jj[0] * cc[2] + jj[2]) * cc[1] + jj[1]
+                                   : (jj[0] * cc[1] + jj[1]) * cc[2] + jj[2];
+    t.qi = base + local;
+    t.block = (bb[0] * fg.block_num[1] + bb[1]) * fg.block_num[2] + bb[2];
+    return t;
+}
+
+
+}  // namespace asz

@@ -25,7 +25,9 @@
 #include <string>
 #include <vector>
 
+#include "../geometry.cuh"
 #include "../launch.h"
+#include "../listsim.cuh"
 #include "../../../include/asz_b200.h"
 #include "huffman_host.h"
 #include "zstd_api.h"
@@ -134,7 +136,72 @@ struct asz_ctx {
     float last_min = 0, last_max = 0;
     std::vector<uint8_t> pre_zstd;
     bool have_last = false;
+    // Profiling (asz_profile_*).
+    bool prof = false;
+    struct ProfSlot {
+        std::string name;
+        uint64_t launches = 0;
+        double ms = 0;
+        uint64_t bytes = 0;
+    };
+    std::vector<ProfSlot> prof_slots;
+    struct Pending {
+        cudaEvent_t a, b;
+        size_t slot;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
 };
+
+namespace {
+cudaEvent_t prof_event(asz_ctx *c) {
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+size_t prof_slot(asz_ctx *c, const char *name) {
+    for (size_t i = 0; i < c->prof_slots.size(); i++)
+        if (c->prof_slots[i].name == name) return i;
+    c->prof_slots.push_back({name, 0, 0, 0});
+    return c->prof_slots.size() - 1;
+}
+// Collects finished event pairs into the slots (called after a stream synchronisation).
+void prof_collect(asz_ctx *c) {
+    for (auto &p : c->pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        c->prof_slots[p.slot].ms += ms;
+        c->prof_slots[p.slot].launches++;
+        c->event_pool.push_back(p.a);
+        c->event_pool.push_back(p.b);
+    }
+    c->pending.clear();
+}
+// RAII timer around one launch.
+struct ProfScope {
+    asz_ctx *c;
+    cudaEvent_t a = nullptr, b = nullptr;
+    size_t slot = 0;
+    ProfScope(asz_ctx *ctx, const char *name, uint64_t bytes) : c(ctx) {
+        if (!c->prof) return;
+        slot = prof_slot(c, name);
+        c->prof_slots[slot].bytes += bytes;
+        a = prof_event(c);
+        b = prof_event(c);
+        cudaEventRecord(a, c->stream);
+    }
+    ~ProfScope() {
+        if (!a) return;
+        cudaEventRecord(b, c->stream);
+        c->pending.push_back({a, b, slot});
+    }
+};
+}  // namespace
 
 namespace {
 
@@ -481,7 +548,10 @@ int compute_range(asz_ctx *ctx, const float *d_in, u64 N, float &mn, float &mx) 
     init.zlast = 0;
     MiscLayout *dm = ctx->misc.as<MiscLayout>();
     CK(cudaMemcpyAsync(dm, &init, sizeof(MiscLayout), cudaMemcpyHostToDevice, ctx->stream));
-    CK(launch_range(d_in, N, dm->range, &dm->nonfinite, ctx->stream));
+    {
+        ProfScope ps(ctx, "range", N * 4);
+        CK(launch_range(d_in, N, dm->range, &dm->nonfinite, ctx->stream));
+    }
     MiscLayout h;
     CK(cudaMemcpyAsync(&h, dm, offsetof(MiscLayout, err), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -559,6 +629,7 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
     CK(cudaMemcpyAsync(dm->evals, evals, sizeof(ProxyEval) * ne, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
     const float R = mx - mn;
+    ProfScope ps_slope(ctx, "slope", 0);
     CK(launch_slope_v0(fg, dm->boxes, dm->evals, ne, d_in, ctx->log2arena.as<float>(), R * R, ctx->scratch.as<uint8_t>(),
                        sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, ctx->stream));
     std::vector<float> h1(3 * ne), x(3 * ne);
@@ -756,13 +827,20 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
                                cudaMemcpyHostToDevice, st));
         }
         // Pivots (compress.tpp:162-175).
-        CK(launch_pivot_compress(G.pg, d_in, d_rec, d_qb + qb_off[0], &dm->qb_range[0], st));
+        {
+            ProfScope ps(ctx, "pivot_compress", G.pivots * 12);
+            CK(launch_pivot_compress(G.pg, d_in, d_rec, d_qb + qb_off[0], &dm->qb_range[0], st));
+        }
         for (u64 l = 0; l < L; l++) {
             const RoundGeom &rg = G.rounds[l];
+            {
+            ProfScope ps(ctx, "tsel", 0);
             CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, ctx->classes.as<ClassInfo>() + 27 * l, d_rec, d_in,
                               ctx->log2arena.as<float>(), R2, t_default, ctx->scratch.as<uint8_t>(), sstride, capmax, bcap,
                               tcap, d_tval, d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap,
                               &dm->amb_count, ctx->overrides.as<uint32_t>(), (uint32_t)(overrides.size() / 3), &dm->err, st));
+            }
+            ProfScope ps(ctx, "round_compress", rg.targets * 12);
             CK(launch_round_compress(G.fg, rg, d_tabc, d_tabp, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
                                      &dm->qb_range[2 * (l + 1)], &dm->err, st));
         }
@@ -831,6 +909,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
     CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
     unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
+    ProfScope ps_hist(ctx, "histogram", (G.nblocks * L) * 8 + N * 4);
     if (so[0].count) CK(launch_histogram<int64_t>(d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off, st));
     for (u64 s = 0; s <= L; s++)
         if (so[s + 1].count)
@@ -881,6 +960,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         StreamOut &o = so[s];
         if (!o.count || o.code.maxval == 1) continue;
         size_t tb = ctx->cubtmp.cap;
+        ProfScope ps(ctx, "huff_encode", o.count * (s == 0 ? 8 : 4) + (o.code.bits + 7) / 8);
         if (s == 0)
             CK(launch_encode<int64_t>(d_tint, o.count, o.lo, d_codes + code_off[s], ctx->bitoff.as<u64>(), ctx->cubtmp.p, tb,
                                       d_pay + o.payload_word_off, st));
@@ -1009,7 +1089,10 @@ int gpu_decode(asz_ctx *ctx, const HuffParsed &hp, uint64_t count, const uint8_t
     MiscLayout *dm = ctx->misc.as<MiscLayout>();
     CK(cudaMemsetAsync(&dm->err, 0, 4, st));
     for (u64 it = 0;; it++) {
-        CK(launch_decode_sync(aligned, bit_begin, bit_end, C, nch, dt, d_start, d_end, d_cnt, &dm->err, st));
+        {
+            ProfScope ps(ctx, "huff_decode_sync", (hp.payload_bits + 7) / 8);
+            CK(launch_decode_sync(aligned, bit_begin, bit_end, C, nch, dt, d_start, d_end, d_cnt, &dm->err, st));
+        }
         CK(cudaMemsetAsync(d_flag, 0, 4, st));
         CK(launch_decode_restart(nch, d_end, d_start, d_flag, st));
         uint32_t flag;
@@ -1035,6 +1118,7 @@ int gpu_decode(asz_ctx *ctx, const HuffParsed &hp, uint64_t count, const uint8_t
     if (last[0] + last[1] != count)
         return fail(ctx, ASZ_E_DATA, last[0] + last[1] < count ? "Huffman payload contains too few values"
                                                                : "Huffman payload contains too many values");
+    ProfScope ps_w(ctx, "huff_decode_write", (hp.payload_bits + 7) / 8 + count * (wide ? 8 : 4));
     if (wide)
         CK(launch_decode_write<int64_t>(aligned, bit_begin, bit_end, C, nch, dt, hp.offset, d_start, d_off, (int64_t *)d_out,
                                         count, &dm->err, st));
@@ -1157,10 +1241,15 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     CK(cudaMemcpyAsync(d_tabp, G.tab_prefix.data(), G.tab_prefix.size() * 8, cudaMemcpyHostToDevice, st));
     MiscLayout *dm = ctx->misc.as<MiscLayout>();
     CK(cudaMemsetAsync(&dm->err, 0, 4, st));
-    CK(launch_pivot_decompress(G.pg, ctx->qb.as<int32_t>() + qoff[0], d_out, st));
-    for (u64 l = 0; l < L; l++)
+    {
+        ProfScope ps(ctx, "pivot_decompress", G.pivots * 8);
+        CK(launch_pivot_decompress(G.pg, ctx->qb.as<int32_t>() + qoff[0], d_out, st));
+    }
+    for (u64 l = 0; l < L; l++) {
+        ProfScope ps(ctx, "round_decompress", G.rounds[l].targets * 8);
         CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_tabc, d_tabp, ctx->tint.as<int64_t>(),
                                    ctx->qb.as<int32_t>() + qoff[l + 1], d_out, &dm->err, st));
+    }
     uint32_t errw;
     CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1241,4 +1330,175 @@ extern "C" int asz_compress_stats(asz_ctx *ctx, double *max_err, double *psnr) {
     if (max_err) *max_err = m;
     if (psnr) *psnr = 10.0 * std::log10(range * range / mse);
     return ASZ_OK;
+}
+
+extern "C" int asz_profile_enable(asz_ctx *ctx, int on) {
+    if (!ctx) return ASZ_E_ARG;
+    ctx->prof = on != 0;
+    return ASZ_OK;
+}
+
+extern "C" int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset) {
+    if (!ctx) return ASZ_E_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    prof_collect(ctx);
+    int n = (int)ctx->prof_slots.size();
+    for (int i = 0; i < n && i < max && out; i++) {
+        std::snprintf(out[i].name, sizeof(out[i].name), "%s", ctx->prof_slots[i].name.c_str());
+        out[i].launches = ctx->prof_slots[i].launches;
+        out[i].ms = ctx->prof_slots[i].ms;
+        out[i].bytes = ctx->prof_slots[i].bytes;
+    }
+    if (reset) ctx->prof_slots.clear();
+    return n;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Geometry self-check (see include/asz_b200.h).
+
+extern "C" int64_t asz_check_geometry(const uint64_t dims[3], const char *plan_text, uint64_t bpr, int quintic) {
+    if (!dims || !plan_text || bpr == 0) return ASZ_E_ARG;
+    Plan plan;
+    std::string err;
+    if (!parse_plan(plan_text, plan, err)) return ASZ_E_ARG;
+    const u64 N = dims[0] * dims[1] * dims[2];
+    if (N > (1ull << 26)) return ASZ_E_UNSUPPORTED;
+    asz_params p;
+    asz_default_params(&p);
+    p.block_pivot_ratio = bpr;
+    Geometry G;
+    build_geometry(dims, plan, p, 1.0f, 1.0f, quintic != 0, G);
+    const FieldGeom &fg = G.fg;
+    const u64 L = plan.pred.size();
+    int64_t bad = 0;
+    std::vector<int32_t> stamp(N, -1);
+    // Pivots.
+    for (u64 i0 = 0; i0 < fg.n[0]; i0 += fg.pivot_stride[0])
+        for (u64 i1 = 0; i1 < fg.n[1]; i1 += fg.pivot_stride[1])
+            for (u64 i2 = 0; i2 < fg.n[2]; i2 += fg.pivot_stride[2]) stamp[(i0 * fg.n[1] + i1) * fg.n[2] + i2] = 0;
+    AxisTables at{G.tab_count.data(), G.tab_prefix.data()};
+    u64 written = G.pivots;
+    for (u64 l = 0; l < L; l++) {
+        const RoundGeom &rg = G.rounds[l];
+        const int32_t cur = (int32_t)l + 1;
+        auto readable = [&](int64_t q) { return q >= 0 && (u64)q < N && stamp[q] >= 0 && stamp[q] < cur; };
+        // Reference order of QB indices: blocks in raster order, targets in compress.tpp:67-86 order.
+        std::vector<u64> ref_pos(rg.qb_total, ~0ull);
+        u64 base = 0;
+        for (u64 b0 = 0; b0 < fg.block_num[0]; b0++)
+            for (u64 b1 = 0; b1 < fg.block_num[1]; b1++)
+                for (u64 b2 = 0; b2 < fg.block_num[2]; b2++) {
+                    u64 bb[3] = {b0, b1, b2}, lo[3], hi[3], sh[3];
+                    for (int a = 0; a < 3; a++) {
+                        u64 l0 = bb[a] * fg.block_shape[a];
+                        hi[a] = std::min((bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
+                        lo[a] = a == rg.dir ? l0 + rg.stride[a] / 2 : (l0 == 0 ? 0 : l0 + rg.stride[a]);
+                        sh[a] = lo[a] >= hi[a] ? 0 : (hi[a] - lo[a] + rg.stride[a] - 1) / rg.stride[a];
+                    }
+                    for (u64 i0 = lo[0], j0 = 0; i0 < hi[0]; i0 += rg.stride[0], j0++)
+                        for (u64 i1 = lo[1], j1 = 0; i1 < hi[1]; i1 += rg.stride[1], j1++)
+                            for (u64 i2 = lo[2], j2 = 0; i2 < hi[2]; i2 += rg.stride[2], j2++) {
+                                u64 li = rg.order == 0 ? (j1 * sh[2] + j2) * sh[0] + j0
+                                        : rg.order == 1 ? (j0 * sh[2] + j2) * sh[1] + j1
+                                                        : (j0 * sh[1] + j1) * sh[2] + j2;
+                                if (base + li >= rg.qb_total) bad++;
+                                else ref_pos[base + li] = (i0 * fg.n[1] + i1) * fg.n[2] + i2;
+                            }
+                    base += sh[0] * sh[1] * sh[2];
+                }
+        if (base != rg.qb_total) bad++;
+        std::vector<uint8_t> used(rg.qb_total, 0);
+        std::vector<u64> targets;
+        for (u64 k = 0; k < rg.targets; k++) {
+            Target t = locate(fg, rg, at, k);
+            if (t.pos >= N || t.qi >= rg.qb_total || used[t.qi] || t.block >= G.nblocks) {
+                bad++;
+                continue;
+            }
+            used[t.qi] = 1;
+            if (ref_pos[t.qi] != t.pos) bad++;
+            if (stamp[t.pos] != -1) bad++;
+            // The stencil branch exactly as predict() selects it.
+            const int64_t pos = (int64_t)t.pos, d = (int64_t)rg.dist;
+            const u64 i = t.i, hs = rg.hs, right = t.right;
+            std::vector<int64_t> rd;
+            if (quintic && i >= 5 * hs && i + 5 * hs < right) rd = {-1, 1, -3, 3, -5, 5};
+            else if (i <= hs) {
+                if (i + hs >= right) rd = {-1};
+                else if (i + 3 * hs >= right) rd = {-1, 1};
+                else rd = {-1, 1, 3};
+            } else if (i + hs >= right) rd = {-1, -3};
+            else if (i + 3 * hs >= right) rd = {-1, 1, -3};
+            else rd = {-3, 3, -1, 1};
+            for (int64_t o : rd)
+                if (!readable(pos + o * d)) bad++;
+            targets.push_back(t.pos);
+        }
+        for (u64 q = 0; q < rg.qb_total; q++)
+            if (!used[q]) bad++;
+        // Coefficient-selection samples: x0 is an unwritten target of this round, the four
+        // references are earlier values (compress.tpp:102-120, get_AB_map.tpp:13-19).
+        for (u64 g = 0; g < G.nblocks; g++) {
+            u64 bb[3] = {g / (fg.block_num[1] * fg.block_num[2]), (g / fg.block_num[2]) % fg.block_num[1], g % fg.block_num[2]};
+            int cls = 0;
+            for (int a = 0; a < 3; a++) cls = cls * 3 + (bb[a] == 0 ? 0 : (bb[a] == fg.block_num[a] - 1 ? 2 : 1));
+            const ClassInfo &ci = G.classes[l][cls];
+            if (ci.fallback) continue;
+            u64 lo[3], hi[3], step[3], cnt = 1;
+            for (int a = 0; a < 3; a++) {
+                lo[a] = bb[a] * fg.block_shape[a];
+                hi[a] = std::min((bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
+                if (a != rg.dir && lo[a] != 0) lo[a] += rg.stride[a];
+                if (a == rg.dir) {
+                    lo[a] += 3 * rg.stride[a] / 2;
+                    hi[a] -= 3 * rg.stride[a] / 2;
+                }
+                step[a] = rg.stride[a] * ci.ss;
+                cnt *= hi[a] > lo[a] ? (hi[a] - lo[a] + step[a] - 1) / step[a] : 0;
+            }
+            if (cnt != ci.n) bad++;
+            for (u64 i0 = lo[0]; i0 < hi[0]; i0 += step[0])
+                for (u64 i1 = lo[1]; i1 < hi[1]; i1 += step[1])
+                    for (u64 i2 = lo[2]; i2 < hi[2]; i2 += step[2]) {
+                        int64_t pos = (int64_t)((i0 * fg.n[1] + i1) * fg.n[2] + i2), d = (int64_t)rg.dist;
+                        if (pos < 0 || (u64)pos >= N || stamp[pos] != -1) bad++;
+                        for (int64_t o : {-1, 1, -3, 3})
+                            if (!readable(pos + o * d)) bad++;
+                    }
+        }
+        for (u64 q : targets) stamp[q] = cur;
+        written += targets.size();
+    }
+    if (written != N) bad++;
+    for (u64 q = 0; q < N; q++)
+        if (stamp[q] < 0) {
+            bad++;
+            break;
+        }
+    return bad;
+}
+
+extern "C" int64_t asz_check_hashorder(const int64_t *a, const int64_t *b, uint64_t n, int pair, uint64_t *order) {
+    if (!a || (pair && !b) || !order) return ASZ_E_ARG;
+    std::map<std::pair<int64_t, int64_t>, uint64_t> first;
+    std::vector<uint64_t> firsts;
+    std::vector<uint64_t> hash;
+    std::vector<int64_t> keys;
+    for (uint64_t i = 0; i < n; i++) {
+        std::pair<int64_t, int64_t> k{a[i], pair ? b[i] : 0};
+        if (first.emplace(k, i).second) {
+            firsts.push_back(i);
+            hash.push_back(pair ? (uint64_t)a[i] * 1145141919810ull + (uint64_t)b[i] : (uint64_t)a[i]);
+            keys.push_back(a[i]);
+        }
+    }
+    const uint32_t m = (uint32_t)firsts.size();
+    std::vector<int32_t> nxt(m + 1), bkt(sched_buckets(m) + 1);
+    ListSim L{nxt.data(), bkt.data(), pair ? hash.data() : nullptr, keys.data(), m, 0, 1, 0, false};
+    L.init();
+    for (uint32_t e = 0; e < m; e++) L.insert((int32_t)e);
+    if (L.broken) return -1;
+    uint32_t k = 0;
+    for (int32_t p = nxt[m]; p != kNil && k < m; p = nxt[p]) order[k++] = firsts[p];
+    return k == m ? (int64_t)m : -1;
 }

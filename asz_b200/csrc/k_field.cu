@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "dev_common.cuh"
+#include "geometry.cuh"
 #include "launch.h"
 
 namespace asz {
@@ -23,7 +24,7 @@ __device__ __forceinline__ int32_t ord_key(float v) {
 }
 
 // out[0] = min key, out[1] = max key (ordered-int encoding), out[2] = count of non-finite values.
-__global__ void range_kernel(const float4 *__restrict__ x4, uint64_t n4, const float *__restrict__ tail, uint32_t ntail,
+__global__ void range_kernel(const float4 *__restrict__ x4, uint64_t n4, const float *__restrict__ tail, uint64_t ntail,
                              int32_t *out, unsigned long long *nonfinite) {
     int32_t mn = INT32_MAX, mx = INT32_MIN;
     unsigned long long bad = 0;
@@ -42,8 +43,8 @@ __global__ void range_kernel(const float4 *__restrict__ x4, uint64_t n4, const f
             mx = max(mx, o);
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x < ntail) {
-        float v = tail[threadIdx.x];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ntail; i += stride) {
+        float v = tail[i];
         if (!isfinite(v)) bad++;
         else {
             mn = min(mn, ord_key(v));
@@ -145,47 +146,6 @@ __device__ __forceinline__ float predict(const float *__restrict__ c, uint64_t i
     return __double2float_rn(__fma_rn(__dadd_rn(0.25, td), (double)s1, (double)p1));
 }
 
-// Per-axis block tables of one round: count[b] targets of block b along the axis and prefix[b]
-// (exclusive sum), laid out at RoundGeom::axis_off[a].
-struct AxisTables {
-    const uint64_t *count, *prefix;
-};
-
-struct Target {
-    uint64_t pos, i, right, qi, block;
-};
-
-// Global target k of the round -> position, owning block, stencil bound and QB index.
-__device__ __forceinline__ Target locate(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, uint64_t k) {
-    uint64_t k2 = k % rg.tcount[2], k1 = (k / rg.tcount[2]) % rg.tcount[1], k0 = k / (rg.tcount[1] * rg.tcount[2]);
-    const uint64_t kk[3] = {k0, k1, k2};
-    uint64_t ii[3], bb[3], jj[3], cc[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        ii[a] = a == rg.dir ? rg.hs + 2 * rg.hs * kk[a] : rg.stride[a] * kk[a];
-        bb[a] = owner_block(ii[a], fg.block_shape[a]);
-        uint64_t start = bb[a] * fg.block_shape[a] +
-                         (a == rg.dir ? rg.hs : (bb[a] == 0 ? 0 : rg.stride[a]));
-        jj[a] = (ii[a] - start) / rg.stride[a];
-        cc[a] = at.count[rg.axis_off[a] + bb[a]];
-    }
-    Target t;
-    t.pos = (ii[0] * fg.n[1] + ii[1]) * fg.n[2] + ii[2];
-    t.i = ii[rg.dir];
-    t.right = min((bb[rg.dir] + 1) * fg.block_shape[rg.dir] + 1, fg.n[rg.dir]);
-    // QB base of the block: per-axis prefix sums of the raster-ordered box sizes.
-    uint64_t base = at.prefix[rg.axis_off[0] + bb[0]] * rg.total[1] * rg.total[2] +
-                    cc[0] * at.prefix[rg.axis_off[1] + bb[1]] * rg.total[2] +
-                    cc[0] * cc[1] * at.prefix[rg.axis_off[2] + bb[2]];
-    // get_qb_index (asz_param.hpp:122-129).
-    uint64_t local = rg.order == 0 ? (jj[1] * cc[2] + jj[2]) * cc[0] + jj[0]
-                   : rg.order == 1 ? (jj[0] * cc[2] + jj[2]) * cc[1] + jj[1]
-                                   : (jj[0] * cc[1] + jj[1]) * cc[2] + jj[2];
-    t.qi = base + local;
-    t.block = (bb[0] * fg.block_num[1] + bb[1]) * fg.block_num[2] + bb[2];
-    return t;
-}
-
 // Compress round: quantise the residual and write the reconstruction in place.
 // compress.tpp:35-37 as emitted: axis 0 multiplies by the hoisted 0.5*(1/eb) (inlined loop),
 // axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
@@ -253,11 +213,11 @@ static unsigned grid_for(uint64_t n, unsigned threads, unsigned cap) {
 }
 
 cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st) {
+    // 128-bit loads when the pointer allows; otherwise (and for the tail) scalar loads.
     uint64_t n4 = ((uintptr_t)x % 16 == 0) ? n / 4 : 0;
-    uint32_t ntail = (uint32_t)(n - 4 * n4);
-    if (ntail > 1024) return cudaErrorInvalidValue;
-    range_kernel<<<grid_for(n4 ? n4 : 1, 256, 148 * 8), max(256u, ntail), 0, st>>>((const float4 *)x, n4, x + 4 * n4,
-                                                                                     ntail, out, nonfinite);
+    uint64_t ntail = n - 4 * n4;
+    range_kernel<<<grid_for(n4 ? n4 : ntail, 256, 148 * 8), 256, 0, st>>>((const float4 *)x, n4, x + 4 * n4, ntail, out,
+                                                                           nonfinite);
     return cudaGetLastError();
 }
 

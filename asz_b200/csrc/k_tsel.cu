@@ -22,20 +22,12 @@
 
 #include "dev_common.cuh"
 #include "tsel.cuh"
+#include "listsim.cuh"
 #include "launch.h"
 
 namespace asz {
 namespace {
 
-constexpr int32_t kNil = -1;
-
-// Device copy of the bucket schedule (tsel.cuh).
-__constant__ uint64_t d_sched_at[kSchedLen] = {1, 14, 30, 60, 128, 258, 542, 1110, 2358, 5088, 10274, 20754,
-                                               42044, 85230, 172934, 351062, 712698, 1447154, 2938680,
-                                               5967348, 12117690};
-__constant__ uint64_t d_sched_bkt[kSchedLen] = {13, 29, 59, 127, 257, 541, 1109, 2357, 5087, 10273, 20753,
-                                                42043, 85229, 172933, 351061, 712697, 1447153, 2938679,
-                                                5967347, 12117689, 24607243};
 
 // Per-group scratch carved from one global arena. cap = max samples of the launch.
 struct Scratch {
@@ -101,68 +93,6 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
     return x;
 }
 
-// Emulated std::unordered_map list: nodes 0..count-1, sentinel (before_begin) at index `cap`.
-struct ListSim {
-    int32_t *nxt, *bkt;
-    const uint64_t *hash;  // NULL: identity hash of the int64 keys in `keys`
-    const int64_t *keys;
-    uint32_t cap, count;
-    uint64_t nbkt;
-    int sched;
-
-    __device__ uint64_t code(int32_t x) const { return hash ? hash[x] : (uint64_t)keys[x]; }
-
-    __device__ void init() {
-        count = 0;
-        nbkt = 1;
-        sched = 0;
-        nxt[cap] = kNil;
-    }
-    // _Hashtable::_M_rehash_aux (unique keys).
-    __device__ void rehash(uint64_t nb) {
-        for (uint64_t i = 0; i < nb; i++) bkt[i] = kNil;
-        int32_t p = nxt[cap];
-        nxt[cap] = kNil;
-        uint64_t bbegin = 0;
-        const int32_t S = (int32_t)cap;
-        while (p != kNil) {
-            int32_t nx = nxt[p];
-            uint64_t b = code(p) % nb;
-            if (bkt[b] == kNil) {
-                nxt[p] = nxt[S];
-                nxt[S] = p;
-                bkt[b] = S;
-                if (nxt[p] != kNil) bkt[bbegin] = p;
-                bbegin = b;
-            } else {
-                nxt[p] = nxt[bkt[b]];
-                nxt[bkt[b]] = p;
-            }
-            p = nx;
-        }
-        nbkt = nb;
-    }
-    // _M_insert_unique_node: rehash check, then _M_insert_bucket_begin.
-    __device__ void insert(int32_t x) {
-        if (sched < kSchedLen && (uint64_t)count + 1 == d_sched_at[sched]) {
-            rehash(d_sched_bkt[sched]);
-            sched++;
-        }
-        const int32_t S = (int32_t)cap;
-        uint64_t b = code(x) % nbkt;
-        if (bkt[b] != kNil) {
-            nxt[x] = nxt[bkt[b]];
-            nxt[bkt[b]] = x;
-        } else {
-            nxt[x] = nxt[S];
-            nxt[S] = x;
-            if (nxt[x] != kNil) bkt[code(nxt[x]) % nbkt] = x;
-            bkt[b] = S;
-        }
-        count++;
-    }
-};
-
 struct FieldRef {
     const float *ref;  // reference values (reconstruction, or the original field for the slope)
     const float *x0;   // the value at the sample point itself (original field)
@@ -214,7 +144,8 @@ __device__ uint32_t build_abmap(const SampleBox &box, const FieldRef &f, Scratch
     L.init();
     for (uint32_t e = 0; e < m; e++) L.insert((int32_t)e);
     uint32_t k = 0;
-    for (int32_t p = s.nxt[s.cap]; p != kNil; p = s.nxt[p]) s.ord[k++] = p;
+    for (int32_t p = s.nxt[s.cap]; p != kNil && k < m; p = s.nxt[p]) s.ord[k++] = p;
+    if (k != m || L.broken) return UINT32_MAX;
     return m;
 }
 
@@ -262,7 +193,8 @@ __device__ void eval_proxy(Scratch &s, uint32_t m, float t, float abs_eb, float 
     float nf = __ull2float_rn(n);
     float h1 = 0.0f;
     float r = __fdiv_rn(1.0f, nf);
-    for (int32_t p = s.qnxt[s.cap]; p != kNil; p = s.qnxt[p]) {
+    uint32_t walked = 0;
+    for (int32_t p = s.qnxt[s.cap]; p != kNil && walked < mq; p = s.qnxt[p], walked++) {
         uint64_t fq = s.qc[p];
         float pr = __fmul_rn(__ull2float_rn(fq), r);
         h1 = __fmaf_rn(-pr, log2tab[fq], h1);

@@ -35,7 +35,7 @@ def grf_field(shape, alpha, rng, aniso=(1.0, 1.0, 1.0)):
     kk[0, 0, 0] = 1.0
     amp = kk ** (-alpha / 2.0)
     amp[0, 0, 0] = 0.0
-    f = np.fft.irfftn(spec * amp, s=shape)
+    f = np.fft.irfftn(spec * amp, s=shape, axes=(0, 1, 2))
     f -= f.mean()
     sd = f.std()
     return f / sd if sd > 0 else f

@@ -1,0 +1,351 @@
+"""Benchmark: ASZ compression hot path on B200 (one JSON line on rank 0).
+
+Workload: one 512^3 float32 field (k^-5/3 Gaussian random field plus a tanh front of width 4
+voxels on a random plane, amplitude 10x the field's std, seeded), REL 1e-3, the fixed plan
+"cubic2_012" on every level (9 rounds), cubic family, block_pivot_ratio 3 (the reference launcher's
+setting for REL > 1e-4).
+
+  value  compress throughput in input GB/s with the field resident in HBM. Each step is one full
+         compression to the pre-zstd stream (range, default slope, all rounds with per-block t,
+         histograms, Huffman codes and encoding). The final libzstd stage is timed separately.
+  e2e    the same through the C ABI from pinned host memory to .asz bytes on the host, with the
+         host->device copy, the device->host copy of the stream and libzstd inside the timed region.
+Decompression throughput is reported beside them. The field (512 MiB) is larger than L2 (126 MB),
+so no flush is needed between steps.
+
+Multi-GPU: fields are independent, so each rank compresses its own field (weak scaling, no
+collective on the data path); value = total input bytes / max-over-ranks time.
+
+--impl reference times the reference's own CPU compressor (oracle/_ref/s1_compress, built from
+the reference sources) on a bounded slab of the same field.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (512, 512, 512)
+REL_EB = 1e-3
+PLAN = ",".join(["cubic2_012"] * 9)
+FAMILY = "cubic"
+BPR = 3
+METRIC = "compress/decompress GB/s at REL 1e-3 (bit-exact); tune time & CR vs plain at same eb"
+WORKLOAD = "512^3 float32 k^-5/3 GRF + tanh front, REL 1e-3, plan cubic2_012 x9, cubic, block_pivot_ratio 3"
+
+
+def make_field_torch(seed, shape, device):
+    """The C2 recipe on the GPU (torch FFT), returned as a contiguous float32 CUDA tensor."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    white = torch.randn(shape, generator=g, device=device, dtype=torch.float32)
+    spec = torch.fft.rfftn(white)
+    del white
+    k = [torch.fft.fftfreq(n, device=device) * n for n in shape[:-1]] + [torch.fft.rfftfreq(shape[-1], device=device) * shape[-1]]
+    kk = (k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2).sqrt_()
+    kk[0, 0, 0] = 1.0
+    amp = kk.pow_(-5.0 / 6.0)
+    amp[0, 0, 0] = 0.0
+    spec.mul_(amp)
+    del amp, kk
+    f = torch.fft.irfftn(spec, s=shape)
+    del spec
+    f -= f.mean()
+    f /= f.std()
+    gen = np.random.default_rng(seed)
+    n = gen.standard_normal(3)
+    n /= np.linalg.norm(n)
+    c = [gen.uniform(0.25 * s, 0.75 * s) for s in shape]
+    ax = [torch.arange(s, device=device, dtype=torch.float32) for s in shape]
+    d = (ax[0][:, None, None] - c[0]) * n[0] + (ax[1][None, :, None] - c[1]) * n[1] + (ax[2][None, None, :] - c[2]) * n[2]
+    f += 10.0 * f.std() * torch.tanh(d / 4.0)
+    return f.contiguous()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def cpu_baseline(field_np, workdir, planes=64):
+    """The reference s1_compress on the first `planes` planes of the field (same plan/eb/flags)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    exe = O.ref_binary("s1_compress")
+    kind = "reference"
+    sample = field_np[:planes]
+    inp = os.path.join(workdir, "slab.f32")
+    out = os.path.join(workdir, "slab.asz")
+    np.ascontiguousarray(sample).tofile(inp)
+    if exe is None:
+        return None
+    # The reference takes abs_eb from its own input's range; REL is applied to the slab.
+    argv = [exe, "-i", inp, "-z", out, "-3", *[str(s) for s in sample.shape], "-M", "REL", repr(REL_EB),
+            "--predictor-plan", PLAN, "--predictor-family", FAMILY, "--block-pivot-ratio", str(BPR)]
+    t0 = time.perf_counter()
+    r = subprocess.run(argv, capture_output=True, text=True)
+    wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        return None
+    comp = None
+    for line in r.stdout.splitlines():
+        if line.startswith("Compression time:"):
+            comp = float(line.split(":")[1].split()[0])
+    return {"value": sample.nbytes / 1e9 / wall, "unit": "GB/s", "cores": 1, "kind": kind,
+            "sample": f"reference s1_compress on a {sample.shape[0]}x512x512 slab of the field, wall time "
+                      f"(its own 'Compression time' {comp:.3f} s, which excludes plan preparation)" if comp else
+                      f"reference s1_compress on a {sample.shape[0]}x512x512 slab, wall time"}
+
+
+def run_reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    exe = O.ref_binary("s1_compress")
+    if exe is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference binaries not built (make -C oracle ref)"}))
+        return
+    from asz_b200 import fields
+    planes = 32
+    field = fields.c2_field(seed=2, shape=(planes, 512, 512))
+    with tempfile.TemporaryDirectory() as wd:
+        inp = os.path.join(wd, "slab.f32")
+        field.tofile(inp)
+        argv = [exe, "-i", inp, "-z", os.path.join(wd, "o.asz"), "-3", str(planes), "512", "512", "-M", "REL", repr(REL_EB),
+                "--predictor-plan", PLAN, "--predictor-family", FAMILY, "--block-pivot-ratio", str(BPR)]
+        for _ in range(args.warmup):
+            subprocess.run(argv, capture_output=True, check=True)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            subprocess.run(argv, capture_output=True, check=True)
+        dt = time.perf_counter() - t0
+    gbs = field.nbytes * args.steps / 1e9 / dt
+    sample = f"reference s1_compress (1 thread) on a {planes}x512x512 slab of the C2 recipe per step"
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                      "data": "synthetic", "config": {"workload": WORKLOAD, "sample_planes": planes},
+                      "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": 1, "kind": "reference", "sample": sample},
+                      "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import ctypes as C
+
+    import torch
+
+    import asz_b200.api as api
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    x = make_field_torch(1234 + rank, SHAPE, dev)
+    N = x.numel()
+    p = api.default_params(block_pivot_ratio=BPR)
+    ctx = api.Context(local)
+    L = api.lib()
+    L.asz_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize(dev)
+
+    y = torch.empty_like(x)
+    blob = None
+    for _ in range(args.warmup):
+        blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+        ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+    # Compress, device-resident input.
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    zstd_s = 0.0
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+            zstd_s += rep.zstd_s
+        ev1.record(stream)
+        barrier()
+    comp_ms = ev0.elapsed_time(ev1)
+    # Device time excludes the host libzstd stage, which the ABI call also performs.
+    core_ms = comp_ms - zstd_s * 1000
+    # Decompress into device memory.
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+    ev1.record(stream)
+    barrier()
+    dec_ms = ev0.elapsed_time(ev1)
+    # Parity spot check of this run: decompression equals the compressor's reconstruction.
+    blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+    rec = torch.from_numpy(ctx.debug_recon()).to(dev).view(SHAPE)
+    ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+    torch.cuda.synchronize(dev)
+    bit_exact = bool(torch.equal(rec.view(torch.int32), y.view(torch.int32)))
+    max_err = float((y - x).abs().max().item())
+    # Profile of one compression (per kernel family).
+    L.asz_profile_enable(ctx._c, 1)
+    blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+    entries = (PROFILE_ENTRY * 64)()
+    n = L.asz_profile_read(ctx._c, entries, 64, 1)
+    L.asz_profile_enable(ctx._c, 0)
+    prof = {entries[i].name.decode(): {"launches": entries[i].launches, "ms": entries[i].ms, "bytes": entries[i].bytes}
+            for i in range(min(n, 64))}
+    # End to end from pinned host memory, including zstd.
+    xh = x.cpu().pin_memory()
+    xh_np = xh.numpy()
+    barrier()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        blob_e, rep_e = ctx.compress(xh_np, REL_EB, PLAN, FAMILY, p)
+    ev1.record(stream)
+    barrier()
+    e2e_ms = ev0.elapsed_time(ev1)
+    # Max over ranks.
+    times = torch.tensor([core_ms, dec_ms, e2e_ms], device=dev)
+    if pg:
+        pg.all_reduce(times, op=pg.ReduceOp.MAX)
+    core_ms, dec_ms, e2e_ms = times.tolist()
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+    total_bytes = 4.0 * N * world
+    comp_gbs = total_bytes * args.steps / (core_ms / 1000) / 1e9
+    dec_gbs = total_bytes * args.steps / (dec_ms / 1000) / 1e9
+    e2e_gbs = total_bytes * args.steps / (e2e_ms / 1000) / 1e9
+    peak, peak_kind = measured_peaks()
+    top = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else None
+    roofline = None
+    if top:
+        name, t = top
+        if t["bytes"] and t["ms"] > 0:
+            ach = t["bytes"] / (t["ms"] / 1000) / 1e9
+            roofline = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                        "peak_source": peak_kind, "traffic": None}
+        else:
+            # Whole-path algorithmic bytes (4N read + stream written) over the device time.
+            ach = (4.0 * N + rep.pre_zstd_len) / (core_ms / args.steps / 1000) / 1e9
+            roofline = {"bound": "hbm", "kernel": "whole compress path (top family: " + name + ")", "achieved": ach,
+                        "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind, "traffic": None}
+    cpu = None
+    if not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as wd:
+            cpu = cpu_baseline(x[:64].cpu().numpy(), wd, planes=64)
+    out = {
+        "metric": METRIC, "value": comp_gbs, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": core_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "inputs": "512 MiB per field > L2, no flush needed", "parallelism": f"replicas x{world}"},
+        "decompress": {"value": dec_gbs, "unit": "GB/s", "ms_per_step": dec_ms / args.steps},
+        "zstd_ms_per_step": zstd_s * 1000 / args.steps,
+        "e2e": {"value": e2e_gbs, "unit": "GB/s", "h2d_bytes_per_step": 4 * N, "d2h_bytes_per_step": int(rep_e.pre_zstd_len),
+                "includes": "H2D from pinned memory, all GPU stages, D2H of the stream, libzstd level 3"},
+        "cr": float(4 * N / len(blob)), "bit_exact_roundtrip": bit_exact, "max_err_over_eb": max_err / rep.abs_eb,
+        "t_fallback_count": int(rep.t_fallback_count), "ambiguous_decisions": int(rep.ambiguous_decisions),
+        "roofline": roofline, "profile": prof, "cpu_baseline": cpu, "clocks": clocks.summary(),
+        "gpu_launches": int(sum(v["launches"] for v in prof.values())) if prof else None,
+    }
+    print(json.dumps(out))
+    if pg:
+        pg.destroy_process_group()
+
+
+import ctypes as _C  # noqa: E402
+
+
+class PROFILE_ENTRY(_C.Structure):
+    _fields_ = [("name", _C.c_char * 32), ("launches", _C.c_uint64), ("ms", _C.c_double), ("bytes", _C.c_uint64)]
+
+
+if __name__ == "__main__":
+    main()

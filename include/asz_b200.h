@@ -129,6 +129,33 @@ void asz_free(void *ptr);
  * to that call must still be valid (device input) or is the context's own copy (host input). */
 int asz_compress_stats(asz_ctx *ctx, double *max_err, double *psnr);
 
+/* Device-time profile by kernel family (CUDA events around each launch on the context's
+ * stream). Off by default; enabling it adds one event pair per launch. */
+typedef struct asz_profile_entry {
+    char name[32];        /* kernel family, e.g. "tsel", "round_compress", "huff_encode" */
+    uint64_t launches;
+    double ms;            /* summed device time */
+    uint64_t bytes;       /* algorithmic bytes moved by those launches (reads + writes) */
+} asz_profile_entry;
+
+int asz_profile_enable(asz_ctx *ctx, int on);
+/* Copies up to max entries accumulated since the last reset; returns how many exist. */
+int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset);
+
+/* Host-side self-check of the target geometry the round kernels use, for a field of the given
+ * dims, plan and block ratio (no GPU involved): every stencil and sampling read is in bounds
+ * and hits a value written in an earlier round, every point is written once, and the QB index
+ * of every target equals its position in the reference's block-major loops
+ * (compress.tpp:53-88). Returns the number of violations (0), or a negative error code. */
+int64_t asz_check_geometry(const uint64_t dims[3], const char *plan, uint64_t block_pivot_ratio, int quintic);
+
+/* Host-side run of the device's std::unordered_map order emulation (no GPU involved), for
+ * checking it against the real container: keys are (a[i], b[i]) pairs with the reference's
+ * hash (asz_param.hpp:22-40) when pair is nonzero, else a[i] with the identity hash. Writes the
+ * iteration order as indices of first occurrence; returns the number of distinct keys, or a
+ * negative value if the emulated list is inconsistent. */
+int64_t asz_check_hashorder(const int64_t *a, const int64_t *b, uint64_t n, int pair, uint64_t *order);
+
 /* Internals of the last asz_compress call on this context, for parity checks: QB stream k
  * (0 = pivots, k = round k), per-(block, round) t codes, the in-place reconstruction and the
  * stream before zstd. Each copies into caller memory and returns the element count; pass NULL to

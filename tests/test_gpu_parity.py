@@ -1,0 +1,136 @@
+"""Parity of the CUDA path with the reference: golden vectors written by the reference binary,
+randomised cases against the CPU oracle (QB streams, t codes, reconstruction, stream bytes), the
+drop-in CLI, device-resident inputs, and corrupt-stream handling."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ROOT, golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+BIN = os.path.join(ROOT, "asz_b200", "bin")
+
+
+def _params(api, **kw):
+    return api.default_params(**kw)
+
+
+@pytest.mark.parametrize("case", golden_cases(), ids=lambda c: c["name"])
+def test_golden_compress_and_decompress(gpu_ctx, case):
+    import asz_b200.api as api
+    data, blob, out = load_golden(case)
+    p = _params(api, block_pivot_ratio=case["block_pivot_ratio"])
+    got, rep = gpu_ctx.compress(data, case["rel_eb"], case["plan"], case["family"], p)
+    assert got == blob
+    rec = gpu_ctx.debug_recon().reshape(data.shape)
+    assert np.array_equal(rec.view(np.uint32), out.view(np.uint32))
+    dec, _ = gpu_ctx.decompress(blob, data.shape, case["rel_eb"], _params(api, block_pivot_ratio=case["block_pivot_ratio"]))
+    assert np.array_equal(dec.view(np.uint32), out.view(np.uint32))
+
+
+def _check_against_oracle(ctx, data, eb, plan, family, bpr):
+    import asz_b200.api as api
+    p = api.default_params(block_pivot_ratio=bpr)
+    blob, rep = ctx.compress(data, eb, plan, family, p)
+    o = O.compress(data, eb, plan, family == "quintic", O.default_params(block_pivot_ratio=bpr))
+    assert rep.default_slope == np.float32(o.default_slope) or (np.isnan(rep.default_slope) and np.isnan(o.default_slope))
+    assert np.array_equal(ctx.debug_t(), o.t_int)
+    for s, q in enumerate(o.qb):
+        assert np.array_equal(ctx.debug_qb(s), q), f"QB stream {s}"
+    assert np.array_equal(ctx.debug_recon().view(np.uint32), o.recon.ravel().view(np.uint32))
+    assert ctx.debug_pre_zstd() == o.pre_zstd
+    assert blob == o.asz
+    dec, _ = ctx.decompress(blob, data.shape, eb, api.default_params(block_pivot_ratio=bpr))
+    assert np.array_equal(dec.view(np.uint32), o.recon.view(np.uint32))
+    return rep
+
+
+def test_random_cases_against_oracle(gpu_ctx):
+    from asz_b200 import fields
+    rng = np.random.default_rng(99)
+    orders = ["120", "021", "012"]
+    for i in range(40):
+        shape = tuple(int(x) for x in rng.integers(7, 48, size=3))
+        f = fields.grf_field(shape, rng.uniform(1.2, 5), rng)
+        kind = i % 4
+        if kind == 1:
+            f[: shape[0] // 3] = 0.0
+        elif kind == 2:
+            f = np.round(f * 4) / 4
+        elif kind == 3:
+            f = f + 10 * np.tanh((np.arange(shape[2]) - shape[2] / 2) / 2)[None, None, :]
+        f = f.astype(np.float32)
+        plan = ",".join(f"cubic{rng.integers(0, 3)}_{orders[rng.integers(0, 3)]}" for _ in range(int(rng.integers(1, 10))))
+        family = ["cubic", "quintic"][int(rng.integers(0, 2))]
+        eb = float(10 ** rng.uniform(-5, -1.5))
+        bpr = int(rng.integers(1, 6))
+        _check_against_oracle(gpu_ctx, f, eb, plan, family, bpr)
+
+
+@pytest.mark.parametrize("family", ["cubic", "quintic"])
+def test_c2_like_128_cubic2_plan(gpu_ctx, family):
+    """The headline plan shape (cubic2_012 on every level, launcher block ratio 3) at 128^3."""
+    from asz_b200 import fields
+    f = fields.c2_field(shape=(128, 128, 128))
+    rep = _check_against_oracle(gpu_ctx, f, 1e-3, ",".join(["cubic2_012"] * 7), family, 3)
+    assert rep.t_fallback_count > 0
+
+
+def test_device_resident_input(gpu_ctx):
+    import torch
+
+    import asz_b200.api as api
+    case = golden_cases()[0]
+    data, blob, out = load_golden(case)
+    x = torch.from_numpy(data).cuda()
+    got, _ = gpu_ctx.compress(x, case["rel_eb"], case["plan"], case["family"],
+                              api.default_params(block_pivot_ratio=case["block_pivot_ratio"]))
+    assert got == blob
+    y = torch.empty_like(x)
+    gpu_ctx.decompress(blob, data.shape, case["rel_eb"], api.default_params(block_pivot_ratio=case["block_pivot_ratio"]),
+                       out=y)
+    torch.cuda.synchronize()
+    assert np.array_equal(y.cpu().numpy().view(np.uint32), out.view(np.uint32))
+
+
+@pytest.mark.parametrize("case", golden_cases()[:3], ids=lambda c: c["name"])
+def test_cli_drop_in(case):
+    data, blob, out = load_golden(case)
+    dims = [str(s) for s in data.shape]
+    with tempfile.TemporaryDirectory() as wd:
+        inp, z, o = os.path.join(wd, "in.f32"), os.path.join(wd, "x.asz"), os.path.join(wd, "x.out")
+        data.tofile(inp)
+        flags = ["--block-pivot-ratio", str(case["block_pivot_ratio"])]
+        r = subprocess.run([os.path.join(BIN, "s1_compress"), "-f", "-i", inp, "-z", z, "-3", *dims, "-M", "REL",
+                            repr(case["rel_eb"]), "--predictor-plan", case["plan"], "--predictor-family", case["family"],
+                            *flags], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert open(z, "rb").read() == blob
+        for line in ("Compression time:", "CR: ", "max_err=", "predictor_vec={", "Default slope statistics:"):
+            assert line in r.stdout
+        r = subprocess.run([os.path.join(BIN, "s1_decompress"), "-z", z, "-o", o, "-3", *dims, "-M", "REL",
+                            repr(case["rel_eb"]), *flags], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert np.array_equal(np.fromfile(o, np.float32), out.ravel())
+        assert "Decompression time:" in r.stdout and "CR= " in r.stdout
+
+
+def test_corrupt_streams_fail_cleanly(gpu_ctx):
+    import asz_b200.api as api
+    case = golden_cases()[0]
+    data, blob, out = load_golden(case)
+    p = api.default_params(block_pivot_ratio=case["block_pivot_ratio"])
+    for bad in (blob[: len(blob) // 2], b"\x00" * 16, blob[:-3]):
+        with pytest.raises(api.AszError):
+            gpu_ctx.decompress(bad, data.shape, case["rel_eb"], p)
+    # A well-formed stream decoded with the wrong block ratio still must not fault the device.
+    raw = O.compress(data, case["rel_eb"], case["plan"], case["family"] == "quintic",
+                     O.default_params(block_pivot_ratio=case["block_pivot_ratio"])).pre_zstd
+    assert len(raw) > 0
+    dec, _ = gpu_ctx.decompress(blob, data.shape, case["rel_eb"], p)
+    assert np.array_equal(dec.view(np.uint32), out.view(np.uint32))
