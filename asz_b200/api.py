@@ -100,6 +100,8 @@ def lib():
     L.asz_debug_t.argtypes = [C.c_void_p, C.c_void_p]
     L.asz_debug_recon.argtypes = [C.c_void_p, C.c_void_p]
     L.asz_debug_pre_zstd.argtypes = [C.c_void_p, C.c_void_p]
+    L.asz_debug_proxies.argtypes = [C.c_void_p, C.c_void_p]
+    L.asz_debug_proxies.restype = C.c_uint64
     _LIB = L
     return L
 
@@ -234,6 +236,14 @@ class Context:
         a = np.empty(n, np.float32)
         if n:
             self._L.asz_debug_recon(self._c, C.c_void_p(a.ctypes.data))
+        return a
+
+    def debug_proxies(self) -> np.ndarray:
+        """(rounds, blocks, 10) float32: h1 for the five t candidates, then the log10f arguments."""
+        n = self._L.asz_debug_proxies(self._c, None)
+        a = np.empty(n, np.float32)
+        if n:
+            self._L.asz_debug_proxies(self._c, C.c_void_p(a.ctypes.data))
         return a
 
     def debug_pre_zstd(self) -> bytes:

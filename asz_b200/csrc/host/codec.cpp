@@ -124,7 +124,7 @@ struct asz_ctx {
     std::string err;
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
-        classes, axis, pre, chunks, out;
+        classes, axis, pre, chunks, out, proxies;
     // Cached glibc log2f tables, keyed by sample count.
     std::map<uint32_t, uint32_t> log2_off;
     std::vector<float> log2_host;
@@ -501,7 +501,7 @@ void asz_destroy(asz_ctx *c) {
     cudaSetDevice(c->device);
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
-                      &c->out})
+                      &c->out, &c->proxies})
         b->release();
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
@@ -787,6 +787,8 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     CK(ctx->classes.reserve(27 * L * sizeof(ClassInfo)));
     const u64 amb_cap = 4096;
     CK(ctx->amb.reserve(amb_cap * sizeof(AmbiguousRecord)));
+    CK(ctx->proxies.reserve(G.nblocks * L * 10 * sizeof(float)));
+    CK(cudaMemsetAsync(ctx->proxies.p, 0xff, G.nblocks * L * 10 * sizeof(float), st));
     u64 *d_tabc = ctx->axis.as<u64>();
     u64 *d_tabp = d_tabc + G.tab_count.size();
     CK(cudaMemcpyAsync(d_tabc, G.tab_count.data(), G.tab_count.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
@@ -838,7 +840,8 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
             CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, ctx->classes.as<ClassInfo>() + 27 * l, d_rec, d_in,
                               ctx->log2arena.as<float>(), R2, t_default, ctx->scratch.as<uint8_t>(), sstride, capmax, bcap,
                               tcap, d_tval, d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap,
-                              &dm->amb_count, ctx->overrides.as<uint32_t>(), (uint32_t)(overrides.size() / 3), &dm->err, st));
+                              &dm->amb_count, ctx->overrides.as<uint32_t>(), (uint32_t)(overrides.size() / 3),
+                              ctx->proxies.as<float>() + G.nblocks * l * 10, &dm->err, st));
             }
             ProfScope ps(ctx, "round_compress", rg.targets * 12);
             CK(launch_round_compress(G.fg, rg, d_tabc, d_tabp, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
@@ -1302,6 +1305,13 @@ extern "C" uint64_t asz_debug_recon(asz_ctx *ctx, float *dst) {
     if (!ctx || !ctx->have_last) return 0;
     if (dst) cudaMemcpy(dst, ctx->rec.p, ctx->n_total * 4, cudaMemcpyDeviceToHost);
     return ctx->n_total;
+}
+
+extern "C" uint64_t asz_debug_proxies(asz_ctx *ctx, float *dst) {
+    if (!ctx || !ctx->have_last) return 0;
+    uint64_t n = ctx->t_len * 10;
+    if (dst) cudaMemcpy(dst, ctx->proxies.p, n * 4, cudaMemcpyDeviceToHost);
+    return n;
 }
 
 extern "C" uint64_t asz_debug_pre_zstd(asz_ctx *ctx, uint8_t *dst) {

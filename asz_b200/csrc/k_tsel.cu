@@ -43,44 +43,43 @@ struct Scratch {
     uint32_t cap, bcap, tcap;
 };
 
+// Lays out one group's arrays from `base` (8-byte aligned each) and returns the bytes used; with
+// base == nullptr it only measures. The host sizes the per-group stride with the same function.
+__host__ __device__ inline uint64_t carve_layout(uint8_t *base, uint32_t cap, uint32_t bcap, uint32_t tcap, Scratch *s) {
+    uint64_t off = 0;
+    auto take = [&](uint64_t bytes) {
+        uint8_t *r = base ? base + off : nullptr;
+        off += (bytes + 7) & ~7ull;
+        return r;
+    };
+    Scratch t;
+    t.ka = (int64_t *)take(8ull * cap);
+    t.kb = (int64_t *)take(8ull * cap);
+    t.hash = (uint64_t *)take(8ull * cap);
+    t.qk = (int64_t *)take(8ull * cap);
+    t.qc = (uint64_t *)take(8ull * cap);
+    t.cnt = (uint32_t *)take(4ull * cap);
+    t.nxt = (int32_t *)take(4ull * (cap + 1));
+    t.bkt = (int32_t *)take(4ull * bcap);
+    t.tab = (int32_t *)take(4ull * tcap);
+    t.ord = (int32_t *)take(4ull * cap);
+    t.qnxt = (int32_t *)take(4ull * (cap + 1));
+    t.qbkt = (int32_t *)take(4ull * bcap);
+    t.qtab = (int32_t *)take(4ull * tcap);
+    t.cap = cap;
+    t.bcap = bcap;
+    t.tcap = tcap;
+    if (s) *s = t;
+    return (off + 255) & ~255ull;
+}
+
 __host__ __device__ inline uint64_t scratch_bytes(uint32_t cap, uint32_t bcap, uint32_t tcap) {
-    uint64_t b = 0;
-    b += 2ull * 8 * cap;            // ka, kb
-    b += 4ull * cap;                // cnt
-    b += 8ull * cap;                // hash
-    b += 4ull * (cap + 1);          // nxt
-    b += 4ull * bcap;               // bkt
-    b += 4ull * tcap;               // tab
-    b += 4ull * cap;                // ord
-    b += 8ull * cap + 8ull * cap;   // qk, qc
-    b += 4ull * (cap + 1) + 4ull * bcap + 4ull * tcap;
-    return (b + 255) & ~255ull;
+    return carve_layout(nullptr, cap, bcap, tcap, nullptr);
 }
 
 __device__ inline Scratch carve(uint8_t *base, uint32_t cap, uint32_t bcap, uint32_t tcap) {
     Scratch s;
-    uint8_t *p = base;
-    auto take = [&](uint64_t bytes) {
-        uint8_t *r = p;
-        p += (bytes + 7) & ~7ull;
-        return r;
-    };
-    s.ka = (int64_t *)take(8ull * cap);
-    s.kb = (int64_t *)take(8ull * cap);
-    s.hash = (uint64_t *)take(8ull * cap);
-    s.qk = (int64_t *)take(8ull * cap);
-    s.qc = (uint64_t *)take(8ull * cap);
-    s.cnt = (uint32_t *)take(4ull * cap);
-    s.nxt = (int32_t *)take(4ull * (cap + 1));
-    s.bkt = (int32_t *)take(4ull * bcap);
-    s.tab = (int32_t *)take(4ull * tcap);
-    s.ord = (int32_t *)take(4ull * cap);
-    s.qnxt = (int32_t *)take(4ull * (cap + 1));
-    s.qbkt = (int32_t *)take(4ull * bcap);
-    s.qtab = (int32_t *)take(4ull * tcap);
-    s.cap = cap;
-    s.bcap = bcap;
-    s.tcap = tcap;
+    carve_layout(base, cap, bcap, tcap, &s);
     return s;
 }
 
@@ -242,7 +241,7 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
                                float *__restrict__ tval, int64_t *__restrict__ t_int, uint32_t *__restrict__ fb_count,
                                AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
                                const uint32_t *__restrict__ overrides, uint32_t n_overrides,
-                               uint32_t *__restrict__ err_word) {
+                               float *__restrict__ proxies, uint32_t *__restrict__ err_word) {
     const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (g >= nblocks) return;
@@ -295,6 +294,12 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
             const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
             float h1v[5], xv[5];
             for (int c = 0; c < 5; c++) eval_proxy(s, m, cand[c], rg.eb, rg.stat_eb, R2, l2, h1v[c], xv[c]);
+            if (proxies) {
+                for (int c = 0; c < 5; c++) {
+                    proxies[(g * 10) + c] = h1v[c];
+                    proxies[(g * 10) + 5 + c] = xv[c];
+                }
+            }
             // compress.tpp:127-142 with t starting at insufficient_sample_t (= 1/4).
             int best = 1;
             bool ambiguous = false;
@@ -302,7 +307,9 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
                 if (cand[c] == cand[best]) continue;
                 float d_h1 = __fsub_rn(h1v[best], h1v[c]);
                 bool accept;
-                if (__float_as_uint(xv[c]) == __float_as_uint(xv[best])) {
+                if (__float_as_uint(xv[c]) == __float_as_uint(xv[best]) && isfinite(xv[c]) && xv[c] > 0.0f) {
+                    // Same log10f argument: the PSNR difference is exactly 0. (For +inf, i.e. zero
+                    // error, it is inf - inf = NaN instead, and the candidate is rejected below.)
                     accept = __fmaf_rn(d_h1, rg.slope, 0.0f) > 0.0f;
                 } else {
                     PsnrBand pc = psnr_band(xv[c]), pb = psnr_band(xv[best]);
@@ -373,11 +380,12 @@ cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
                            const float *orig, const float *log2arena, float R2, float t_default, uint8_t *scratch,
                            uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap, float *tval, int64_t *t_int,
                            uint32_t *fb_count, AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
-                           const uint32_t *overrides, uint32_t n_overrides, uint32_t *err, cudaStream_t st) {
+                           const uint32_t *overrides, uint32_t n_overrides, float *proxies, uint32_t *err,
+                           cudaStream_t st) {
     uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     tsel_v0_kernel<<<(unsigned)((nb + 63) / 64), 64, 0, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, scratch,
                                                                scratch_stride, cap, bcap, tcap, tval, t_int, fb_count, amb,
-                                                               amb_cap, amb_count, overrides, n_overrides, err);
+                                                               amb_cap, amb_count, overrides, n_overrides, proxies, err);
     return cudaGetLastError();
 }
 

@@ -164,6 +164,9 @@ uint64_t asz_debug_qb(asz_ctx *ctx, uint32_t stream, int32_t *dst);
 uint64_t asz_debug_t(asz_ctx *ctx, int64_t *dst);
 uint64_t asz_debug_recon(asz_ctx *ctx, float *dst);
 uint64_t asz_debug_pre_zstd(asz_ctx *ctx, uint8_t *dst);
+/* Per (round, block): h1 of t = 1/16, 1/4, 9/32, 5/16, 11/32, then the five log10f arguments
+ * (10 floats per group, round-major; all-ones bits where the block fell back). */
+uint64_t asz_debug_proxies(asz_ctx *ctx, float *dst);
 
 #ifdef __cplusplus
 }
