@@ -54,7 +54,7 @@ class Report(C.Structure):
         ("max_err", C.c_float), ("psnr", C.c_float), ("cr", C.c_float), ("br", C.c_float),
         ("t_fallback_count", C.c_uint64), ("pre_zstd_len", C.c_uint64), ("asz_len", C.c_uint64),
         ("layer_num", C.c_uint64), ("slope_max_invalid_ratio", C.c_float), ("slope_fallback_reason", C.c_int32),
-        ("ambiguous_decisions", C.c_uint64), ("reruns", C.c_uint64),
+        ("ambiguous_decisions", C.c_uint64), ("reruns", C.c_uint64), ("exact_groups", C.c_uint64),
         ("pivot_stride", C.c_uint32 * 3), ("block_shape", C.c_uint32 * 3), ("block_num", C.c_uint32 * 3),
         ("quintic", C.c_int32), ("plan", C.c_char * (64 * 11 + 1)),
     ]
@@ -101,6 +101,7 @@ def lib():
     L.asz_debug_recon.argtypes = [C.c_void_p, C.c_void_p]
     L.asz_debug_pre_zstd.argtypes = [C.c_void_p, C.c_void_p]
     L.asz_debug_proxies.argtypes = [C.c_void_p, C.c_void_p]
+    L.asz_set_tsel_mode.argtypes = [C.c_void_p, C.c_int]
     L.asz_debug_proxies.restype = C.c_uint64
     _LIB = L
     return L
@@ -210,6 +211,10 @@ class Context:
                                     C.c_void_p(res.ctypes.data), 0, C.byref(rep))
         self._check(rc)
         return res, rep
+
+    def set_tsel_mode(self, mode: int):
+        """0: certified fast path + exact replay for the rest (default); 1: exact replay everywhere."""
+        self._check(self._L.asz_set_tsel_mode(self._c, int(mode)))
 
     def stats(self):
         m, ps = C.c_double(), C.c_double()

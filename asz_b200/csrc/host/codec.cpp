@@ -124,7 +124,8 @@ struct asz_ctx {
     std::string err;
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
-        classes, axis, pre, chunks, out, proxies;
+        classes, axis, pre, chunks, out, proxies, tlist;
+    int tsel_mode = 0;  // 0: certified fast path + exact path for the rest; 1: exact path for all groups
     // Cached glibc log2f tables, keyed by sample count.
     std::map<uint32_t, uint32_t> log2_off;
     std::vector<float> log2_host;
@@ -532,6 +533,7 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t fb;
     uint32_t amb_count;
     uint32_t changed;
+    uint32_t list_count[64];
     int32_t qb_range[2 * 64];
     float h1[3 * 64];
     float x[3 * 64];
@@ -806,7 +808,11 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     uint32_t bcap, tcap;
     u64 sstride;
     scratch_dims(capmax, bcap, tcap, sstride);
-    CK(ctx->scratch.reserve(G.nblocks * sstride));
+    // Exact-path scratch: one slot per thread; every group in exact mode, otherwise a pool that
+    // the listed groups share.
+    const u64 slots = ctx->tsel_mode == 1 ? G.nblocks : std::min<u64>(G.nblocks, 8192);
+    CK(ctx->scratch.reserve(slots * sstride));
+    CK(ctx->tlist.reserve(G.nblocks * sizeof(uint32_t)));
     const float Rg = mx - mn, R2 = Rg * Rg;
     const float t_default = 4.0f / 16;  // insufficient_sample_t (asz_param.hpp:206)
     int32_t init_range[2] = {INT32_MAX, INT32_MIN};
@@ -835,21 +841,36 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         }
         for (u64 l = 0; l < L; l++) {
             const RoundGeom &rg = G.rounds[l];
+            const ClassInfo *cls = ctx->classes.as<ClassInfo>() + 27 * l;
+            const uint32_t nov = (uint32_t)(overrides.size() / 3);
+            uint32_t *d_list = ctx->tlist.as<uint32_t>(), *d_lcount = &dm->list_count[l % 64];
+            if (ctx->tsel_mode == 0) {
+                ProfScope ps(ctx, "tsel_fast", 0);
+                CK(cudaMemsetAsync(d_lcount, 0, 4, st));
+                CK(launch_tsel_fast(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default, d_tval,
+                                    d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, st));
+            }
             {
-            ProfScope ps(ctx, "tsel", 0);
-            CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, ctx->classes.as<ClassInfo>() + 27 * l, d_rec, d_in,
-                              ctx->log2arena.as<float>(), R2, t_default, ctx->scratch.as<uint8_t>(), sstride, capmax, bcap,
-                              tcap, d_tval, d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap,
-                              &dm->amb_count, ctx->overrides.as<uint32_t>(), (uint32_t)(overrides.size() / 3),
-                              ctx->proxies.as<float>() + G.nblocks * l * 10, &dm->err, st));
+                ProfScope ps(ctx, "tsel_exact", 0);
+                CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default,
+                                  ctx->scratch.as<uint8_t>(), sstride, capmax, bcap, tcap, d_tval, d_tint, &dm->fb,
+                                  ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap, &dm->amb_count,
+                                  ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10,
+                                  ctx->tsel_mode == 0 ? d_list : nullptr, ctx->tsel_mode == 0 ? d_lcount : nullptr, slots,
+                                  &dm->err, st));
             }
             ProfScope ps(ctx, "round_compress", rg.targets * 12);
             CK(launch_round_compress(G.fg, rg, d_tabc, d_tabp, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
                                      &dm->qb_range[2 * (l + 1)], &dm->err, st));
         }
         uint32_t words[3];
+        uint32_t lcounts[64];
         CK(cudaMemcpyAsync(words, &dm->err, sizeof(words), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(lcounts, dm->list_count, sizeof(lcounts), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        R.exact_groups = 0;
+        if (ctx->tsel_mode == 0)
+            for (u64 l = 0; l < L; l++) R.exact_groups += lcounts[l % 64];
         if (words[0]) return fail(ctx, ASZ_E_DEVICE, "round kernels reported an internal error " + std::to_string(words[0]));
         fb_total = words[1];
         uint32_t namb = words[2];
@@ -1511,4 +1532,10 @@ extern "C" int64_t asz_check_hashorder(const int64_t *a, const int64_t *b, uint6
     uint32_t k = 0;
     for (int32_t p = nxt[m]; p != kNil && k < m; p = nxt[p]) order[k++] = firsts[p];
     return k == m ? (int64_t)m : -1;
+}
+
+extern "C" int asz_set_tsel_mode(asz_ctx *ctx, int mode) {
+    if (!ctx || mode < 0 || mode > 1) return ASZ_E_ARG;
+    ctx->tsel_mode = mode;
+    return ASZ_OK;
 }

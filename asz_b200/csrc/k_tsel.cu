@@ -241,10 +241,17 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
                                float *__restrict__ tval, int64_t *__restrict__ t_int, uint32_t *__restrict__ fb_count,
                                AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
                                const uint32_t *__restrict__ overrides, uint32_t n_overrides,
-                               float *__restrict__ proxies, uint32_t *__restrict__ err_word) {
+                               float *__restrict__ proxies, const uint32_t *__restrict__ list,
+                               const uint32_t *__restrict__ list_count, uint32_t *__restrict__ err_word) {
     const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (g >= nblocks) return;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    // With a list, each thread settles the listed groups tid, tid+nthreads, ... in its own scratch
+    // slot; without one, thread g settles group g.
+    const uint64_t items = list ? *list_count : nblocks;
+    for (uint64_t it = tid; it < items; it += nthreads) {
+    const uint64_t g = list ? list[it] : it;
+    if (g >= nblocks) continue;
     const uint64_t b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1],
                    b0 = g / (fg.block_num[1] * fg.block_num[2]);
     const uint64_t bb[3] = {b0, b1, b2};
@@ -279,12 +286,12 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
         box.neg_2_stat_eb = rg.neg_2_stat_eb;
         box.stat_eb = rg.stat_eb;
         box.n = ci.n;
-        Scratch s = carve(scratch + g * scratch_stride, cap, bcap, tcap);
+        Scratch s = carve(scratch + tid * scratch_stride, cap, bcap, tcap);
         FieldRef fr{rec, orig, fg.n[1] * fg.n[2], fg.n[2]};
         uint32_t m = ci.n == 0 ? 0 : build_abmap(box, fr, s);
         if (m == UINT32_MAX) {
             atomicOr(err_word, 1u);
-            return;
+            continue;
         }
         if (m == 0) {
             fb = true;
@@ -345,6 +352,7 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
     if (fb) atomicAdd(fb_count, 1u);
     tval[g] = best_t;
     t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(best_t, (float)fg.t_precision));
+    }
 }
 
 // Default-slope proxies: three AB maps (one per axis) over the original field, each evaluated
@@ -380,12 +388,12 @@ cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
                            const float *orig, const float *log2arena, float R2, float t_default, uint8_t *scratch,
                            uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap, float *tval, int64_t *t_int,
                            uint32_t *fb_count, AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
-                           const uint32_t *overrides, uint32_t n_overrides, float *proxies, uint32_t *err,
-                           cudaStream_t st) {
-    uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    tsel_v0_kernel<<<(unsigned)((nb + 63) / 64), 64, 0, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, scratch,
-                                                               scratch_stride, cap, bcap, tcap, tval, t_int, fb_count, amb,
-                                                               amb_cap, amb_count, overrides, n_overrides, proxies, err);
+                           const uint32_t *overrides, uint32_t n_overrides, float *proxies, const uint32_t *list,
+                           const uint32_t *list_count, uint64_t slots, uint32_t *err, cudaStream_t st) {
+    tsel_v0_kernel<<<(unsigned)((slots + 63) / 64), 64, 0, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default,
+                                                                  scratch, scratch_stride, cap, bcap, tcap, tval, t_int,
+                                                                  fb_count, amb, amb_cap, amb_count, overrides, n_overrides,
+                                                                  proxies, list, list_count, err);
     return cudaGetLastError();
 }
 

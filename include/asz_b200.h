@@ -92,6 +92,7 @@ typedef struct asz_report {
     int32_t slope_fallback_reason; /* 0 none, 1 invalid_ratio, 2 invalid_difference */
     uint64_t ambiguous_decisions; /* per-block t decisions re-checked on the host */
     uint64_t reruns;              /* compressions repeated after a host re-check */
+    uint64_t exact_groups;        /* (block, round) groups the certified fast path handed to the exact path */
     uint32_t pivot_stride[3], block_shape[3], block_num[3];
     int32_t quintic;
     char plan[64 * 11 + 1];       /* comma-separated predictor plan actually used */
@@ -139,6 +140,11 @@ typedef struct asz_profile_entry {
 } asz_profile_entry;
 
 int asz_profile_enable(asz_ctx *ctx, int on);
+
+/* Per-block coefficient selection strategy. 0 (default): a certified order-free fast path settles
+ * most (block, round) groups and the exact hash-order replay settles the rest. 1: the exact replay
+ * for every group. Both give the reference's choices; 1 exists to test the exact path alone. */
+int asz_set_tsel_mode(asz_ctx *ctx, int mode);
 /* Copies up to max entries accumulated since the last reset; returns how many exist. */
 int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset);
 

@@ -50,9 +50,11 @@ def _check_against_oracle(ctx, data, eb, plan, family, bpr):
     return rep
 
 
-def test_random_cases_against_oracle(gpu_ctx):
+@pytest.mark.parametrize("mode", [0, 1], ids=["fast+exact", "exact-only"])
+def test_random_cases_against_oracle(gpu_ctx, mode):
     from asz_b200 import fields
-    rng = np.random.default_rng(99)
+    gpu_ctx.set_tsel_mode(mode)
+    rng = np.random.default_rng(99 + mode)
     orders = ["120", "021", "012"]
     for i in range(40):
         shape = tuple(int(x) for x in rng.integers(7, 48, size=3))
@@ -70,6 +72,7 @@ def test_random_cases_against_oracle(gpu_ctx):
         eb = float(10 ** rng.uniform(-5, -1.5))
         bpr = int(rng.integers(1, 6))
         _check_against_oracle(gpu_ctx, f, eb, plan, family, bpr)
+    gpu_ctx.set_tsel_mode(0)
 
 
 @pytest.mark.parametrize("family", ["cubic", "quintic"])
