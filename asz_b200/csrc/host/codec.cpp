@@ -124,7 +124,7 @@ struct asz_ctx {
     std::string err;
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
-        classes, axis, pre, chunks, out, proxies, tlist;
+        classes, axis, pre, chunks, out, proxies, tlist, spill, iota;
     int tsel_mode = 0;  // 0: certified fast path + exact path for the rest; 1: exact path for all groups
     // Cached glibc log2f tables, keyed by sample count.
     std::map<uint32_t, uint32_t> log2_off;
@@ -436,6 +436,20 @@ void scratch_dims(uint32_t cap, uint32_t &bcap, uint32_t &tcap, u64 &stride) {
     stride = tsel_scratch_bytes(cap, bcap, tcap);
 }
 
+// Largest group (samples) the shared-memory exact kernel takes, within the per-CTA limit.
+uint32_t exact_cap() {
+    static uint32_t cap = 0;
+    if (!cap) {
+        int dev = 0, lim = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        uint32_t c = 2048;
+        while (c > 64 && exact_smem_bytes(c) + 2048 > (uint32_t)lim) c -= 64;
+        cap = c;
+    }
+    return cap;
+}
+
 // Replays one ambiguous decision with glibc log10f (compress.tpp:127-142).
 float replay_decision(const AmbiguousRecord &r, float slope) {
     const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
@@ -534,6 +548,8 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t amb_count;
     uint32_t changed;
     uint32_t list_count[64];
+    uint32_t spill_count[64];
+    uint32_t all_count;
     int32_t qb_range[2 * 64];
     float h1[3 * 64];
     float x[3 * 64];
@@ -631,9 +647,28 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
     CK(cudaMemcpyAsync(dm->evals, evals, sizeof(ProxyEval) * ne, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
     const float R = mx - mn;
-    ProfScope ps_slope(ctx, "slope", 0);
-    CK(launch_slope_v0(fg, dm->boxes, dm->evals, ne, d_in, ctx->log2arena.as<float>(), R * R, ctx->scratch.as<uint8_t>(),
-                       sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, ctx->stream));
+    // The shared-memory exact kernel when the maps fit; the serial kernel otherwise, or when a
+    // key exceeds int32 (the exact kernel then reports error bit 2).
+    bool serial = cap > exact_cap();
+    if (!serial) {
+        {
+            ProfScope ps_slope(ctx, "slope", 0);
+            CK(launch_slope_exact(dm->boxes, dm->evals, ne, d_in, dims[1] * dims[2], dims[2], ctx->log2arena.as<float>(),
+                                  R * R, dm->h1, dm->x, dm->m, &dm->err, exact_cap(), ctx->stream));
+        }
+        uint32_t e1 = 0;
+        CK(cudaMemcpyAsync(&e1, &dm->err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (e1) {
+            serial = true;
+            CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
+        }
+    }
+    if (serial) {
+        ProfScope ps_slope(ctx, "slope_serial", 0);
+        CK(launch_slope_v0(fg, dm->boxes, dm->evals, ne, d_in, ctx->log2arena.as<float>(), R * R, ctx->scratch.as<uint8_t>(),
+                           sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, ctx->stream));
+    }
     std::vector<float> h1(3 * ne), x(3 * ne);
     uint32_t m[3], errw;
     CK(cudaMemcpyAsync(h1.data(), dm->h1, 4 * 3 * ne, cudaMemcpyDeviceToHost, ctx->stream));
@@ -810,9 +845,18 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     scratch_dims(capmax, bcap, tcap, sstride);
     // Exact-path scratch: one slot per thread; every group in exact mode, otherwise a pool that
     // the listed groups share.
-    const u64 slots = ctx->tsel_mode == 1 ? G.nblocks : std::min<u64>(G.nblocks, 8192);
+    const u64 slots = std::min<u64>(G.nblocks, 2048);
     CK(ctx->scratch.reserve(slots * sstride));
     CK(ctx->tlist.reserve(G.nblocks * sizeof(uint32_t)));
+    CK(ctx->spill.reserve(G.nblocks * sizeof(uint32_t)));
+    if (ctx->tsel_mode == 1) {
+        std::vector<uint32_t> iota(G.nblocks);
+        for (u64 i = 0; i < G.nblocks; i++) iota[i] = (uint32_t)i;
+        CK(ctx->iota.reserve(G.nblocks * sizeof(uint32_t)));
+        CK(cudaMemcpyAsync(ctx->iota.p, iota.data(), G.nblocks * 4, cudaMemcpyHostToDevice, st));
+        uint32_t cnt = (uint32_t)G.nblocks;
+        CK(cudaMemcpyAsync(&dm->all_count, &cnt, 4, cudaMemcpyHostToDevice, st));
+    }
     const float Rg = mx - mn, R2 = Rg * Rg;
     const float t_default = 4.0f / 16;  // insufficient_sample_t (asz_param.hpp:206)
     int32_t init_range[2] = {INT32_MAX, INT32_MIN};
@@ -844,33 +888,48 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
             const ClassInfo *cls = ctx->classes.as<ClassInfo>() + 27 * l;
             const uint32_t nov = (uint32_t)(overrides.size() / 3);
             uint32_t *d_list = ctx->tlist.as<uint32_t>(), *d_lcount = &dm->list_count[l % 64];
+            uint32_t *d_spill = ctx->spill.as<uint32_t>(), *d_scount = &dm->spill_count[l % 64];
+            CK(cudaMemsetAsync(d_scount, 0, 4, st));
             if (ctx->tsel_mode == 0) {
                 ProfScope ps(ctx, "tsel_fast", 0);
                 CK(cudaMemsetAsync(d_lcount, 0, 4, st));
                 CK(launch_tsel_fast(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default, d_tval,
                                     d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, st));
+            } else {
+                d_list = ctx->iota.as<uint32_t>();
+                d_lcount = &dm->all_count;
             }
             {
                 ProfScope ps(ctx, "tsel_exact", 0);
+                CK(launch_tsel_exact(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default, d_tval,
+                                     d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap, &dm->amb_count,
+                                     ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10,
+                                     d_list, d_lcount, d_spill, d_scount, exact_cap(), 148, st));
+            }
+            {
+                ProfScope ps(ctx, "tsel_serial", 0);
                 CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default,
                                   ctx->scratch.as<uint8_t>(), sstride, capmax, bcap, tcap, d_tval, d_tint, &dm->fb,
                                   ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap, &dm->amb_count,
-                                  ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10,
-                                  ctx->tsel_mode == 0 ? d_list : nullptr, ctx->tsel_mode == 0 ? d_lcount : nullptr, slots,
-                                  &dm->err, st));
+                                  ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10, d_spill,
+                                  d_scount, slots, &dm->err, st));
             }
             ProfScope ps(ctx, "round_compress", rg.targets * 12);
             CK(launch_round_compress(G.fg, rg, d_tabc, d_tabp, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
                                      &dm->qb_range[2 * (l + 1)], &dm->err, st));
         }
         uint32_t words[3];
-        uint32_t lcounts[64];
+        uint32_t lcounts[64], scounts[64];
         CK(cudaMemcpyAsync(words, &dm->err, sizeof(words), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(lcounts, dm->list_count, sizeof(lcounts), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(scounts, dm->spill_count, sizeof(scounts), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         R.exact_groups = 0;
-        if (ctx->tsel_mode == 0)
-            for (u64 l = 0; l < L; l++) R.exact_groups += lcounts[l % 64];
+        R.serial_groups = 0;
+        for (u64 l = 0; l < L && l < 64; l++) {
+            if (ctx->tsel_mode == 0) R.exact_groups += lcounts[l];
+            R.serial_groups += scounts[l];
+        }
         if (words[0]) return fail(ctx, ASZ_E_DEVICE, "round kernels reported an internal error " + std::to_string(words[0]));
         fb_total = words[1];
         uint32_t namb = words[2];
@@ -933,12 +992,16 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
     CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
     unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
-    ProfScope ps_hist(ctx, "histogram", (G.nblocks * L) * 8 + N * 4);
-    if (so[0].count) CK(launch_histogram<int64_t>(d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off, st));
-    for (u64 s = 0; s <= L; s++)
-        if (so[s + 1].count)
-            CK(launch_histogram<int32_t>(d_qb + qb_off[s], qb_len[s], so[s + 1].lo, (u64)(so[s + 1].hi - so[s + 1].lo) + 1,
-                                         d_hist + so[s + 1].hist_off, st));
+    {
+        ProfScope ps_hist(ctx, "histogram", (G.nblocks * L) * 8 + N * 4);
+        if (so[0].count)
+            CK(launch_histogram<int64_t>(d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off,
+                                         st));
+        for (u64 s = 0; s <= L; s++)
+            if (so[s + 1].count)
+                CK(launch_histogram<int32_t>(d_qb + qb_off[s], qb_len[s], so[s + 1].lo, (u64)(so[s + 1].hi - so[s + 1].lo) + 1,
+                                             d_hist + so[s + 1].hist_off, st));
+    }
     std::vector<u64> hist(hist_total);
     if (hist_total) CK(cudaMemcpyAsync(hist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

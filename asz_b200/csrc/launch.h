@@ -61,6 +61,16 @@ cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t 
                              const float *orig, const float *log2arena, float R2, float t_default, float *tval,
                              int64_t *t_int, uint32_t *fb_count, uint32_t *list_out, uint32_t *list_count,
                              const uint32_t *overrides, uint32_t n_overrides, cudaStream_t st);
+uint32_t exact_smem_bytes(uint32_t cap);
+cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
+                              const float *orig, const float *log2arena, float R2, float t_default, float *tval,
+                              int64_t *t_int, uint32_t *fb_count, AmbiguousRecord *amb, uint32_t amb_cap,
+                              uint32_t *amb_count, const uint32_t *overrides, uint32_t n_overrides, float *proxies,
+                              const uint32_t *list, const uint32_t *list_count, uint32_t *spill, uint32_t *spill_count,
+                              uint32_t cap, unsigned grid, cudaStream_t st);
+cudaError_t launch_slope_exact(const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals, const float *orig,
+                               uint64_t n1n2, uint64_t n2, const float *log2arena, float R2, float *h1, float *x,
+                               uint32_t *m_out, uint32_t *err, uint32_t cap, cudaStream_t st);
 cudaError_t launch_slope_v0(const FieldGeom &fg, const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals,
                             const float *orig, const float *log2arena, float R2, uint8_t *scratch, uint64_t scratch_stride,
                             uint32_t cap, uint32_t bcap, uint32_t tcap, float *h1, float *x, uint32_t *m_out, uint32_t *err,

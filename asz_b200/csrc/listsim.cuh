@@ -40,6 +40,14 @@ ASZ_HD uint64_t sched_bkt(int i) {
 #endif
 }
 
+// Bucket count in use after `m` insertions.
+ASZ_HD uint64_t sched_buckets(uint64_t m) {
+    uint64_t b = 1;
+    for (int i = 0; i < kSchedLen; i++)
+        if (sched_at(i) <= m) b = sched_bkt(i);
+    return b;
+}
+
 // Emulated std::unordered_map list: nodes 0..count-1, sentinel (before_begin) at index `cap`.
 struct ListSim {
     int32_t *nxt, *bkt;

@@ -17,13 +17,6 @@ constexpr uint64_t kSchedBkt[kSchedLen] = {13, 29, 59, 127, 257, 541, 1109, 2357
                                            42043, 85229, 172933, 351061, 712697, 1447153, 2938679,
                                            5967347, 12117689, 24607243};
 
-// Bucket count in use after `m` insertions.
-ASZ_HD uint64_t sched_buckets(uint64_t m) {
-    uint64_t b = 1;
-    for (int i = 0; i < kSchedLen; i++)
-        if (kSchedAt[i] <= m) b = kSchedBkt[i];
-    return b;
-}
 
 // One AB map: the sample box of get_AB_map (c_codes/asz_core/get_AB_map.tpp:7-24) after
 // sampling_stride is applied. lo/hi bound the coordinates; step = stride * sampling_stride.

@@ -332,6 +332,7 @@ def main():
                 "includes": "H2D from pinned memory, all GPU stages, D2H of the stream, libzstd level 3"},
         "cr": float(4 * N / len(blob)), "bit_exact_roundtrip": bit_exact, "max_err_over_eb": max_err / rep.abs_eb,
         "t_fallback_count": int(rep.t_fallback_count), "ambiguous_decisions": int(rep.ambiguous_decisions),
+        "exact_groups": int(rep.exact_groups), "serial_groups": int(rep.serial_groups),
         "roofline": roofline, "profile": prof, "cpu_baseline": cpu, "clocks": clocks.summary(),
         "gpu_launches": int(sum(v["launches"] for v in prof.values())) if prof else None,
     }
