@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <optional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -63,6 +64,28 @@ struct DevBuf {
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
+    }
+};
+
+// Grow-only pinned host buffer: the stream before zstd is staged here, so the device<->host copies
+// of the Huffman payloads run at DMA speed straight into (or out of) their final positions.
+struct PinnedBuf {
+    uint8_t *p = nullptr;
+    size_t cap = 0, len = 0;
+    cudaError_t reserve(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes + bytes / 8, 4096);
+        cudaError_t e = cudaHostAlloc((void **)&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = len = 0;
     }
 };
 
@@ -135,7 +158,8 @@ struct asz_ctx {
     u64 t_len = 0, n_total = 0;
     const float *last_in = nullptr;   // device input of the last compress call
     float last_min = 0, last_max = 0;
-    std::vector<uint8_t> pre_zstd;
+    PinnedBuf pre_zstd;   // the last compress call's stream before zstd
+    PinnedBuf raw_in;     // decompress: the stream after zstd
     bool have_last = false;
     // Profiling (asz_profile_*).
     bool prof = false;
@@ -184,6 +208,23 @@ void prof_collect(asz_ctx *c) {
     c->pending.clear();
 }
 // RAII timer around one launch.
+// Host wall time of one phase of a call, recorded as "host:<phase>" while profiling is on.
+struct HostScope {
+    asz_ctx *c;
+    size_t slot = 0;
+    clk::time_point t0;
+    HostScope(asz_ctx *ctx, const char *name) : c(ctx) {
+        if (!c->prof) return;
+        slot = prof_slot(c, name);
+        t0 = clk::now();
+    }
+    ~HostScope() {
+        if (!c->prof) return;
+        c->prof_slots[slot].ms += 1000.0 * secs(t0, clk::now());
+        c->prof_slots[slot].launches++;
+    }
+};
+
 struct ProfScope {
     asz_ctx *c;
     cudaEvent_t a = nullptr, b = nullptr;
@@ -516,8 +557,11 @@ void asz_destroy(asz_ctx *c) {
     cudaSetDevice(c->device);
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
-                      &c->out, &c->proxies})
+                      &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota})
         b->release();
+    c->pre_zstd.release();
+    c->raw_in.release();
+    for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
 }
@@ -550,6 +594,7 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t list_count[64];
     uint32_t spill_count[64];
     uint32_t all_count;
+    uint32_t why[2];  // fast path hand-offs: [0] errors outside the histogram window, [1] undecided
     int32_t qb_range[2 * 64];
     float h1[3 * 64];
     float x[3 * 64];
@@ -787,7 +832,10 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     // Data range (s1_compress.cpp:131-138).
     auto t_range = clk::now();
     float mn, mx;
-    rc = compute_range(ctx, d_in, N, mn, mx);
+    {
+        HostScope hs(ctx, "host:range");
+        rc = compute_range(ctx, d_in, N, mn, mx);
+    }
     if (rc) return rc;
     R.data_range_s = secs(t_range, clk::now());
     if (mn == mx) return fail(ctx, ASZ_E_DATA, "max_val==min_val");
@@ -797,11 +845,15 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     const std::vector<float> cand = candidate_t(p);
     float slope, max_invalid = 0;
     int reason = 0;
-    rc = default_slope(ctx, d_in, dims, p, abs_eb, mn, mx, cand, slope, max_invalid, reason);
+    {
+        HostScope hs(ctx, "host:slope");
+        rc = default_slope(ctx, d_in, dims, p, abs_eb, mn, mx, cand, slope, max_invalid, reason);
+    }
     if (rc) return rc;
     R.default_slope_s = secs(t_slope, clk::now());
 
     auto t_core = clk::now();
+    std::optional<HostScope> hs_prep(std::in_place, ctx, "host:prepare");
     Geometry G;
     build_geometry(dims, plan, p, abs_eb, slope, quintic, G);
     u64 qb_sum = G.pivots;
@@ -868,9 +920,12 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     int32_t *d_qb = ctx->qb.as<int32_t>();
     float *d_tval = ctx->tval.as<float>();
     int64_t *d_tint = ctx->tint.as<int64_t>();
+    hs_prep.reset();
+    std::optional<HostScope> hs_rounds(std::in_place, ctx, "host:rounds");
     while (true) {
         // Error word, fallback count, ambiguity count, QB ranges.
         CK(cudaMemsetAsync(&dm->err, 0, 3 * sizeof(uint32_t), st));
+        CK(cudaMemsetAsync(dm->why, 0, sizeof(dm->why), st));
         for (u64 s = 0; s <= L; s++)
             CK(cudaMemcpyAsync(&dm->qb_range[2 * s], init_range, 8, cudaMemcpyHostToDevice, st));
         if (!overrides.empty()) {
@@ -894,7 +949,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
                 ProfScope ps(ctx, "tsel_fast", 0);
                 CK(cudaMemsetAsync(d_lcount, 0, 4, st));
                 CK(launch_tsel_fast(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default, d_tval,
-                                    d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, st));
+                                    d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, dm->why, st));
             } else {
                 d_list = ctx->iota.as<uint32_t>();
                 d_lcount = &dm->all_count;
@@ -923,7 +978,11 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         CK(cudaMemcpyAsync(words, &dm->err, sizeof(words), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(lcounts, dm->list_count, sizeof(lcounts), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(scounts, dm->spill_count, sizeof(scounts), cudaMemcpyDeviceToHost, st));
+        uint32_t why[2];
+        CK(cudaMemcpyAsync(why, dm->why, sizeof(why), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        R.exact_window = why[0];
+        R.exact_undecided = why[1];
         R.exact_groups = 0;
         R.serial_groups = 0;
         for (u64 l = 0; l < L && l < 64; l++) {
@@ -956,6 +1015,8 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     }
     R.reruns = (u64)reruns;
     R.t_fallback_count = fb_total;
+    hs_rounds.reset();
+    std::optional<HostScope> hs_codes(std::in_place, ctx, "host:codes");
 
     // ---- Huffman stage: t stream (int64) and L+1 QB streams (int32). ----
     auto t_huff = clk::now();
@@ -1043,6 +1104,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     CK(ctx->cubtmp.reserve(tmp_bytes));
     uint32_t *d_pay = ctx->payload.as<uint32_t>();
     CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
+    hs_codes.reset();
     for (u64 s = 0; s < nstreams; s++) {
         StreamOut &o = so[s];
         if (!o.count || o.code.maxval == 1) continue;
@@ -1055,18 +1117,15 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
             CK(launch_encode<int32_t>(d_qb + qb_off[s - 1], o.count, o.lo, d_codes + code_off[s], ctx->bitoff.as<u64>(),
                                       ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
     }
-    std::vector<uint32_t> pay(words_total);
-    auto t_d2h = clk::now();
-    if (words_total) CK(cudaMemcpyAsync(pay.data(), d_pay, words_total * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    R.d2h_s = secs(t_d2h, clk::now());
-    // Stream assembly (compress.tpp:233-291).
-    std::vector<uint8_t> &bs = ctx->pre_zstd;
-    bs.clear();
+    // Stream assembly (compress.tpp:233-291) in pinned memory: the host writes the headers and
+    // code trees while each payload is copied from the device straight into its place.
     u64 total_len = 9 + 2 * L;
     for (auto &o : so) total_len += 8 + (o.count ? o.code.save_size() + o.code.encode_size() : 0);
-    bs.resize(total_len);
-    uint8_t *w = bs.data();
+    PinnedBuf &pb = ctx->pre_zstd;
+    CK(pb.reserve(total_len));
+    pb.len = total_len;
+    uint8_t *const bs0 = pb.p;
+    uint8_t *w = bs0;
     std::memcpy(w, &mn, 4);
     std::memcpy(w + 4, &mx, 4);
     w[8] = (uint8_t)(L | 0x40 | (quintic ? 0x80 : 0));
@@ -1076,30 +1135,37 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         w[1] = (uint8_t)plan.pred[l][9];
         w += 2;
     }
-    for (u64 s = 0; s < nstreams; s++) {
-        const StreamOut &o = so[s];
-        for (int i = 0; i < 8; i++) w[i] = (uint8_t)(o.count >> (8 * i));
-        w += 8;
-        if (!o.count) continue;
-        write_tree(o.code, w);
-        w += o.code.save_size();
-        write_len_word(o.code, w);
-        w += 8;
-        if (o.code.maxval != 1) {
-            u64 nb = (o.code.bits + 7) >> 3;
-            std::memcpy(w, (const uint8_t *)(pay.data() + o.payload_word_off), nb);
-            w += nb;
+    auto t_d2h = clk::now();
+    {
+        HostScope hs(ctx, "host:assembly");
+        for (u64 s = 0; s < nstreams; s++) {
+            const StreamOut &o = so[s];
+            for (int i = 0; i < 8; i++) w[i] = (uint8_t)(o.count >> (8 * i));
+            w += 8;
+            if (!o.count) continue;
+            write_tree(o.code, w);
+            w += o.code.save_size();
+            write_len_word(o.code, w);
+            w += 8;
+            if (o.code.maxval != 1) {
+                u64 nb = (o.code.bits + 7) >> 3;
+                if (nb) CK(cudaMemcpyAsync(w, d_pay + o.payload_word_off, nb, cudaMemcpyDeviceToHost, st));
+                w += nb;
+            }
         }
+        CK(cudaStreamSynchronize(st));
     }
-    if ((u64)(w - bs.data()) != total_len) return fail(ctx, ASZ_E_DEVICE, "Huffman encoded size mismatch");
+    R.d2h_s = secs(t_d2h, clk::now());
+    if ((u64)(w - bs0) != total_len) return fail(ctx, ASZ_E_DEVICE, "Huffman encoded size mismatch");
     R.huffman_s = secs(t_huff, clk::now());
     R.core_s = secs(t_core, clk::now());
     // zstd level 3 (compress.tpp:294-299).
     auto t_z = clk::now();
-    size_t bound = ZSTD_compressBound(bs.size());
+    HostScope hs_z(ctx, "host:zstd");
+    size_t bound = ZSTD_compressBound(pb.len);
     uint8_t *z = (uint8_t *)std::malloc(bound ? bound : 1);
     if (!z) return fail(ctx, ASZ_E_DATA, "out of host memory");
-    size_t zl = ZSTD_compress(z, bound, bs.data(), bs.size(), 3);
+    size_t zl = ZSTD_compress(z, bound, pb.p, pb.len, 3);
     if (ZSTD_isError(zl)) {
         std::free(z);
         return fail(ctx, ASZ_E_DATA, std::string("ZSTD_compress: ") + ZSTD_getErrorName(zl));
@@ -1123,7 +1189,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         R.default_slope = slope;
         R.slope_max_invalid_ratio = max_invalid;
         R.slope_fallback_reason = reason;
-        R.pre_zstd_len = bs.size();
+        R.pre_zstd_len = pb.len;
         R.asz_len = zl;
         R.layer_num = L;
         R.quintic = quintic ? 1 : 0;
@@ -1239,17 +1305,23 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     unsigned long long raw = ZSTD_getFrameContentSize(in, len);
     if (raw == ZSTD_CONTENTSIZE_ERROR || raw == ZSTD_CONTENTSIZE_UNKNOWN || raw > (1ull << 40))
         return fail(ctx, ASZ_E_DATA, "ZSTD_decompress error in decompress()");
-    std::vector<uint8_t> bs(raw + 16, 0);
-    size_t got = ZSTD_decompress(bs.data(), raw, in, len);
+    CK(ctx->raw_in.reserve(raw + 16));
+    uint8_t *const bsp = ctx->raw_in.p;
+    std::memset(bsp + raw, 0, 16);
+    size_t got;
+    {
+        HostScope hs(ctx, "host:zstd");
+        got = ZSTD_decompress(bsp, raw, in, len);
+    }
     if (ZSTD_isError(got) || got != raw) return fail(ctx, ASZ_E_DATA, "ZSTD_decompress error in decompress()");
     R.zstd_s = secs(t_z, clk::now());
     auto t_h = clk::now();
     // Header (decompress.tpp:89-119).
     if (raw < 9) return fail(ctx, ASZ_E_DATA, "truncated header");
     float mn, mx;
-    std::memcpy(&mn, bs.data(), 4);
-    std::memcpy(&mx, bs.data() + 4, 4);
-    uint8_t flags = bs[8];
+    std::memcpy(&mn, bsp, 4);
+    std::memcpy(&mx, bsp + 4, 4);
+    uint8_t flags = bsp[8];
     u64 L = flags;
     bool quintic = p.predictor_family == ASZ_FAMILY_QUINTIC;
     if (flags & 0x40) {
@@ -1260,7 +1332,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     if (raw - pos < 2 * L) return fail(ctx, ASZ_E_DATA, "truncated header");
     std::string ptxt;
     for (u64 l = 0; l < L; l++) {
-        uint8_t a = bs[pos], o = bs[pos + 1];
+        uint8_t a = bsp[pos], o = bsp[pos + 1];
         if (a < '0' || a > '2' || o < '0' || o > '2') return fail(ctx, ASZ_E_DATA, "compressed stream contains an invalid predictor");
         ptxt += (l ? "," : "") + std::string("cubic") + (char)a + "_" + (o == '0' ? "120" : o == '1' ? "021" : "012");
         pos += 2;
@@ -1271,7 +1343,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     auto rd64 = [&](u64 &v) {
         if (raw - pos < 8) return false;
         v = 0;
-        for (int i = 0; i < 8; i++) v |= (u64)bs[pos + i] << (8 * i);
+        for (int i = 0; i < 8; i++) v |= (u64)bsp[pos + i] << (8 * i);
         pos += 8;
         return true;
     };
@@ -1281,7 +1353,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         if (!rd64(counts[s])) return fail(ctx, ASZ_E_DATA, "truncated stream length");
         if (!counts[s]) continue;
         std::string e;
-        if (!parse_stream(bs.data(), raw, pos, hp[s], e)) return fail(ctx, ASZ_E_DATA, e);
+        if (!parse_stream(bsp, raw, pos, hp[s], e)) return fail(ctx, ASZ_E_DATA, e);
     }
     const float abs_eb = rel_eb * (mx - mn);
     Geometry G;
@@ -1295,7 +1367,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     CK(ctx->misc.reserve(sizeof(MiscLayout)));
     CK(ctx->pre.reserve(raw + 16));
     auto t0 = clk::now();
-    CK(cudaMemcpyAsync(ctx->pre.p, bs.data(), raw + 16, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->pre.p, bsp, raw + 16, cudaMemcpyHostToDevice, st));
     R.h2d_s += secs(t0, clk::now());
     std::vector<u64> qoff(L + 1);
     u64 qtot = 0;
@@ -1305,6 +1377,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     }
     CK(ctx->tint.reserve(std::max<u64>(counts[0], 1) * 8));
     CK(ctx->qb.reserve(std::max<u64>(qtot, 1) * 4));
+    std::optional<HostScope> hs_dec(std::in_place, ctx, "host:huffman_decode");
     if (counts[0]) {
         rc = gpu_decode(ctx, hp[0], counts[0], ctx->pre.as<uint8_t>(), 0, ctx->tint.p, true, st);
         if (rc) return rc;
@@ -1314,9 +1387,11 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         rc = gpu_decode(ctx, hp[s + 1], counts[s + 1], ctx->pre.as<uint8_t>(), 0, ctx->qb.as<int32_t>() + qoff[s], false, st);
         if (rc) return rc;
     }
+    hs_dec.reset();
     R.huffman_s = secs(t_h, clk::now());
     // Reconstruction.
     auto t_core = clk::now();
+    std::optional<HostScope> hs_rec(std::in_place, ctx, "host:reconstruct");
     float *d_out = out;
     if (!out_on_device) {
         CK(ctx->rec.reserve(N * sizeof(float)));
@@ -1340,6 +1415,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     uint32_t errw;
     CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    hs_rec.reset();
     if (errw) return fail(ctx, ASZ_E_DEVICE, "reconstruction kernels reported an internal error");
     R.core_s = secs(t_core, clk::now());
     if (!out_on_device) {
@@ -1400,8 +1476,8 @@ extern "C" uint64_t asz_debug_proxies(asz_ctx *ctx, float *dst) {
 
 extern "C" uint64_t asz_debug_pre_zstd(asz_ctx *ctx, uint8_t *dst) {
     if (!ctx || !ctx->have_last) return 0;
-    if (dst) std::memcpy(dst, ctx->pre_zstd.data(), ctx->pre_zstd.size());
-    return ctx->pre_zstd.size();
+    if (dst && ctx->pre_zstd.len) std::memcpy(dst, ctx->pre_zstd.p, ctx->pre_zstd.len);
+    return ctx->pre_zstd.len;
 }
 
 extern "C" int asz_compress_stats(asz_ctx *ctx, double *max_err, double *psnr) {

@@ -9,7 +9,8 @@
 // - log10f: glibc's result is within 2.06 ulp of exact (measured over all floats); 3 ulp allowed.
 // A candidate comparison whose sign holds over the whole interval is decided here. A group with
 // any undecidable comparison goes to the exact path (k_tsel.cu), which replays the maps' order.
-// So does a group whose quantised errors span more than the histogram window. Groups whose A
+// So does a group whose quantised errors do not fit the histogram window (1024 bins per candidate,
+// placed on the exact bin range or, when that is wider, on the bin of the mean keys). Groups whose A
 // keys are all zero give every candidate identical sums, and keep t = 1/4 exactly.
 //
 // One warp per group; the sample positions follow get_AB_map's loops (get_AB_map.tpp:13-15).
@@ -22,8 +23,10 @@
 namespace asz {
 namespace {
 
-constexpr int kWin = 256;          // histogram window (quantised-error values) per candidate
+constexpr int kWin = 1024;         // histogram window (quantised-error values) per candidate
 constexpr int kWarpsPerBlock = 8;
+// Counts are 16-bit (a group has < 65536 samples), two per 32-bit word.
+constexpr int kWinWords = kWin / 2;
 
 __device__ __forceinline__ int class_of(uint64_t b, uint64_t nb) { return b == 0 ? 0 : (b == nb - 1 ? 2 : 1); }
 
@@ -98,15 +101,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                      const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
                      float R2, float t_default, float *__restrict__ tval, int64_t *__restrict__ t_int,
                      uint32_t *__restrict__ fb_count, uint32_t *__restrict__ list_out, uint32_t *__restrict__ list_count,
-                     const uint32_t *__restrict__ overrides, uint32_t n_overrides) {
-    __shared__ uint32_t hist_sh[kWarpsPerBlock][5][kWin];
+                     const uint32_t *__restrict__ overrides, uint32_t n_overrides, uint32_t *__restrict__ why) {
+    extern __shared__ uint32_t hist_dyn[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t(*hist)[kWin] = hist_sh[warp];
+    uint32_t(*hist)[kWinWords] = (uint32_t(*)[kWinWords])(hist_dyn + warp * 5 * kWinWords);
     const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
     const int d = rg.dir;
     for (int c = 0; c < 5; c++)
-        for (int i = lane; i < kWin; i += 32) hist[c][i] = 0;
+        for (int i = lane; i < kWinWords; i += 32) hist[c][i] = 0;
     __syncwarp();
     for (uint64_t g = (uint64_t)blockIdx.x * kWarpsPerBlock + warp; g < nblocks; g += (uint64_t)gridDim.x * kWarpsPerBlock) {
         const uint64_t b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1],
@@ -145,8 +148,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         }
         const uint32_t n = ci.n;
         const uint64_t n1 = fg.n[1], n2 = fg.n[2];
-        // Pass 1: key ranges and whether any A key is nonzero.
+        if (n > 0xffffu) {  // a bin count could overflow its 16-bit half word
+            if (lane == 0) {
+                list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
+                atomicAdd(&why[0], 1u);
+            }
+            continue;
+        }
+        // Pass 1: key ranges and sums, and whether any A key is nonzero.
         float afmin = INFINITY, afmax = -INFINITY, bfmin = INFINITY, bfmax = -INFINITY;
+        double asum = 0.0, bsum = 0.0;
         bool anz = false;
         for (uint32_t s = lane; s < n; s += 32) {
             float af, bf;
@@ -156,6 +167,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             afmax = fmaxf(afmax, af);
             bfmin = fminf(bfmin, bf);
             bfmax = fmaxf(bfmax, bf);
+            asum += (double)af;
+            bsum += (double)bf;
             anz |= nz;
         }
         for (int o = 16; o; o >>= 1) {
@@ -163,6 +176,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             afmax = fmaxf(afmax, __shfl_xor_sync(0xffffffffu, afmax, o));
             bfmin = fminf(bfmin, __shfl_xor_sync(0xffffffffu, bfmin, o));
             bfmax = fmaxf(bfmax, __shfl_xor_sync(0xffffffffu, bfmax, o));
+            asum += __shfl_xor_sync(0xffffffffu, asum, o);
+            bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
         }
         anz = __any_sync(0xffffffffu, anz);
         if (!anz) {
@@ -175,21 +190,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             continue;
         }
         const float eb = rg.eb, neg_eb = __fdiv_rn(0.5f, eb), eb2 = __fadd_rn(eb, eb);
+        // Histogram window per candidate: the exact bin range when it fits, else centred on the
+        // bin of the mean keys; samples outside it send the group to the exact path.
         int64_t qlo[5];
-        bool wide = false;
         for (int c = 0; c < 5; c++) {
             float t2 = __fadd_rn(cand[c], cand[c]);
             int64_t q0 = lround_f(__fmul_rn(cand_err(afmin, bfmin, t2, rg.stat_eb), neg_eb));
             int64_t q1 = lround_f(__fmul_rn(cand_err(afmax, bfmax, t2, rg.stat_eb), neg_eb));
-            qlo[c] = q0;
-            if (q1 - q0 >= kWin || q1 < q0) wide = true;
-        }
-        if (wide) {
-            if (lane == 0) list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
-            continue;
+            if (q1 >= q0 && (uint64_t)q1 - (uint64_t)q0 < (uint64_t)kWin) {
+                qlo[c] = q0;
+            } else {
+                float am = (float)(asum / n), bm = (float)(bsum / n);
+                qlo[c] = lround_f(__fmul_rn(cand_err(am, bm, t2, rg.stat_eb), neg_eb)) - kWin / 2;
+            }
         }
         // Pass 2: per-candidate sums and histograms.
         double S[5] = {0, 0, 0, 0, 0};
+        bool out = false;
         for (uint32_t s = lane; s < n; s += 32) {
             float af, bf;
             bool nz;
@@ -202,8 +219,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 float de = __fmaf_rn(-__ll2float_rn(q), eb2, err);
                 double dd = (double)de;
                 S[c] = __fma_rn(dd, dd, S[c]);
-                atomicAdd(&hist[c][(int)(q - qlo[c])], 1u);
+                const uint64_t bin = (uint64_t)q - (uint64_t)qlo[c];
+                if (bin < (uint64_t)kWin) atomicAdd(&hist[c][bin >> 1], 1u << (16 * (bin & 1)));
+                else out = true;
             }
+        }
+        out = __any_sync(0xffffffffu, out);
+        if (out) {
+            for (int c = 0; c < 5; c++)
+                for (int i = lane; i < kWinWords; i += 32) hist[c][i] = 0;
+            __syncwarp();
+            if (lane == 0) {
+                list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
+                atomicAdd(&why[0], 1u);
+            }
+            continue;
         }
         __syncwarp();
         const float nf = __ull2float_rn((uint64_t)n), r = __fdiv_rn(1.0f, nf);
@@ -214,12 +244,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         for (int c = 0; c < 5; c++) {
             double h = 0.0;
             uint32_t k = 0;
-            for (int i = lane; i < kWin; i += 32) {
-                uint32_t cnt = hist[c][i];
-                if (cnt) {
-                    float p = __fmul_rn(__ull2float_rn((uint64_t)cnt), r);
-                    h = __fma_rn(-(double)p, (double)l2[cnt], h);
-                    k++;
+            for (int i = lane; i < kWinWords; i += 32) {
+                uint32_t w = hist[c][i];
+                if (w) {
+                    uint32_t c0 = w & 0xffffu, c1 = w >> 16;
+                    if (c0) {
+                        float p = __fmul_rn(__ull2float_rn((uint64_t)c0), r);
+                        h = __fma_rn(-(double)p, (double)l2[c0], h);
+                        k++;
+                    }
+                    if (c1) {
+                        float p = __fmul_rn(__ull2float_rn((uint64_t)c1), r);
+                        h = __fma_rn(-(double)p, (double)l2[c1], h);
+                        k++;
+                    }
                     hist[c][i] = 0;
                 }
             }
@@ -272,6 +310,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             }
             if (!sure) {
                 list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
+                atomicAdd(&why[1], 1u);
             } else {
                 tval[g] = cand[best];
                 t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(cand[best], (float)fg.t_precision));
@@ -284,13 +323,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
                              const float *orig, const float *log2arena, float R2, float t_default, float *tval,
                              int64_t *t_int, uint32_t *fb_count, uint32_t *list_out, uint32_t *list_count,
-                             const uint32_t *overrides, uint32_t n_overrides, cudaStream_t st) {
+                             const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st) {
     uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     uint64_t blocks = (nb + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    tsel_fast_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, 0, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2,
-                                                                       t_default, tval, t_int, fb_count, list_out,
-                                                                       list_count, overrides, n_overrides);
+    const int smem = kWarpsPerBlock * 5 * kWinWords * 4;
+    cudaError_t e = cudaFuncSetAttribute(tsel_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    tsel_fast_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2,
+                                                                          t_default, tval, t_int, fb_count, list_out,
+                                                                          list_count, overrides, n_overrides, why);
     return cudaGetLastError();
 }
 

@@ -279,6 +279,18 @@ def main():
     L.asz_profile_enable(ctx._c, 0)
     prof = {entries[i].name.decode(): {"launches": entries[i].launches, "ms": entries[i].ms, "bytes": entries[i].bytes}
             for i in range(min(n, 64))}
+    # The same for one decompression.
+    L.asz_profile_enable(ctx._c, 1)
+    ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+    n = L.asz_profile_read(ctx._c, entries, 64, 1)
+    L.asz_profile_enable(ctx._c, 0)
+    prof_dec = {entries[i].name.decode(): {"launches": entries[i].launches, "ms": entries[i].ms, "bytes": entries[i].bytes}
+                for i in range(min(n, 64))}
+    # Host wall-time phases ("host:*") are reported apart from the device kernel families.
+    host_phases = {k[5:]: round(v["ms"], 3) for k, v in prof.items() if k.startswith("host:")}
+    host_phases_dec = {k[5:]: round(v["ms"], 3) for k, v in prof_dec.items() if k.startswith("host:")}
+    prof = {k: v for k, v in prof.items() if not k.startswith("host:")}
+    prof_dec = {k: v for k, v in prof_dec.items() if not k.startswith("host:")}
     # End to end from pinned host memory, including zstd.
     xh = x.cpu().pin_memory()
     xh_np = xh.numpy()
@@ -333,7 +345,10 @@ def main():
         "cr": float(4 * N / len(blob)), "bit_exact_roundtrip": bit_exact, "max_err_over_eb": max_err / rep.abs_eb,
         "t_fallback_count": int(rep.t_fallback_count), "ambiguous_decisions": int(rep.ambiguous_decisions),
         "exact_groups": int(rep.exact_groups), "serial_groups": int(rep.serial_groups),
-        "roofline": roofline, "profile": prof, "cpu_baseline": cpu, "clocks": clocks.summary(),
+        "exact_window": int(rep.exact_window), "exact_undecided": int(rep.exact_undecided),
+        "roofline": roofline, "profile": prof, "host_phases_ms": host_phases,
+        "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
+        "cpu_baseline": cpu, "clocks": clocks.summary(),
         "gpu_launches": int(sum(v["launches"] for v in prof.values())) if prof else None,
     }
     print(json.dumps(out))

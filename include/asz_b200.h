@@ -94,6 +94,8 @@ typedef struct asz_report {
     uint64_t reruns;              /* compressions repeated after a host re-check */
     uint64_t exact_groups;        /* (block, round) groups the certified fast path handed to the exact path */
     uint64_t serial_groups;       /* groups too large for the shared-memory exact kernel (serial kernel) */
+    uint64_t exact_window;        /* of exact_groups: errors spread wider than the fast path's histogram */
+    uint64_t exact_undecided;     /* of exact_groups: a comparison the fast path's bounds could not settle */
     uint32_t pivot_stride[3], block_shape[3], block_num[3];
     int32_t quintic;
     char plan[64 * 11 + 1];       /* comma-separated predictor plan actually used */
