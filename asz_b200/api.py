@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "libasz_b200.so")
 _LIB = None
 
 ASZ_FAMILY_AUTO, ASZ_FAMILY_CUBIC, ASZ_FAMILY_QUINTIC = -1, 0, 1
+ASZ_OK, ASZ_E_ARG, ASZ_E_DATA, ASZ_E_CUDA, ASZ_E_DEVICE, ASZ_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 
 
 class AszError(RuntimeError):
@@ -104,6 +105,8 @@ def lib():
     L.asz_debug_proxies.argtypes = [C.c_void_p, C.c_void_p]
     L.asz_set_tsel_mode.argtypes = [C.c_void_p, C.c_int]
     L.asz_debug_proxies.restype = C.c_uint64
+    L.asz_error_stats_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_char_p, C.c_size_t]
     _LIB = L
     return L
 
@@ -132,6 +135,26 @@ def _dims(shape):
 
 def _is_cuda_tensor(x):
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+def error_stats_noalloc(x, y, value_range: float):
+    """max |x - y| and PSNR of two equal-size float32 CUDA tensors, computed without allocating
+    (fixed library scratch). Runs on torch's current stream of x's device; returns (max_err, psnr)."""
+    import torch
+    if not (_is_cuda_tensor(x) and _is_cuda_tensor(y)) or x.dtype != torch.float32 or y.dtype != torch.float32:
+        raise ValueError("x and y must be float32 CUDA tensors")
+    if x.numel() != y.numel() or not x.is_contiguous() or not y.is_contiguous():
+        raise ValueError("x and y must be contiguous and of equal size")
+    m, ps = C.c_double(), C.c_double()
+    err = C.create_string_buffer(256)
+    with torch.cuda.device(x.device):
+        rc = lib().asz_error_stats_noalloc(C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), x.numel(),
+                                           float(value_range),
+                                           C.c_void_p(torch.cuda.current_stream(x.device).cuda_stream),
+                                           C.byref(m), C.byref(ps), err, 256)
+    if rc != ASZ_OK:
+        raise AszError(rc, err.value.decode(errors="replace"))
+    return m.value, ps.value
 
 
 class Context:

@@ -151,6 +151,21 @@ int asz_set_tsel_mode(asz_ctx *ctx, int mode);
 /* Copies up to max entries accumulated since the last reset; returns how many exist. */
 int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset);
 
+/* Error statistics of any reconstruction y of x (device pointers, n floats) that allocate nothing:
+ * max |x - y| and PSNR = 10 log10(value_range^2 / mse), the figures asz_compress_stats gives for
+ * the last compression. No reference counterpart: the reference computes these on the host inside
+ * compress() (compress.tpp:307-319); this is the device form for callers without a context or
+ * that must not allocate device memory. Scratch is a fixed 1 MiB device array in the library, so
+ * n is limited to 65520 * 65536 values; larger n returns ASZ_E_ARG with a message. Squared
+ * differences are summed in a fixed order, so repeated calls return identical bits.
+ * Runs on the current device and on cuda_stream (NULL: the legacy default stream) and waits for
+ * its result. The first call on a device looks up the scratch address (setup), so make it before
+ * any stream capture. Calls on one device share the scratch: overlapping calls (from several
+ * threads or streams) race and must be serialised by the caller. err (may be NULL) receives a
+ * message of at most err_len bytes. */
+int asz_error_stats_noalloc(const float *x, const float *y, uint64_t n, double value_range, void *cuda_stream,
+                            double *max_err, double *psnr, char *err, size_t err_len);
+
 /* Host-side self-check of the target geometry the round kernels use, for a field of the given
  * dims, plan and block ratio (no GPU involved): every stencil and sampling read is in bounds
  * and hits a value written in an earlier round, every point is written once, and the QB index
