@@ -49,6 +49,28 @@ struct RoundGeom {
     uint64_t total[3];       // sum of per-block counts along each axis
     uint64_t qb_total;       // QBs of this round (stream length)
     uint32_t fallback_all;   // 1 when every block falls back to the default t
+    uint64_t ent_off[3];     // offset of this round's per-axis AxisEntry tables, per axis
+};
+
+// Stencil forms of one target along the round axis (compress.tpp:7-34), decided by its index i,
+// the half stride and the block's right bound.
+enum StencilCase : uint32_t {
+    kStencilCubic = 0,    // interior 1D4R with the block's t
+    kStencilQuintic = 1,  // interior 1D6R
+    kStencilLeft1 = 2,    // i <= hs, only x-1 inside
+    kStencilLeft2 = 3,    // i <= hs, x-1 and x1
+    kStencilLeft3 = 4,    // i <= hs, x-1, x1, x3
+    kStencilRight1 = 5,   // i + hs >= right
+    kStencilRight2 = 6,   // i + 3hs >= right
+};
+
+// What a round's target geometry needs along one axis, for lattice index k on that axis: the
+// coordinate, the owning block, the index inside the block's QB box, the box extent and the
+// exclusive prefix of box extents before the block. Along the round axis, also the stencil case.
+struct AxisEntry {
+    uint32_t ii, bb, jj, cc;
+    uint64_t pre;
+    uint32_t stencil, pad;
 };
 
 struct FieldGeom {

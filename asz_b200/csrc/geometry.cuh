@@ -45,5 +45,45 @@ ASZ_HD Target locate(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, ui
     return t;
 }
 
+ASZ_HD uint32_t stencil_case(uint64_t i, uint64_t hs, uint64_t right, bool quintic) {
+    if (quintic && i >= 5 * hs && i + 5 * hs < right) return kStencilQuintic;
+    if (i <= hs) {
+        if (i + hs >= right) return kStencilLeft1;
+        if (i + 3 * hs >= right) return kStencilLeft2;
+        return kStencilLeft3;
+    }
+    if (i + hs >= right) return kStencilRight1;
+    if (i + 3 * hs >= right) return kStencilRight2;
+    return kStencilCubic;
+}
+
+// The per-axis part of locate() for lattice index k along axis a.
+ASZ_HD AxisEntry axis_entry(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, int a, uint64_t k) {
+    AxisEntry e{};
+    const uint64_t ii = a == rg.dir ? rg.hs + 2 * rg.hs * k : rg.stride[a] * k;
+    const uint64_t bb = owner_block(ii, fg.block_shape[a]);
+    const uint64_t start = bb * fg.block_shape[a] + (a == rg.dir ? rg.hs : (bb == 0 ? 0 : rg.stride[a]));
+    e.ii = (uint32_t)ii;
+    e.bb = (uint32_t)bb;
+    e.jj = (uint32_t)((ii - start) / rg.stride[a]);
+    e.cc = (uint32_t)at.count[rg.axis_off[a] + bb];
+    e.pre = at.prefix[rg.axis_off[a] + bb];
+    if (a == rg.dir) {
+        const uint64_t r = (bb + 1) * fg.block_shape[a] + 1;
+        e.stencil = stencil_case(ii, rg.hs, r < fg.n[a] ? r : fg.n[a], fg.quintic != 0);
+    }
+    return e;
+}
+
+// Serialised QB index of the target with per-axis entries e0, e1, e2 (get_qb_index,
+// asz_param.hpp:122-129, after the block's base offset).
+ASZ_HD uint64_t qb_index(const RoundGeom &rg, const AxisEntry &e0, const AxisEntry &e1, const AxisEntry &e2) {
+    const uint64_t base = e0.pre * rg.total[1] * rg.total[2] + (uint64_t)e0.cc * e1.pre * rg.total[2] +
+                          (uint64_t)e0.cc * e1.cc * e2.pre;
+    const uint64_t local = rg.order == 0 ? ((uint64_t)e1.jj * e2.cc + e2.jj) * e0.cc + e0.jj
+                         : rg.order == 1 ? ((uint64_t)e0.jj * e2.cc + e2.jj) * e1.cc + e1.jj
+                                         : ((uint64_t)e0.jj * e1.cc + e1.jj) * e2.cc + e2.jj;
+    return base + local;
+}
 
 }  // namespace asz

@@ -24,6 +24,7 @@
 #include <limits>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../geometry.cuh"
@@ -133,6 +134,7 @@ struct Geometry {
     FieldGeom fg{};
     std::vector<RoundGeom> rounds;
     std::vector<u64> tab_count, tab_prefix;     // per round, per axis, per block
+    std::vector<AxisEntry> ent;                 // per round, per axis, per lattice index
     std::vector<std::vector<ClassInfo>> classes;
     std::vector<uint32_t> cap;                  // max samples per round
     PivotGeom pg{};
@@ -314,6 +316,10 @@ int validate_dims(asz_ctx *ctx, const uint64_t dims[3], float rel_eb) {
 }
 
 // Plan geometry (generate_config.tpp:52-68) and per-round tables.
+// The round kernels index lines (k0, k1) and positions along axis 2 in 32 bits, and the axis
+// tables store coordinates and box extents in 32 bits.
+bool kernel_limits_ok(const struct Geometry &G);
+
 void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &p, float abs_eb, float default_slope,
                     bool quintic, Geometry &G) {
     FieldGeom &fg = G.fg;
@@ -350,6 +356,7 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
     G.cap.assign(L, 0);
     G.tab_count.clear();
     G.tab_prefix.clear();
+    G.ent.clear();
     for (u64 l = 0; l < L; l++) {
         RoundGeom &rg = G.rounds[l];
         const int d = plan.dir[l];
@@ -385,6 +392,14 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
             }
             rg.total[a] = sum;
             rg.qb_total *= sum;
+        }
+        // Per-axis target tables for the round kernels.
+        {
+            AxisTables at{G.tab_count.data(), G.tab_prefix.data()};
+            for (int a = 0; a < 3; a++) {
+                rg.ent_off[a] = G.ent.size();
+                for (u64 k = 0; k < rg.tcount[a]; k++) G.ent.push_back(axis_entry(fg, rg, at, a, k));
+            }
         }
         // Block classes for coefficient selection (compress.tpp:96-116, get_AB_map.tpp:9-12).
         bool all_fb = true;
@@ -440,6 +455,17 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
         rg.fallback_all = all_fb ? 1 : 0;
         stride[d] /= 2;
     }
+}
+
+bool kernel_limits_ok(const Geometry &G) {
+    for (int a = 0; a < 3; a++)
+        if (G.fg.n[a] >= (1ull << 32)) return false;
+    for (const RoundGeom &rg : G.rounds) {
+        if (rg.tcount[0] * rg.tcount[1] >= (1ull << 32) || rg.tcount[2] >= (1ull << 32)) return false;
+        for (int a = 0; a < 3; a++)
+            if (rg.total[a] >= (1ull << 32)) return false;
+    }
+    return true;
 }
 
 // glibc log2f(freq * (1/n)) for freq = 0..n (index 0 unused), cached per n.
@@ -793,6 +819,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
                             const asz_params *pp, const char *plan_text, uint8_t **out, size_t *out_len, asz_report *rep) {
     if (!ctx) return ASZ_E_ARG;
     auto t_start = clk::now();
+    const uint64_t launches0 = launch_counter();
     ctx->err.clear();
     ctx->have_last = false;
     if (!in || !out || !out_len) return fail(ctx, ASZ_E_ARG, "null argument");
@@ -856,6 +883,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     std::optional<HostScope> hs_prep(std::in_place, ctx, "host:prepare");
     Geometry G;
     build_geometry(dims, plan, p, abs_eb, slope, quintic, G);
+    if (!kernel_limits_ok(G)) return fail(ctx, ASZ_E_UNSUPPORTED, "field too large for the round kernels' 32-bit line indexing");
     u64 qb_sum = G.pivots;
     for (auto &rg : G.rounds) qb_sum += rg.qb_total;
     if (qb_sum != N) return fail(ctx, ASZ_E_DATA, "total_qb_num!=data.size()");
@@ -872,16 +900,14 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     CK(ctx->qb.reserve(std::max<u64>(acc, 1) * sizeof(int32_t)));
     CK(ctx->tval.reserve(G.nblocks * sizeof(float)));
     CK(ctx->tint.reserve(G.nblocks * L * sizeof(int64_t)));
-    CK(ctx->axis.reserve(2 * G.tab_count.size() * sizeof(u64)));
+    CK(ctx->axis.reserve(std::max<size_t>(G.ent.size(), 1) * sizeof(AxisEntry)));
     CK(ctx->classes.reserve(27 * L * sizeof(ClassInfo)));
     const u64 amb_cap = 4096;
     CK(ctx->amb.reserve(amb_cap * sizeof(AmbiguousRecord)));
     CK(ctx->proxies.reserve(G.nblocks * L * 10 * sizeof(float)));
     CK(cudaMemsetAsync(ctx->proxies.p, 0xff, G.nblocks * L * 10 * sizeof(float), st));
-    u64 *d_tabc = ctx->axis.as<u64>();
-    u64 *d_tabp = d_tabc + G.tab_count.size();
-    CK(cudaMemcpyAsync(d_tabc, G.tab_count.data(), G.tab_count.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d_tabp, G.tab_prefix.data(), G.tab_prefix.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+    const AxisEntry *d_ent = ctx->axis.as<AxisEntry>();
+    CK(cudaMemcpyAsync(ctx->axis.p, G.ent.data(), G.ent.size() * sizeof(AxisEntry), cudaMemcpyHostToDevice, st));
     for (u64 l = 0; l < L; l++)
         for (auto &ci : G.classes[l])
             if (ci.n) ci.log2_off = log2_table(ctx, ci.n);
@@ -946,7 +972,23 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
             uint32_t *d_spill = ctx->spill.as<uint32_t>(), *d_scount = &dm->spill_count[l % 64];
             CK(cudaMemsetAsync(d_scount, 0, 4, st));
             if (ctx->tsel_mode == 0) {
-                ProfScope ps(ctx, "tsel_fast", 0);
+                // Algorithmic bytes: one read of the 5 operands (4 neighbours + original) per sample.
+                u64 sample_bytes = 0;
+                if (ctx->prof) {
+                    u64 per_axis[3][3];
+                    for (int a = 0; a < 3; a++) {
+                        const u64 nb = G.fg.block_num[a];
+                        per_axis[a][0] = 1;
+                        per_axis[a][1] = nb > 2 ? nb - 2 : 0;
+                        per_axis[a][2] = nb >= 2 ? 1 : 0;
+                    }
+                    for (int c = 0; c < 27; c++) {
+                        const ClassInfo &ci = G.classes[l][c];
+                        if (ci.fallback || !ci.n) continue;
+                        sample_bytes += per_axis[0][c / 9] * per_axis[1][(c / 3) % 3] * per_axis[2][c % 3] * ci.n * 20;
+                    }
+                }
+                ProfScope ps(ctx, "tsel_fast", sample_bytes);
                 CK(cudaMemsetAsync(d_lcount, 0, 4, st));
                 CK(launch_tsel_fast(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default, d_tval,
                                     d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, dm->why, st));
@@ -970,7 +1012,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
                                   d_scount, slots, &dm->err, st));
             }
             ProfScope ps(ctx, "round_compress", rg.targets * 12);
-            CK(launch_round_compress(G.fg, rg, d_tabc, d_tabp, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
+            CK(launch_round_compress(G.fg, rg, d_ent, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
                                      &dm->qb_range[2 * (l + 1)], &dm->err, st));
         }
         uint32_t words[3];
@@ -1063,31 +1105,50 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
                 CK(launch_histogram<int32_t>(d_qb + qb_off[s], qb_len[s], so[s + 1].lo, (u64)(so[s + 1].hi - so[s + 1].lo) + 1,
                                              d_hist + so[s + 1].hist_off, st));
     }
+    std::optional<HostScope> hs_h(std::in_place, ctx, "host:codes_hist_d2h");
     std::vector<u64> hist(hist_total);
     if (hist_total) CK(cudaMemcpyAsync(hist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    hs_h.reset();
+    std::optional<HostScope> hs_b(std::in_place, ctx, "host:codes_build");
     // Codes (host) and payload layout.
     u64 code_total = 0, words_total = 0, max_count = 0;
     std::vector<u64> code_off(nstreams);
-    for (u64 s = 0; s < nstreams; s++) {
+    // Streams are independent: their codes are built on parallel host threads.
+    std::vector<std::string> code_err(nstreams);
+    std::vector<char> code_ok(nstreams, 1);
+    auto build_one = [&](u64 s) {
         StreamOut &o = so[s];
-        if (!o.count) continue;
+        if (!o.count) return;
         u64 range = (u64)(o.hi - o.lo) + 1;
-        std::vector<u64> h(hist.begin() + o.hist_off, hist.begin() + o.hist_off + range);
+        const u64 *h = hist.data() + o.hist_off;
         // Trim to the symbols present so the code's offset and range match the reference.
         u64 a = 0, b = range;
         while (a < b && h[a] == 0) a++;
         while (b > a && h[b - 1] == 0) b--;
-        std::vector<u64> hh(h.begin() + a, h.begin() + b);
-        std::string e;
-        if (!build_code(hh, o.lo + (int64_t)a, o.lo + (int64_t)b - 1, o.count, s == 0, o.code, e)) return fail(ctx, ASZ_E_UNSUPPORTED, e);
+        std::vector<u64> hh(h + a, h + b);
+        code_ok[s] = build_code(hh, o.lo + (int64_t)a, o.lo + (int64_t)b - 1, o.count, s == 0, o.code, code_err[s]);
         o.lo += (int64_t)a;
+    };
+    {
+        std::vector<std::thread> pool;
+        for (u64 s = 1; s < nstreams; s++)
+            if (so[s].count) pool.emplace_back(build_one, s);
+        build_one(0);
+        for (auto &t : pool) t.join();
+    }
+    for (u64 s = 0; s < nstreams; s++)
+        if (!code_ok[s]) return fail(ctx, ASZ_E_UNSUPPORTED, code_err[s]);
+    for (u64 s = 0; s < nstreams; s++) {
+        StreamOut &o = so[s];
+        if (!o.count) continue;
         code_off[s] = code_total;
         code_total += o.code.table.size();
         o.payload_word_off = words_total;
         words_total += (o.code.bits + 31) / 32 + 2;
         max_count = std::max(max_count, o.count);
     }
+    hs_b.reset();
     std::vector<CodeEntry> codes(std::max<u64>(code_total, 1));
     for (u64 s = 0; s < nstreams; s++)
         if (so[s].count) std::copy(so[s].code.table.begin(), so[s].code.table.end(), codes.begin() + code_off[s]);
@@ -1203,6 +1264,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         std::snprintf(R.plan, sizeof(R.plan), "%s", pl.c_str());
         R.cr = (float)N * sizeof(float) / (float)zl;
         R.br = 8 * sizeof(float) / R.cr;
+        R.kernel_launches = launch_counter() - launches0;
         R.total_s = secs(t_start, clk::now());
         *rep = R;
     }
@@ -1287,6 +1349,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
                               const asz_params *pp, float *out, int out_on_device, asz_report *rep) {
     if (!ctx) return ASZ_E_ARG;
     auto t_start = clk::now();
+    const uint64_t launches0 = launch_counter();
     ctx->err.clear();
     if (!in || !out) return fail(ctx, ASZ_E_ARG, "null argument");
     asz_params p;
@@ -1358,6 +1421,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     const float abs_eb = rel_eb * (mx - mn);
     Geometry G;
     build_geometry(dims, plan, p, abs_eb, 0.0f, quintic, G);
+    if (!kernel_limits_ok(G)) return fail(ctx, ASZ_E_UNSUPPORTED, "field too large for the round kernels' 32-bit line indexing");
     const u64 N = dims[0] * dims[1] * dims[2];
     if (counts[0] < G.nblocks * L) return fail(ctx, ASZ_E_DATA, "compressed stream contains too few t values");
     if (counts[1] < G.pivots) return fail(ctx, ASZ_E_DATA, "compressed stream has too few QBs");
@@ -1397,10 +1461,9 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         CK(ctx->rec.reserve(N * sizeof(float)));
         d_out = ctx->rec.as<float>();
     }
-    CK(ctx->axis.reserve(2 * G.tab_count.size() * sizeof(u64)));
-    u64 *d_tabc = ctx->axis.as<u64>(), *d_tabp = d_tabc + G.tab_count.size();
-    CK(cudaMemcpyAsync(d_tabc, G.tab_count.data(), G.tab_count.size() * 8, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d_tabp, G.tab_prefix.data(), G.tab_prefix.size() * 8, cudaMemcpyHostToDevice, st));
+    CK(ctx->axis.reserve(std::max<size_t>(G.ent.size(), 1) * sizeof(AxisEntry)));
+    const AxisEntry *d_ent = ctx->axis.as<AxisEntry>();
+    CK(cudaMemcpyAsync(ctx->axis.p, G.ent.data(), G.ent.size() * sizeof(AxisEntry), cudaMemcpyHostToDevice, st));
     MiscLayout *dm = ctx->misc.as<MiscLayout>();
     CK(cudaMemsetAsync(&dm->err, 0, 4, st));
     {
@@ -1409,7 +1472,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     }
     for (u64 l = 0; l < L; l++) {
         ProfScope ps(ctx, "round_decompress", G.rounds[l].targets * 8);
-        CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_tabc, d_tabp, ctx->tint.as<int64_t>(),
+        CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_ent, ctx->tint.as<int64_t>(),
                                    ctx->qb.as<int32_t>() + qoff[l + 1], d_out, &dm->err, st));
     }
     uint32_t errw;
@@ -1440,6 +1503,7 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
             R.block_shape[a] = (uint32_t)G.fg.block_shape[a];
             R.block_num[a] = (uint32_t)G.fg.block_num[a];
         }
+        R.kernel_launches = launch_counter() - launches0;
         R.total_s = secs(t_start, clk::now());
         *rep = R;
     }
@@ -1584,6 +1648,18 @@ extern "C" int64_t asz_check_geometry(const uint64_t dims[3], const char *plan_t
             if (t.pos >= N || t.qi >= rg.qb_total || used[t.qi] || t.block >= G.nblocks) {
                 bad++;
                 continue;
+            }
+            {
+                // The round kernels' table form of the same target.
+                const u64 T1 = rg.tcount[1], T2 = rg.tcount[2];
+                const u64 k2 = k % T2, line = k / T2, k0 = line / T1, k1 = line % T1;
+                const AxisEntry &e0 = G.ent[rg.ent_off[0] + k0], &e1 = G.ent[rg.ent_off[1] + k1], &e2 = G.ent[rg.ent_off[2] + k2];
+                const u64 pos = ((u64)e0.ii * fg.n[1] + e1.ii) * fg.n[2] + e2.ii;
+                const u64 blk = ((u64)e0.bb * fg.block_num[1] + e1.bb) * fg.block_num[2] + e2.bb;
+                const uint32_t sc = rg.dir == 0 ? e0.stencil : rg.dir == 1 ? e1.stencil : e2.stencil;
+                if (pos != t.pos || qb_index(rg, e0, e1, e2) != t.qi || blk != t.block ||
+                    sc != stencil_case(t.i, rg.hs, t.right, quintic != 0))
+                    bad++;
             }
             used[t.qi] = 1;
             if (ref_pos[t.qi] != t.pos) bad++;

@@ -1,6 +1,8 @@
 // Host side of the Huffman stage (see huffman_host.h).
 #include "huffman_host.h"
 
+#include <algorithm>
+
 #include <queue>
 #include <utility>
 
@@ -56,18 +58,35 @@ bool build_code(const std::vector<uint64_t> &hist, int64_t min_sym, int64_t max_
     const uint64_t n = c.n;
     c.left.assign(n, -1);
     c.right.assign(n, -1);
-    using pr = std::pair<uint64_t, uint64_t>;  // (node index, frequency)
-    auto cmp = [](const pr &u, const pr &v) { return u.second == v.second ? u.first > v.first : u.second > v.second; };
-    std::priority_queue<pr, std::vector<pr>, decltype(cmp)> q(cmp);
-    for (uint64_t i = 0; i < n; i++) q.push({i, freq[i]});
-    while (q.size() > 1) {
-        pr u = q.top();
-        q.pop();
-        pr v = q.top();
-        q.pop();
-        c.left.push_back((int32_t)u.first);
-        c.right.push_back((int32_t)v.first);
-        q.push({c.left.size() - 1, u.second + v.second});
+    // The reference pops a min-heap on (frequency, node index) (huffman.hpp:222-240). Merged
+    // weights come out nondecreasing and internal nodes are numbered after all leaves, so the
+    // leaves sorted by (frequency, index) and a FIFO of internal nodes in creation order give
+    // the same pops: at each step take the smaller front, the leaf on a frequency tie.
+    std::vector<uint32_t> order(n);
+    for (uint64_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+    std::sort(order.begin(), order.end(),
+              [&](uint32_t a, uint32_t b) { return freq[a] != freq[b] ? freq[a] < freq[b] : a < b; });
+    std::vector<uint64_t> ifreq;
+    ifreq.reserve(n);
+    uint64_t ia = 0, ib = 0;
+    auto pop = [&](uint64_t &node, uint64_t &f) {
+        if (ia < n && (ib == ifreq.size() || freq[order[ia]] <= ifreq[ib])) {
+            node = order[ia];
+            f = freq[order[ia]];
+            ia++;
+        } else {
+            node = n + ib;
+            f = ifreq[ib];
+            ib++;
+        }
+    };
+    for (uint64_t k = 0; k + 1 < n; k++) {
+        uint64_t u, fu, v, fv;
+        pop(u, fu);
+        pop(v, fv);
+        c.left.push_back((int32_t)u);
+        c.right.push_back((int32_t)v);
+        ifreq.push_back(fu + fv);
     }
     c.root = c.left.size() - 1;
     // dfs_vec (huffman.hpp:80-95): bit k of the code is the branch taken at depth k+1.

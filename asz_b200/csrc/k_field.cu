@@ -112,7 +112,7 @@ __global__ void pivot_decompress_kernel(PivotGeom pg, const int32_t *__restrict_
 }
 
 // ---------------------------------------------------------------------------------------------
-// Prediction (compress.tpp:7-34, decompress.tpp:6-33) in the emitted form:
+// Prediction (compress.tpp:7-34, decompress.tpp:6-33) in the emitted form, by stencil case:
 //   1D6R:            (float) fma(a*s5, fma(inner*s1, b*s3)) in double
 //   left, one ref:   x-1
 //   left, two refs:  (x-1 + x1) * 0.5
@@ -120,9 +120,10 @@ __global__ void pivot_decompress_kernel(PivotGeom pg, const int32_t *__restrict_
 //   right edge:      fmaf(x-1, 3, -x-3) * 0.5
 //   right second:    fmaf(x1, 3, fmaf(x-1, 6, -x-3)) * 0.125
 //   interior 1D4R:   p=(float)(s3*(0.25-t)); (float)fma(0.25+t, s1, p) in double
-__device__ __forceinline__ float predict(const float *__restrict__ c, uint64_t i, uint64_t hs, uint64_t right, uint64_t pos,
-                                         uint64_t dist, float t, bool quintic) {
-    if (quintic && i >= 5 * hs && i + 5 * hs < right) {
+__device__ __forceinline__ float predict_case(const float *__restrict__ c, uint64_t pos, uint64_t dist, uint32_t sc,
+                                              float t) {
+    switch (sc) {
+    case kStencilQuintic: {
         float s1 = __fadd_rn(c[pos - dist], c[pos + dist]);
         float s3 = __fadd_rn(c[pos - 3 * dist], c[pos + 3 * dist]);
         float s5 = __fadd_rn(c[pos - 5 * dist], c[pos + 5 * dist]);
@@ -131,73 +132,187 @@ __device__ __forceinline__ float predict(const float *__restrict__ c, uint64_t i
         acc = __fma_rn((double)s5, kQuinticA, acc);
         return __double2float_rn(acc);
     }
-    if (i <= hs) {
-        if (i + hs >= right) return c[pos - dist];
-        if (i + 3 * hs >= right) return __fmul_rn(__fadd_rn(c[pos - dist], c[pos + dist]), 0.5f);
+    case kStencilLeft1:
+        return c[pos - dist];
+    case kStencilLeft2:
+        return __fmul_rn(__fadd_rn(c[pos - dist], c[pos + dist]), 0.5f);
+    case kStencilLeft3:
         return __fmul_rn(__fsub_rn(__fmaf_rn(c[pos - dist], 3.0f, __fmul_rn(c[pos + dist], 6.0f)), c[pos + 3 * dist]), 0.125f);
-    }
-    if (i + hs >= right) return __fmul_rn(__fmaf_rn(c[pos - dist], 3.0f, -c[pos - 3 * dist]), 0.5f);
-    if (i + 3 * hs >= right)
+    case kStencilRight1:
+        return __fmul_rn(__fmaf_rn(c[pos - dist], 3.0f, -c[pos - 3 * dist]), 0.5f);
+    case kStencilRight2:
         return __fmul_rn(__fmaf_rn(c[pos + dist], 3.0f, __fmaf_rn(c[pos - dist], 6.0f, -c[pos - 3 * dist])), 0.125f);
-    float s3 = __fadd_rn(c[pos - 3 * dist], c[pos + 3 * dist]);
-    float s1 = __fadd_rn(c[pos - dist], c[pos + dist]);
-    double td = (double)t;
-    float p1 = __double2float_rn(__dmul_rn((double)s3, __dsub_rn(0.25, td)));
-    return __double2float_rn(__fma_rn(__dadd_rn(0.25, td), (double)s1, (double)p1));
+    default: {
+        float s3 = __fadd_rn(c[pos - 3 * dist], c[pos + 3 * dist]);
+        float s1 = __fadd_rn(c[pos - dist], c[pos + dist]);
+        double td = (double)t;
+        float p1 = __double2float_rn(__dmul_rn((double)s3, __dsub_rn(0.25, td)));
+        return __double2float_rn(__fma_rn(__dadd_rn(0.25, td), (double)s1, (double)p1));
+    }
+    }
+}
+
+__device__ __forceinline__ AxisEntry load_entry(const AxisEntry *e) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(e);
+    uint4 a = __ldg(p), b = __ldg(p + 1);
+    AxisEntry r;
+    r.ii = a.x;
+    r.bb = a.y;
+    r.jj = a.z;
+    r.cc = a.w;
+    r.pre = (uint64_t)b.x | ((uint64_t)b.y << 32);
+    r.stencil = b.z;
+    r.pad = b.w;
+    return r;
+}
+
+// The parts of qb_index() that depend only on the line (k0, k1); qi = base + mul * e2.pre + local.
+struct LineQB {
+    uint64_t base, mul;
+    uint32_t a, b;  // order 2: local = a * cc2 + jj2; order 0: (jj1 * cc2 + jj2) * cc0 + jj0; order 1 likewise
+};
+
+__device__ __forceinline__ LineQB line_qb(const RoundGeom &rg, const AxisEntry &e0, const AxisEntry &e1) {
+    LineQB q;
+    q.base = e0.pre * rg.total[1] * rg.total[2] + (uint64_t)e0.cc * e1.pre * rg.total[2];
+    q.mul = (uint64_t)e0.cc * e1.cc;
+    if (rg.order == 2) {
+        q.a = e0.jj * e1.cc + e1.jj;
+        q.b = 0;
+    } else if (rg.order == 0) {
+        q.a = e1.jj;  // times cc2, plus jj2, times cc0, plus jj0
+        q.b = 0;
+    } else {
+        q.a = e0.jj;
+        q.b = 0;
+    }
+    return q;
+}
+
+__device__ __forceinline__ uint64_t target_qb(const RoundGeom &rg, const LineQB &q, const AxisEntry &e0, const AxisEntry &e1,
+                                              const AxisEntry &e2) {
+    uint64_t local;
+    if (rg.order == 2) local = (uint64_t)q.a * e2.cc + e2.jj;
+    else if (rg.order == 0) local = ((uint64_t)q.a * e2.cc + e2.jj) * e0.cc + e0.jj;
+    else local = ((uint64_t)q.a * e2.cc + e2.jj) * e1.cc + e1.jj;
+    return q.base + q.mul * e2.pre + local;
+}
+
+// (diff * 0.5) / eb rounded to nearest, as far as lround of it is concerned: h * (1/eb) is within
+// 2^-51.4 relative of the correctly rounded quotient, so unless it lies within 2^-48 relative of a
+// rounding boundary of lround (a half-integer) both round to the same integer; the exact division
+// runs only in that band.
+__device__ __forceinline__ double quot_for_lround(double h, double eb, double rinv) {
+    const double qa = __dmul_rn(h, rinv);
+    const double aq = fabs(qa);
+    const double fr = aq - floor(aq);
+    if (aq < 0x1p50 && fabs(fr - 0.5) > aq * 0x1p-48 + 0x1p-60) return qa;
+    return __ddiv_rn(h, eb);
+}
+
+// Thread layout of the round kernels: the targets form lines along axis 2 (tcount[2] long, one
+// per (k0, k1)); a line is covered by tpl = 2^tpl_log2 threads and a CTA holds blockDim/tpl lines.
+// All per-target geometry comes from the per-axis tables, so no division is done per target.
+struct LineMap {
+    uint32_t sub, row, lines_per_cta;
+};
+
+__device__ __forceinline__ LineMap line_map(uint32_t tpl_log2) {
+    LineMap m;
+    m.sub = threadIdx.x & ((1u << tpl_log2) - 1);
+    m.row = threadIdx.x >> tpl_log2;
+    m.lines_per_cta = blockDim.x >> tpl_log2;
+    return m;
 }
 
 // Compress round: quantise the residual and write the reconstruction in place.
 // compress.tpp:35-37 as emitted: axis 0 multiplies by the hoisted 0.5*(1/eb) (inlined loop),
 // axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
-__global__ void round_compress_kernel(FieldGeom fg, RoundGeom rg, const uint64_t *__restrict__ tab_count,
-                                      const uint64_t *__restrict__ tab_prefix, const float *__restrict__ tval,
-                                      const float *__restrict__ in, float *__restrict__ rec, int32_t *__restrict__ qb,
-                                      int32_t *qb_range, uint32_t *err_word) {
-    AxisTables at{tab_count, tab_prefix};
-    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), r0 = __dmul_rn(__ddiv_rn(1.0, ebd), 0.5);
+__global__ void __launch_bounds__(256)
+    round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
+                          const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
+                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word) {
+    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd), r0 = __dmul_rn(rinv, 0.5);
+    const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
+    const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
+    const uint32_t lines = (uint32_t)rg.tcount[0] * T1;
+    const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
+    const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
+    const LineMap m = line_map(tpl_log2);
+    const int dir = rg.dir;
     int32_t lo = INT32_MAX, hi = INT32_MIN;
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < rg.targets; k += (uint64_t)gridDim.x * blockDim.x) {
-        Target tg = locate(fg, rg, at, k);
-        if (tg.qi >= rg.qb_total) {
-            atomicOr(err_word, 4u);
-            continue;
+    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += gridDim.x * m.lines_per_cta) {
+        const uint32_t k0 = line / T1, k1 = line - k0 * T1;
+        const AxisEntry e0 = load_entry(e0t + k0), e1 = load_entry(e1t + k1);
+        const uint64_t line_pos = (uint64_t)e0.ii * n1n2 + (uint64_t)e1.ii * n2;
+        const uint32_t line_blk = e0.bb * nb1 + e1.bb;
+        const LineQB lq = line_qb(rg, e0, e1);
+        for (uint32_t k2 = m.sub; k2 < T2; k2 += 1u << tpl_log2) {
+            const AxisEntry e2 = load_entry(e2t + k2);
+            const uint64_t pos = line_pos + e2.ii;
+            const uint64_t qi = target_qb(rg, lq, e0, e1, e2);
+            if (qi >= rg.qb_total) {
+                atomicOr(err_word, 4u);
+                continue;
+            }
+            const uint32_t sc = dir == 0 ? e0.stencil : dir == 1 ? e1.stencil : e2.stencil;
+            const float t = sc == kStencilCubic ? tval[(uint64_t)line_blk * nb2 + e2.bb] : 0.0f;
+            const float pred = predict_case(rec, pos, rg.dist, sc, t);
+            const double pd = (double)pred;
+            const double diff = __dsub_rn(pd, (double)in[pos]);
+            const double q = dir == 0 ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+            const int32_t v = (int32_t)lround_d(q);
+            qb[qi] = v;
+            rec[pos] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
+            lo = min(lo, v);
+            hi = max(hi, v);
         }
-        float pred = predict(rec, tg.i, rg.hs, tg.right, tg.pos, rg.dist, tval[tg.block], fg.quintic != 0);
-        double pd = (double)pred;
-        double diff = __dsub_rn(pd, (double)in[tg.pos]);
-        double q = rg.dir == 0 ? __dmul_rn(diff, r0) : __ddiv_rn(__dmul_rn(diff, 0.5), ebd);
-        int32_t v = (int32_t)lround_d(q);
-        qb[tg.qi] = v;
-        rec[tg.pos] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
-        lo = min(lo, v);
-        hi = max(hi, v);
     }
     for (int o = 16; o > 0; o >>= 1) {
         lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
         hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     }
-    if ((threadIdx.x & 31) == 0) {
+    if ((threadIdx.x & 31) == 0 && lo <= hi) {
         atomicMin(&qb_range[0], lo);
         atomicMax(&qb_range[1], hi);
     }
 }
 
 // Decompress round (decompress.tpp:34): value = fma(-qb, 2eb, pred) in double, t = t_int/t_precision.
-__global__ void round_decompress_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const uint64_t *__restrict__ tab_count,
-                                        const uint64_t *__restrict__ tab_prefix, const int64_t *__restrict__ t_int,
-                                        const int32_t *__restrict__ qb, float *__restrict__ rec, uint32_t *err_word) {
-    AxisTables at{tab_count, tab_prefix};
+__global__ void __launch_bounds__(256)
+    round_decompress_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
+                            const int64_t *__restrict__ t_int, const int32_t *__restrict__ qb, float *__restrict__ rec,
+                            uint32_t *err_word) {
     const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd);
     const float tp = (float)fg.t_precision;
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < rg.targets; k += (uint64_t)gridDim.x * blockDim.x) {
-        Target tg = locate(fg, rg, at, k);
-        if (tg.qi >= rg.qb_total) {
-            atomicOr(err_word, 4u);
-            continue;
+    const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
+    const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
+    const uint32_t lines = (uint32_t)rg.tcount[0] * T1;
+    const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
+    const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
+    const LineMap m = line_map(tpl_log2);
+    const int dir = rg.dir;
+    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += gridDim.x * m.lines_per_cta) {
+        const uint32_t k0 = line / T1, k1 = line - k0 * T1;
+        const AxisEntry e0 = load_entry(e0t + k0), e1 = load_entry(e1t + k1);
+        const uint64_t line_pos = (uint64_t)e0.ii * n1n2 + (uint64_t)e1.ii * n2;
+        const uint32_t line_blk = e0.bb * nb1 + e1.bb;
+        const LineQB lq = line_qb(rg, e0, e1);
+        for (uint32_t k2 = m.sub; k2 < T2; k2 += 1u << tpl_log2) {
+            const AxisEntry e2 = load_entry(e2t + k2);
+            const uint64_t pos = line_pos + e2.ii;
+            const uint64_t qi = target_qb(rg, lq, e0, e1, e2);
+            if (qi >= rg.qb_total) {
+                atomicOr(err_word, 4u);
+                continue;
+            }
+            const uint32_t sc = dir == 0 ? e0.stencil : dir == 1 ? e1.stencil : e2.stencil;
+            float t = 0.0f;
+            if (sc == kStencilCubic)
+                t = __fdiv_rn(__ll2float_rn(t_int[((uint64_t)line_blk * nb2 + e2.bb) * fg.layer_num + l]), tp);
+            const float pred = predict_case(rec, pos, rg.dist, sc, t);
+            rec[pos] = __double2float_rn(__fma_rn(-(double)qb[qi], eb2, (double)pred));
         }
-        float t = __fdiv_rn(__ll2float_rn(t_int[tg.block * fg.layer_num + l]), tp);
-        float pred = predict(rec, tg.i, rg.hs, tg.right, tg.pos, rg.dist, t, fg.quintic != 0);
-        rec[tg.pos] = __double2float_rn(__fma_rn(-(double)qb[tg.qi], eb2, (double)pred));
     }
 }
 
@@ -218,12 +333,14 @@ cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long
     uint64_t ntail = n - 4 * n4;
     range_kernel<<<grid_for(n4 ? n4 : ntail, 256, 148 * 8), 256, 0, st>>>((const float4 *)x, n4, x + 4 * n4, ntail, out,
                                                                            nonfinite);
+    count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
                                    cudaStream_t st) {
     zero_first_last_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(x, n, first, last);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -231,28 +348,44 @@ cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *r
                                   cudaStream_t st) {
     uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
     pivot_compress_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, st>>>(pg, in, rec, qb, qb_range);
+    count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, float *rec, cudaStream_t st) {
     uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
     pivot_decompress_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, st>>>(pg, qb, rec);
+    count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const uint64_t *tab_count,
-                                  const uint64_t *tab_prefix, const float *tval, const float *in, float *rec, int32_t *qb,
-                                  int32_t *qb_range, uint32_t *err, cudaStream_t st) {
-    round_compress_kernel<<<grid_for(rg.targets, 256, 148 * 32), 256, 0, st>>>(fg, rg, tab_count, tab_prefix, tval, in, rec,
-                                                                                qb, qb_range, err);
+static uint32_t tpl_log2_for(uint64_t t2) {
+    uint32_t lg = 0;
+    while ((1ull << lg) < t2 && lg < 8) lg++;
+    return lg;
+}
+
+static unsigned round_grid(const RoundGeom &rg, uint32_t tpl_log2) {
+    const uint64_t lines = rg.tcount[0] * rg.tcount[1];
+    const uint64_t per_cta = 256u >> tpl_log2;
+    return grid_for(lines, (unsigned)per_cta, 148 * 32);
+}
+
+cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
+                                  const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, cudaStream_t st) {
+    if (rg.targets == 0) return cudaSuccess;
+    const uint32_t lg = tpl_log2_for(rg.tcount[2]);
+    round_compress_kernel<<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err);
+    count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const uint64_t *tab_count,
-                                    const uint64_t *tab_prefix, const int64_t *t_int, const int32_t *qb, float *rec,
-                                    uint32_t *err, cudaStream_t st) {
-    round_decompress_kernel<<<grid_for(rg.targets, 256, 148 * 32), 256, 0, st>>>(fg, rg, l, tab_count, tab_prefix, t_int, qb,
-                                                                                  rec, err);
+cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const AxisEntry *ent,
+                                    const int64_t *t_int, const int32_t *qb, float *rec, uint32_t *err, cudaStream_t st) {
+    if (rg.targets == 0) return cudaSuccess;
+    const uint32_t lg = tpl_log2_for(rg.tcount[2]);
+    round_decompress_kernel<<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, l, ent, lg, t_int, qb, rec, err);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -285,6 +418,14 @@ __global__ void error_stats_kernel(const float *__restrict__ x, const float *__r
 cudaError_t launch_error_stats(const float *x, const float *y, uint64_t n, unsigned int *max_bits, double *sse,
                                cudaStream_t st) {
     error_stats_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(x, y, n, max_bits, sse);
+    count_launch();
     return cudaGetLastError();
+}
+}  // namespace asz
+
+namespace asz {
+uint64_t &launch_counter() {
+    thread_local uint64_t count = 0;
+    return count;
 }
 }  // namespace asz

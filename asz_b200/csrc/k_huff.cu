@@ -181,6 +181,7 @@ cudaError_t launch_histogram(const T *s, uint64_t n, int64_t offset, uint64_t ra
     size_t sh = range <= 8192 ? range * sizeof(unsigned int) : 0;
     uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 8);
     histogram_kernel<T><<<(unsigned)blocks, 256, sh, st>>>(s, n, offset, range, hist);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -191,9 +192,11 @@ cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntr
     if (n == 0) return cudaSuccess;
     uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 16);
     code_len_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(s, n, offset, tab, bitoff);
+    count_launch();
     cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, bitoff, bitoff, (int64_t)n, st);
     if (e != cudaSuccess) return e;
     encode_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(s, n, offset, tab, bitoff, out);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -207,12 +210,14 @@ cudaError_t launch_decode_sync(const uint8_t *payload, uint64_t bit_begin, uint6
                                uint32_t *err, cudaStream_t st) {
     decode_sync_kernel<<<(unsigned)((nchunks + 127) / 128), 128, 0, st>>>(payload, bit_begin, bit_end, chunk_bits, nchunks,
                                                                            dt, start, end, count, err);
+    count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_decode_restart(uint64_t nchunks, const uint64_t *end, uint64_t *start, uint32_t *changed,
                                   cudaStream_t st) {
     decode_restart_kernel<<<(unsigned)((nchunks + 255) / 256), 256, 0, st>>>(nchunks, end, start, changed);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -222,6 +227,7 @@ cudaError_t launch_decode_write(const uint8_t *payload, uint64_t bit_begin, uint
                                 T *out, uint64_t nout, uint32_t *err, cudaStream_t st) {
     decode_write_kernel<T><<<(unsigned)((nchunks + 127) / 128), 128, 0, st>>>(payload, bit_begin, bit_end, chunk_bits,
                                                                                nchunks, dt, offset, start, off, out, nout, err);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -230,6 +236,7 @@ cudaError_t launch_fill(T *out, uint64_t n, T v, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 16);
     fill_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(out, n, v);
+    count_launch();
     return cudaGetLastError();
 }
 

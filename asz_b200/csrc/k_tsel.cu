@@ -394,6 +394,7 @@ cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
                                                                   scratch, scratch_stride, cap, bcap, tcap, tval, t_int,
                                                                   fb_count, amb, amb_cap, amb_count, overrides, n_overrides,
                                                                   proxies, list, list_count, err);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -403,6 +404,7 @@ cudaError_t launch_slope_v0(const FieldGeom &fg, const SampleBox *boxes, const P
                             cudaStream_t st) {
     slope_v0_kernel<<<1, 32, 0, st>>>(fg, boxes, evals, n_evals, orig, log2arena, R2, scratch, scratch_stride, cap, bcap, tcap,
                                       h1, x, m_out, err);
+    count_launch();
     return cudaGetLastError();
 }
 }  // namespace asz

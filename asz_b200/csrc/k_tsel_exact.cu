@@ -556,6 +556,7 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
     tsel_exact_kernel<<<grid, kThreads, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int,
                                                      fb_count, amb, amb_cap, amb_count, overrides, n_overrides, proxies, list,
                                                      list_count, spill, spill_count, smem, cap);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -567,6 +568,7 @@ cudaError_t launch_slope_exact(const SampleBox *boxes, const ProxyEval *evals, u
     if (e != cudaSuccess) return e;
     slope_exact_kernel<<<3, kThreads, smem, st>>>(boxes, evals, n_evals, orig, n1n2, n2, log2arena, R2, h1, x, m_out, err,
                                                   smem, cap);
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -24,22 +24,10 @@ namespace asz {
 namespace {
 
 constexpr int kWin = 1024;         // histogram window (quantised-error values) per candidate
-constexpr int kWarpsPerBlock = 8;
 // Counts are 16-bit (a group has < 65536 samples), two per 32-bit word.
 constexpr int kWinWords = kWin / 2;
 
 __device__ __forceinline__ int class_of(uint64_t b, uint64_t nb) { return b == 0 ? 0 : (b == nb - 1 ? 2 : 1); }
-
-struct SampleGeo {
-    uint64_t lo[3], step[3];
-    uint32_t cnt[3];
-};
-
-__device__ __forceinline__ uint64_t sample_pos(const SampleGeo &sg, uint32_t s, uint64_t n1, uint64_t n2) {
-    uint32_t k2 = s % sg.cnt[2], k1 = (s / sg.cnt[2]) % sg.cnt[1], k0 = s / (sg.cnt[1] * sg.cnt[2]);
-    uint64_t i0 = sg.lo[0] + k0 * sg.step[0], i1 = sg.lo[1] + k1 * sg.step[1], i2 = sg.lo[2] + k2 * sg.step[2];
-    return (i0 * n1 + i1) * n2 + i2;
-}
 
 // AB keys of one sample (get_AB_map.tpp:18-21 as emitted), returned as the floats get_h1_psnr
 // converts them to.
@@ -93,25 +81,127 @@ __device__ Interval psnr_interval(double S, uint32_t n, float R2, float nf) {
     return iv;
 }
 
+
+// Quotient s / d for s * d < 2^32 with m = floor((2^32 - 1) / d) + 1 (d > 1): floor(s * m / 2^32)
+// is exact because the error term s * (m * d - 2^32) / (d * 2^32) stays below 1/d.
+struct SmallDiv {
+    uint32_t d, m;
+};
+
+__device__ __forceinline__ SmallDiv small_div(uint32_t d) { return SmallDiv{d, d > 1 ? 0xffffffffu / d + 1u : 0u}; }
+__device__ __forceinline__ uint32_t div_small(uint32_t s, SmallDiv q) { return q.d > 1 ? __umulhi(s, q.m) : s; }
+
+struct FastSampleGeo {
+    uint64_t lo[3], step[3];
+    SmallDiv c2, c12;
+    uint32_t cnt2;
+};
+
+__device__ __forceinline__ uint64_t fast_sample_pos(const FastSampleGeo &sg, uint32_t s, uint64_t n1, uint64_t n2) {
+    const uint32_t k0 = div_small(s, sg.c12);
+    const uint32_t r = s - k0 * sg.c12.d;
+    const uint32_t k1 = div_small(r, sg.c2);
+    const uint32_t k2 = r - k1 * sg.cnt2;
+    const uint64_t i0 = sg.lo[0] + k0 * sg.step[0], i1 = sg.lo[1] + k1 * sg.step[1], i2 = sg.lo[2] + k2 * sg.step[2];
+    return (i0 * n1 + i1) * n2 + i2;
+}
+
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+
+// Shared state of one group (one CTA).
+struct GroupShared {
+    uint32_t hist[5][kWinWords];
+    Interval psnr[5];
+    float fmin[kWarps][2], fmax[kWarps][2];
+    double dsum[kWarps][5];
+    uint32_t cnt[kWarps][5];
+    uint32_t flag[kWarps];
+};
+
+// Block-wide reductions over kThreads threads; every thread receives the result.
+__device__ __forceinline__ void block_minmax(GroupShared &sh, float &amin, float &amax, float &bmin, float &bmax) {
+    for (int o = 16; o; o >>= 1) {
+        amin = fminf(amin, __shfl_xor_sync(0xffffffffu, amin, o));
+        amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        bmin = fminf(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
+        bmax = fmaxf(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sh.fmin[w][0] = amin;
+        sh.fmin[w][1] = bmin;
+        sh.fmax[w][0] = amax;
+        sh.fmax[w][1] = bmax;
+    }
+    __syncthreads();
+    amin = sh.fmin[0][0];
+    bmin = sh.fmin[0][1];
+    amax = sh.fmax[0][0];
+    bmax = sh.fmax[0][1];
+    for (int i = 1; i < kWarps; i++) {
+        amin = fminf(amin, sh.fmin[i][0]);
+        bmin = fminf(bmin, sh.fmin[i][1]);
+        amax = fmaxf(amax, sh.fmax[i][0]);
+        bmax = fmaxf(bmax, sh.fmax[i][1]);
+    }
+}
+
+// Sums of nv doubles and nv counts per thread, and the OR of a flag word. Fixed order (warp tree, then
+// warps in index order), so every thread gets the same bits.
+template <int NV>
+__device__ __forceinline__ void block_sums(GroupShared &sh, double (&v)[NV], uint32_t (&c)[NV], uint32_t &flag) {
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+        for (int o = 16; o; o >>= 1) {
+            v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+            c[i] += __shfl_xor_sync(0xffffffffu, c[i], o);
+        }
+    flag = __reduce_or_sync(0xffffffffu, flag);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            sh.dsum[w][i] = v[i];
+            sh.cnt[w][i] = c[i];
+        }
+        sh.flag[w] = flag;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+        v[i] = sh.dsum[0][i];
+        c[i] = sh.cnt[0][i];
+        for (int k = 1; k < kWarps; k++) {
+            v[i] += sh.dsum[k][i];
+            c[i] += sh.cnt[k][i];
+        }
+    }
+    flag = sh.flag[0];
+    for (int k = 1; k < kWarps; k++) flag |= sh.flag[k];
+    __syncthreads();  // the staging arrays are reused by the next reduction
+}
+
 }  // namespace
 
-// Groups are listed per round; list_out receives the groups this path could not settle.
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+// One CTA per (block, round) group at a time (persistent grid). list_out receives the groups this
+// path could not settle; why[0] counts those whose errors overflow the histogram window, why[1]
+// those with an undecidable comparison.
+__global__ void __launch_bounds__(kThreads, 8)
     tsel_fast_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
                      const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
                      float R2, float t_default, float *__restrict__ tval, int64_t *__restrict__ t_int,
                      uint32_t *__restrict__ fb_count, uint32_t *__restrict__ list_out, uint32_t *__restrict__ list_count,
                      const uint32_t *__restrict__ overrides, uint32_t n_overrides, uint32_t *__restrict__ why) {
-    extern __shared__ uint32_t hist_dyn[];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t(*hist)[kWinWords] = (uint32_t(*)[kWinWords])(hist_dyn + warp * 5 * kWinWords);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GroupShared &sh = *reinterpret_cast<GroupShared *>(smem_raw);
+    const uint32_t tid = threadIdx.x;
     const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
     const int d = rg.dir;
-    for (int c = 0; c < 5; c++)
-        for (int i = lane; i < kWinWords; i += 32) hist[c][i] = 0;
-    __syncwarp();
-    for (uint64_t g = (uint64_t)blockIdx.x * kWarpsPerBlock + warp; g < nblocks; g += (uint64_t)gridDim.x * kWarpsPerBlock) {
+    for (int i = tid; i < 5 * kWinWords; i += kThreads) (&sh.hist[0][0])[i] = 0;
+    __syncthreads();
+    for (uint64_t g = blockIdx.x; g < nblocks; g += gridDim.x) {
         const uint64_t b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1],
                        b0 = g / (fg.block_num[1] * fg.block_num[2]);
         const uint64_t bb[3] = {b0, b1, b2};
@@ -125,7 +215,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 forced_t = __uint_as_float(overrides[3 * i + 2]);
             }
         if (ci.fallback || ci.n == 0 || forced) {
-            if (lane == 0) {
+            if (tid == 0) {
                 float t = forced ? forced_t : t_default;
                 if (!forced) atomicAdd(fb_count, 1u);
                 tval[g] = t;
@@ -133,7 +223,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             }
             continue;
         }
-        SampleGeo sg;
+        const uint32_t n = ci.n;
+        if (n > 0xffffu) {  // a bin count could overflow its 16-bit half word
+            if (tid == 0) {
+                list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
+                atomicAdd(&why[0], 1u);
+            }
+            continue;
+        }
+        FastSampleGeo sg;
+        uint32_t cnt[3];
         for (int a = 0; a < 3; a++) {
             uint64_t lo = bb[a] * fg.block_shape[a];
             uint64_t hi = min((bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
@@ -144,98 +243,128 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             }
             sg.lo[a] = lo;
             sg.step[a] = rg.stride[a] * ci.ss;
-            sg.cnt[a] = (uint32_t)((hi - lo + sg.step[a] - 1) / sg.step[a]);
+            cnt[a] = (uint32_t)((hi - lo + sg.step[a] - 1) / sg.step[a]);
         }
-        const uint32_t n = ci.n;
+        sg.cnt2 = cnt[2];
+        sg.c2 = small_div(cnt[2]);
+        sg.c12 = small_div(cnt[1] * cnt[2]);
         const uint64_t n1 = fg.n[1], n2 = fg.n[2];
-        if (n > 0xffffu) {  // a bin count could overflow its 16-bit half word
-            if (lane == 0) {
-                list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
-                atomicAdd(&why[0], 1u);
-            }
-            continue;
-        }
-        // Pass 1: key ranges and sums, and whether any A key is nonzero.
+        const float eb = rg.eb, neg_eb = __fdiv_rn(0.5f, eb), eb2 = __fadd_rn(eb, eb);
+        // Window placement from the first kThreads samples (one per thread): their bin range per
+        // candidate, centred in the window. A group whose samples overflow the window is redone
+        // with the exact ranges of all samples.
+        float af0 = 0.0f, bf0 = 0.0f;
+        bool nz0 = false;
         float afmin = INFINITY, afmax = -INFINITY, bfmin = INFINITY, bfmax = -INFINITY;
-        double asum = 0.0, bsum = 0.0;
-        bool anz = false;
-        for (uint32_t s = lane; s < n; s += 32) {
-            float af, bf;
-            bool nz;
-            sample_keys(rec, orig, sample_pos(sg, s, n1, n2), rg.dist, rg.neg_2_stat_eb, af, bf, nz);
-            afmin = fminf(afmin, af);
-            afmax = fmaxf(afmax, af);
-            bfmin = fminf(bfmin, bf);
-            bfmax = fmaxf(bfmax, bf);
-            asum += (double)af;
-            bsum += (double)bf;
-            anz |= nz;
+        if (tid < n) {
+            sample_keys(rec, orig, fast_sample_pos(sg, tid, n1, n2), rg.dist, rg.neg_2_stat_eb, af0, bf0, nz0);
+            afmin = afmax = af0;
+            bfmin = bfmax = bf0;
         }
-        for (int o = 16; o; o >>= 1) {
-            afmin = fminf(afmin, __shfl_xor_sync(0xffffffffu, afmin, o));
-            afmax = fmaxf(afmax, __shfl_xor_sync(0xffffffffu, afmax, o));
-            bfmin = fminf(bfmin, __shfl_xor_sync(0xffffffffu, bfmin, o));
-            bfmax = fmaxf(bfmax, __shfl_xor_sync(0xffffffffu, bfmax, o));
-            asum += __shfl_xor_sync(0xffffffffu, asum, o);
-            bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
+        block_minmax(sh, afmin, afmax, bfmin, bfmax);
+        int64_t qlo[5];
+        bool fits = true;
+        for (int c = 0; c < 5; c++) {
+            const float t2 = __fadd_rn(cand[c], cand[c]);
+            const int64_t q0 = lround_f(__fmul_rn(cand_err(afmin, bfmin, t2, rg.stat_eb), neg_eb));
+            const int64_t q1 = lround_f(__fmul_rn(cand_err(afmax, bfmax, t2, rg.stat_eb), neg_eb));
+            if (q1 >= q0 && (uint64_t)q1 - (uint64_t)q0 < (uint64_t)kWin) qlo[c] = q0 - (kWin - 1 - (q1 - q0)) / 2;
+            else fits = false;
         }
-        anz = __any_sync(0xffffffffu, anz);
+        double S[5];
+        uint32_t anz = 0, out = 1;
+        for (int attempt = 0; attempt < 2 && out; attempt++) {
+            if (attempt == 1) {
+                // Exact key ranges over all samples; the window is their bin range, or centred on
+                // the bin of the mean keys when that range is wider than the window.
+                afmin = bfmin = INFINITY;
+                afmax = bfmax = -INFINITY;
+                double ab[2] = {0.0, 0.0};
+                for (uint32_t s = tid; s < n; s += kThreads) {
+                    float af, bf;
+                    bool nz;
+                    sample_keys(rec, orig, fast_sample_pos(sg, s, n1, n2), rg.dist, rg.neg_2_stat_eb, af, bf, nz);
+                    afmin = fminf(afmin, af);
+                    afmax = fmaxf(afmax, af);
+                    bfmin = fminf(bfmin, bf);
+                    bfmax = fmaxf(bfmax, bf);
+                    ab[0] += (double)af;
+                    ab[1] += (double)bf;
+                }
+                block_minmax(sh, afmin, afmax, bfmin, bfmax);
+                uint32_t dummy[2] = {0, 0}, none = 0;
+                block_sums<2>(sh, ab, dummy, none);
+                for (int c = 0; c < 5; c++) {
+                    const float t2 = __fadd_rn(cand[c], cand[c]);
+                    const int64_t q0 = lround_f(__fmul_rn(cand_err(afmin, bfmin, t2, rg.stat_eb), neg_eb));
+                    const int64_t q1 = lround_f(__fmul_rn(cand_err(afmax, bfmax, t2, rg.stat_eb), neg_eb));
+                    if (q1 >= q0 && (uint64_t)q1 - (uint64_t)q0 < (uint64_t)kWin) {
+                        qlo[c] = q0;
+                    } else {
+                        const float am = (float)(ab[0] / n), bm = (float)(ab[1] / n);
+                        qlo[c] = lround_f(__fmul_rn(cand_err(am, bm, t2, rg.stat_eb), neg_eb)) - kWin / 2;
+                    }
+                }
+            } else if (!fits) {
+                continue;
+            }
+            // Per-candidate sums and histograms over every sample.
+            for (int c = 0; c < 5; c++) S[c] = 0.0;
+            anz = 0;
+            out = 0;
+            for (uint32_t s = tid; s < n; s += kThreads) {
+                float af, bf;
+                bool nz;
+                if (s == tid) {
+                    af = af0;
+                    bf = bf0;
+                    nz = nz0;
+                } else {
+                    sample_keys(rec, orig, fast_sample_pos(sg, s, n1, n2), rg.dist, rg.neg_2_stat_eb, af, bf, nz);
+                }
+                anz |= nz ? 1u : 0u;
+#pragma unroll
+                for (int c = 0; c < 5; c++) {
+                    const float t2 = __fadd_rn(cand[c], cand[c]);
+                    const float err = cand_err(af, bf, t2, rg.stat_eb);
+                    const int64_t q = lround_f(__fmul_rn(err, neg_eb));
+                    const float de = __fmaf_rn(-__ll2float_rn(q), eb2, err);
+                    const double dd = (double)de;
+                    S[c] = __fma_rn(dd, dd, S[c]);
+                    const uint64_t bin = (uint64_t)q - (uint64_t)qlo[c];
+                    if (bin < (uint64_t)kWin) atomicAdd(&sh.hist[c][bin >> 1], 1u << (16 * (bin & 1)));
+                    else out = 1;
+                }
+            }
+            {
+                // One reduction: S, and the OR of the flags (overflow in bit 0, a nonzero A key in bit 1).
+                uint32_t flags = out | (anz << 1), dummy[5] = {0, 0, 0, 0, 0};
+                block_sums<5>(sh, S, dummy, flags);
+                out = flags & 1u;
+                anz = (flags >> 1) & 1u;
+            }
+            if (out || !anz) {
+                for (int i = tid; i < 5 * kWinWords; i += kThreads) (&sh.hist[0][0])[i] = 0;
+                __syncthreads();
+            }
+            if (!anz) break;
+        }
         if (!anz) {
             // Every candidate sees identical errors, so every comparison is fmaf(0, slope, 0 or NaN)
             // and nothing is accepted: t stays at 1/4.
-            if (lane == 0) {
+            if (tid == 0) {
                 tval[g] = cand[1];
                 t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(cand[1], (float)fg.t_precision));
             }
             continue;
         }
-        const float eb = rg.eb, neg_eb = __fdiv_rn(0.5f, eb), eb2 = __fadd_rn(eb, eb);
-        // Histogram window per candidate: the exact bin range when it fits, else centred on the
-        // bin of the mean keys; samples outside it send the group to the exact path.
-        int64_t qlo[5];
-        for (int c = 0; c < 5; c++) {
-            float t2 = __fadd_rn(cand[c], cand[c]);
-            int64_t q0 = lround_f(__fmul_rn(cand_err(afmin, bfmin, t2, rg.stat_eb), neg_eb));
-            int64_t q1 = lround_f(__fmul_rn(cand_err(afmax, bfmax, t2, rg.stat_eb), neg_eb));
-            if (q1 >= q0 && (uint64_t)q1 - (uint64_t)q0 < (uint64_t)kWin) {
-                qlo[c] = q0;
-            } else {
-                float am = (float)(asum / n), bm = (float)(bsum / n);
-                qlo[c] = lround_f(__fmul_rn(cand_err(am, bm, t2, rg.stat_eb), neg_eb)) - kWin / 2;
-            }
-        }
-        // Pass 2: per-candidate sums and histograms.
-        double S[5] = {0, 0, 0, 0, 0};
-        bool out = false;
-        for (uint32_t s = lane; s < n; s += 32) {
-            float af, bf;
-            bool nz;
-            sample_keys(rec, orig, sample_pos(sg, s, n1, n2), rg.dist, rg.neg_2_stat_eb, af, bf, nz);
-#pragma unroll
-            for (int c = 0; c < 5; c++) {
-                float t2 = __fadd_rn(cand[c], cand[c]);
-                float err = cand_err(af, bf, t2, rg.stat_eb);
-                int64_t q = lround_f(__fmul_rn(err, neg_eb));
-                float de = __fmaf_rn(-__ll2float_rn(q), eb2, err);
-                double dd = (double)de;
-                S[c] = __fma_rn(dd, dd, S[c]);
-                const uint64_t bin = (uint64_t)q - (uint64_t)qlo[c];
-                if (bin < (uint64_t)kWin) atomicAdd(&hist[c][bin >> 1], 1u << (16 * (bin & 1)));
-                else out = true;
-            }
-        }
-        out = __any_sync(0xffffffffu, out);
         if (out) {
-            for (int c = 0; c < 5; c++)
-                for (int i = lane; i < kWinWords; i += 32) hist[c][i] = 0;
-            __syncwarp();
-            if (lane == 0) {
+            if (tid == 0) {
                 list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
                 atomicAdd(&why[0], 1u);
             }
             continue;
         }
-        __syncwarp();
         const float nf = __ull2float_rn((uint64_t)n), r = __fdiv_rn(1.0f, nf);
         const float *l2 = log2arena + ci.log2_off;
         double H[5];
@@ -244,8 +373,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         for (int c = 0; c < 5; c++) {
             double h = 0.0;
             uint32_t k = 0;
-            for (int i = lane; i < kWinWords; i += 32) {
-                uint32_t w = hist[c][i];
+            for (int i = tid; i < kWinWords; i += kThreads) {
+                uint32_t w = sh.hist[c][i];
                 if (w) {
                     uint32_t c0 = w & 0xffffu, c1 = w >> 16;
                     if (c0) {
@@ -258,65 +387,62 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                         h = __fma_rn(-(double)p, (double)l2[c1], h);
                         k++;
                     }
-                    hist[c][i] = 0;
+                    sh.hist[c][i] = 0;
                 }
-            }
-            for (int o = 16; o; o >>= 1) {
-                h += __shfl_xor_sync(0xffffffffu, h, o);
-                k += __shfl_xor_sync(0xffffffffu, k, o);
-                S[c] += __shfl_xor_sync(0xffffffffu, S[c], o);
             }
             H[c] = h;
             mq[c] = k;
         }
-        __syncwarp();
-        if (lane == 0) {
-            // Decision chain (compress.tpp:127-142) on intervals.
-            Interval P[5];
-            double hlo[5], hhi[5];
-            for (int c = 0; c < 5; c++) {
-                P[c] = psnr_interval(S[c], n, R2, nf);
-                double gq = (double)mq[c] * 0x1.0002p-24 + 0x1p-40;
-                hlo[c] = H[c] * (1.0 - gq);
-                hhi[c] = H[c] * (1.0 + gq);
-            }
-            const double slope = (double)rg.slope;
-            bool sure = isfinite(slope) && slope > 0;
-            int best = 1;
-            for (int c = 0; c < 5 && sure; c++) {
-                if (cand[c] == cand[best]) continue;
-                bool accept;
-                if (P[c].exact_inf || P[best].exact_inf) {
-                    // inf - finite = inf (accept), finite - inf = -inf, inf - inf = NaN (reject).
-                    accept = P[c].exact_inf && !P[best].exact_inf;
-                } else {
-                    double dlo = hlo[best] - hhi[c], dhi = hhi[best] - hlo[c];
-                    dlo -= fabs(dlo) * 0x1p-23;
-                    dhi += fabs(dhi) * 0x1p-23;
-                    double plo = P[c].lo - P[best].hi, phi = P[c].hi - P[best].lo;
-                    plo -= fabs(plo) * 0x1p-23;
-                    phi += fabs(phi) * 0x1p-23;
-                    double slo = dlo * slope + plo, shi = dhi * slope + phi;
-                    slo -= 1e-9 * (fabs(dlo * slope) + fabs(plo));
-                    shi += 1e-9 * (fabs(dhi * slope) + fabs(phi));
-                    if (slo > 1e-30) accept = true;
-                    else if (shi <= 0.0) accept = false;
-                    else {
-                        sure = false;
-                        break;
+        {
+            uint32_t none = 0;
+            block_sums<5>(sh, H, mq, none);
+        }
+        if (tid < 32) {
+            // PSNR intervals of the five candidates in parallel, then the decision chain
+            // (compress.tpp:127-142) on intervals by one lane.
+            if (tid < 5) sh.psnr[tid] = psnr_interval(S[tid], n, R2, nf);
+            __syncwarp();
+            if (tid == 0) {
+                const double slope = (double)rg.slope;
+                bool sure = isfinite(slope) && slope > 0;
+                int best = 1;
+                for (int c = 0; c < 5 && sure; c++) {
+                    if (cand[c] == cand[best]) continue;
+                    const Interval Pc = sh.psnr[c], Pb = sh.psnr[best];
+                    const double gb = (double)mq[best] * 0x1.0002p-24 + 0x1p-40, gc = (double)mq[c] * 0x1.0002p-24 + 0x1p-40;
+                    bool accept;
+                    if (Pc.exact_inf || Pb.exact_inf) {
+                        // inf - finite = inf (accept), finite - inf = -inf, inf - inf = NaN (reject).
+                        accept = Pc.exact_inf && !Pb.exact_inf;
+                    } else {
+                        double dlo = H[best] * (1.0 - gb) - H[c] * (1.0 + gc), dhi = H[best] * (1.0 + gb) - H[c] * (1.0 - gc);
+                        dlo -= fabs(dlo) * 0x1p-23;
+                        dhi += fabs(dhi) * 0x1p-23;
+                        double plo = Pc.lo - Pb.hi, phi = Pc.hi - Pb.lo;
+                        plo -= fabs(plo) * 0x1p-23;
+                        phi += fabs(phi) * 0x1p-23;
+                        double slo = dlo * slope + plo, shi = dhi * slope + phi;
+                        slo -= 1e-9 * (fabs(dlo * slope) + fabs(plo));
+                        shi += 1e-9 * (fabs(dhi * slope) + fabs(phi));
+                        if (slo > 1e-30) accept = true;
+                        else if (shi <= 0.0) accept = false;
+                        else {
+                            sure = false;
+                            break;
+                        }
                     }
+                    if (accept) best = c;
                 }
-                if (accept) best = c;
-            }
-            if (!sure) {
-                list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
-                atomicAdd(&why[1], 1u);
-            } else {
-                tval[g] = cand[best];
-                t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(cand[best], (float)fg.t_precision));
+                if (!sure) {
+                    list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
+                    atomicAdd(&why[1], 1u);
+                } else {
+                    tval[g] = cand[best];
+                    t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(cand[best], (float)fg.t_precision));
+                }
             }
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
@@ -325,14 +451,14 @@ cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t 
                              int64_t *t_int, uint32_t *fb_count, uint32_t *list_out, uint32_t *list_count,
                              const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st) {
     uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    uint64_t blocks = (nb + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    if (blocks > 148 * 64) blocks = 148 * 64;
-    const int smem = kWarpsPerBlock * 5 * kWinWords * 4;
+    uint64_t blocks = nb < 148 * 8 * 4 ? nb : 148 * 8 * 4;
+    const int smem = (int)sizeof(GroupShared);
     cudaError_t e = cudaFuncSetAttribute(tsel_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    tsel_fast_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2,
-                                                                          t_default, tval, t_int, fb_count, list_out,
-                                                                          list_count, overrides, n_overrides, why);
+    tsel_fast_kernel<<<(unsigned)blocks, kThreads, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
+                                                              t_int, fb_count, list_out, list_count, overrides, n_overrides,
+                                                              why);
+    count_launch();
     return cudaGetLastError();
 }
 

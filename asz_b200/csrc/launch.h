@@ -10,6 +10,11 @@
 
 namespace asz {
 
+// Kernels launched by this library on the calling thread (each launcher counts its own launches;
+// library kernels such as CUB's scans are not counted).
+uint64_t &launch_counter();
+inline void count_launch() { ++launch_counter(); }
+
 struct PivotGeom {
     uint64_t cnt[3];      // pivots per axis
     uint64_t stride[3];
@@ -40,12 +45,12 @@ cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long lon
 cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *rec, int32_t *qb, int32_t *qb_range,
                                   cudaStream_t st);
 cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, float *rec, cudaStream_t st);
-cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const uint64_t *tab_count,
-                                  const uint64_t *tab_prefix, const float *tval, const float *in, float *rec, int32_t *qb,
-                                  int32_t *qb_range, uint32_t *err, cudaStream_t st);
-cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const uint64_t *tab_count,
-                                    const uint64_t *tab_prefix, const int64_t *t_int, const int32_t *qb, float *rec,
-                                    uint32_t *err, cudaStream_t st);
+// One round over every target; `ent` holds the per-axis AxisEntry tables (RoundGeom::ent_off).
+// Requires tcount[0] * tcount[1] < 2^32 and tcount[2] < 2^32 (checked by the host).
+cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
+                                  const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, cudaStream_t st);
+cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const AxisEntry *ent,
+                                    const int64_t *t_int, const int32_t *qb, float *rec, uint32_t *err, cudaStream_t st);
 
 cudaError_t launch_error_stats(const float *x, const float *y, uint64_t n, unsigned int *max_bits, double *sse,
                                cudaStream_t st);

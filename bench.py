@@ -206,7 +206,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="512,512,512", help="field shape (smaller shapes are for profiler captures)")
     args = ap.parse_args()
+    shape = tuple(int(v) for v in args.shape.split(","))
     if args.impl == "reference":
         run_reference_arm(args)
         return
@@ -224,7 +226,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
-    x = make_field_torch(1234 + rank, SHAPE, dev)
+    x = make_field_torch(1234 + rank, shape, dev)
+    workload = WORKLOAD if shape == SHAPE else WORKLOAD.replace("512^3", "x".join(map(str, shape)))
     N = x.numel()
     p = api.default_params(block_pivot_ratio=BPR)
     ctx = api.Context(local)
@@ -238,50 +241,88 @@ def main():
         torch.cuda.synchronize(dev)
 
     y = torch.empty_like(x)
+    # The timed loops call the C ABI directly (the reference-facing boundary), on torch's stream.
+    L.asz_set_stream(ctx._c, C.c_void_p(stream.cuda_stream))
+    p.predictor_family = api.ASZ_FAMILY_CUBIC
+    dims = api._dims(shape)
+    plan_b = PLAN.encode()
+    outp = C.POINTER(C.c_uint8)()
+    outn = C.c_size_t(0)
+    rep = api.Report()
+
+    def compress_abi(ptr, on_device):
+        rc = L.asz_compress(ctx._c, C.c_void_p(ptr), on_device, dims, C.c_float(REL_EB), C.byref(p), plan_b,
+                            C.byref(outp), C.byref(outn), C.byref(rep))
+        if rc:
+            raise api.AszError(rc, L.asz_last_error(ctx._c).decode())
+        L.asz_free(outp)
+        return rep
+
     blob = None
     for _ in range(args.warmup):
-        blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
-        ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
-    # Compress, device-resident input.
+        blob, _r = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+        L.asz_set_stream(ctx._c, C.c_void_p(stream.cuda_stream))
+        ctx.decompress(blob, shape, REL_EB, p, out=y)
+        L.asz_set_stream(ctx._c, C.c_void_p(stream.cuda_stream))
+    blob_np = np.frombuffer(blob, dtype=np.uint8)
+    blob_ptr = C.c_void_p(blob_np.ctypes.data)
+    drep = api.Report()
+
+    def decompress_abi(out_ptr, on_device):
+        rc = L.asz_decompress(ctx._c, blob_ptr, len(blob), dims, C.c_float(REL_EB), C.byref(p), C.c_void_p(out_ptr),
+                              on_device, C.byref(drep))
+        if rc:
+            raise api.AszError(rc, L.asz_last_error(ctx._c).decode())
+        return drep
+
+    # Compress, device-resident input. libzstd and the device->host copy of the stream run inside
+    # each call; their measured durations are taken out of `value` and reported apart.
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    zstd_s = 0.0
+    zstd_s = d2h_s = 0.0
+    launches = 0
     with ClockSampler(local) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
-            zstd_s += rep.zstd_s
+            r = compress_abi(x.data_ptr(), 1)
+            zstd_s += r.zstd_s
+            d2h_s += r.d2h_s
+            launches += r.kernel_launches
         ev1.record(stream)
         barrier()
-    comp_ms = ev0.elapsed_time(ev1)
-    # Device time excludes the host libzstd stage, which the ABI call also performs.
-    core_ms = comp_ms - zstd_s * 1000
-    # Decompress into device memory.
+    call_ms = ev0.elapsed_time(ev1)
+    core_ms = call_ms - (zstd_s + d2h_s) * 1000
+    pre_zstd_len = int(rep.pre_zstd_len)
+    asz_len = int(rep.asz_len)
+    # Decompress into device memory (zstd and the stream's host->device copy taken out likewise).
     barrier()
+    dz_s = dh2d_s = 0.0
     ev0.record(stream)
     for _ in range(args.steps):
-        ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+        r = decompress_abi(y.data_ptr(), 1)
+        dz_s += r.zstd_s
+        dh2d_s += r.h2d_s
     ev1.record(stream)
     barrier()
-    dec_ms = ev0.elapsed_time(ev1)
+    dec_call_ms = ev0.elapsed_time(ev1)
+    dec_ms = dec_call_ms - (dz_s + dh2d_s) * 1000
     # Parity spot check of this run: decompression equals the compressor's reconstruction.
-    blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
-    rec = torch.from_numpy(ctx.debug_recon()).to(dev).view(SHAPE)
-    ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+    blob, rep1 = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+    rec = torch.from_numpy(ctx.debug_recon()).to(dev).view(shape)
+    ctx.decompress(blob, shape, REL_EB, p, out=y)
     torch.cuda.synchronize(dev)
     bit_exact = bool(torch.equal(rec.view(torch.int32), y.view(torch.int32)))
     max_err = float((y - x).abs().max().item())
-    # Profile of one compression (per kernel family).
+    del rec
+    # Profile of one compression and one decompression (per kernel family, CUDA events).
+    L.asz_set_stream(ctx._c, C.c_void_p(stream.cuda_stream))
     L.asz_profile_enable(ctx._c, 1)
-    blob, rep = ctx.compress(x, REL_EB, PLAN, FAMILY, p)
+    compress_abi(x.data_ptr(), 1)
     entries = (PROFILE_ENTRY * 64)()
     n = L.asz_profile_read(ctx._c, entries, 64, 1)
-    L.asz_profile_enable(ctx._c, 0)
     prof = {entries[i].name.decode(): {"launches": entries[i].launches, "ms": entries[i].ms, "bytes": entries[i].bytes}
             for i in range(min(n, 64))}
-    # The same for one decompression.
-    L.asz_profile_enable(ctx._c, 1)
-    ctx.decompress(blob, SHAPE, REL_EB, p, out=y)
+    decompress_abi(y.data_ptr(), 1)
     n = L.asz_profile_read(ctx._c, entries, 64, 1)
     L.asz_profile_enable(ctx._c, 0)
     prof_dec = {entries[i].name.decode(): {"launches": entries[i].launches, "ms": entries[i].ms, "bytes": entries[i].bytes}
@@ -291,22 +332,28 @@ def main():
     host_phases_dec = {k[5:]: round(v["ms"], 3) for k, v in prof_dec.items() if k.startswith("host:")}
     prof = {k: v for k, v in prof.items() if not k.startswith("host:")}
     prof_dec = {k: v for k, v in prof_dec.items() if not k.startswith("host:")}
-    # End to end from pinned host memory, including zstd.
+    # End to end from pinned host memory to .asz bytes on the host (everything included), and back.
     xh = x.cpu().pin_memory()
-    xh_np = xh.numpy()
+    yh = torch.empty_like(xh).pin_memory()
     barrier()
-    t0 = time.perf_counter()
     ev0.record(stream)
     for _ in range(args.steps):
-        blob_e, rep_e = ctx.compress(xh_np, REL_EB, PLAN, FAMILY, p)
+        r = compress_abi(xh.data_ptr(), 0)
     ev1.record(stream)
     barrier()
     e2e_ms = ev0.elapsed_time(ev1)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        decompress_abi(yh.data_ptr(), 0)
+    ev1.record(stream)
+    barrier()
+    e2e_dec_ms = ev0.elapsed_time(ev1)
+    L.asz_set_stream(ctx._c, None)
     # Max over ranks.
-    times = torch.tensor([core_ms, dec_ms, e2e_ms], device=dev)
+    times = torch.tensor([core_ms, dec_ms, e2e_ms, e2e_dec_ms], device=dev)
     if pg:
         pg.all_reduce(times, op=pg.ReduceOp.MAX)
-    core_ms, dec_ms, e2e_ms = times.tolist()
+    core_ms, dec_ms, e2e_ms, e2e_dec_ms = times.tolist()
     if rank != 0:
         if pg:
             pg.destroy_process_group()
@@ -315,41 +362,52 @@ def main():
     comp_gbs = total_bytes * args.steps / (core_ms / 1000) / 1e9
     dec_gbs = total_bytes * args.steps / (dec_ms / 1000) / 1e9
     e2e_gbs = total_bytes * args.steps / (e2e_ms / 1000) / 1e9
+    e2e_dec_gbs = total_bytes * args.steps / (e2e_dec_ms / 1000) / 1e9
     peak, peak_kind = measured_peaks()
-    top = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else None
+    # Dominant kernel family: algorithmic bytes of its launches over their CUDA-event time.
     roofline = None
-    if top:
-        name, t = top
-        if t["bytes"] and t["ms"] > 0:
-            ach = t["bytes"] / (t["ms"] / 1000) / 1e9
-            roofline = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                        "peak_source": peak_kind, "traffic": None}
-        else:
-            # Whole-path algorithmic bytes (4N read + stream written) over the device time.
-            ach = (4.0 * N + rep.pre_zstd_len) / (core_ms / args.steps / 1000) / 1e9
-            roofline = {"bound": "hbm", "kernel": "whole compress path (top family: " + name + ")", "achieved": ach,
-                        "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind, "traffic": None}
+    ranked = sorted(((k, v) for k, v in prof.items() if v["bytes"]), key=lambda kv: -kv[1]["ms"])
+    if ranked:
+        name, t = ranked[0]
+        ach = t["bytes"] / (t["ms"] / 1000) / 1e9
+        roofline = {"bound": "hbm", "kernel": name, "launches": t["launches"], "achieved": ach, "peak": peak,
+                    "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind,
+                    "traffic": TRAFFIC_PER_LAUNCH.get(name)}
+    # Whole path: 4N read + the stream written, over the compress device time.
+    path_ach = (4.0 * N + pre_zstd_len) / (core_ms / args.steps / 1000) / 1e9
+    roofline_path = {"bound": "hbm", "achieved": path_ach, "peak": peak, "unit": "GB/s", "frac": path_ach / peak,
+                     "bytes_per_step": 4 * N + pre_zstd_len}
     cpu = None
     if not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as wd:
-            cpu = cpu_baseline(x[:64].cpu().numpy(), wd, planes=64)
+            cpu = cpu_baseline(x[:64].cpu().numpy(), wd, planes=min(64, shape[0]))
     out = {
         "metric": METRIC, "value": comp_gbs, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": core_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "inputs": "512 MiB per field > L2, no flush needed", "parallelism": f"replicas x{world}"},
+        "config": {"workload": workload, "inputs": f"{4 * N / 2**20:.0f} MiB per field; "
+                   + ("> L2, no flush needed" if 4 * N > 126e6 else "fits L2 (profiling size only)"),
+                   "parallelism": f"replicas x{world}",
+                   "value_excludes": "libzstd and host<->device copies (timed inside the call, reported apart)"},
         "decompress": {"value": dec_gbs, "unit": "GB/s", "ms_per_step": dec_ms / args.steps},
-        "zstd_ms_per_step": zstd_s * 1000 / args.steps,
-        "e2e": {"value": e2e_gbs, "unit": "GB/s", "h2d_bytes_per_step": 4 * N, "d2h_bytes_per_step": int(rep_e.pre_zstd_len),
-                "includes": "H2D from pinned memory, all GPU stages, D2H of the stream, libzstd level 3"},
-        "cr": float(4 * N / len(blob)), "bit_exact_roundtrip": bit_exact, "max_err_over_eb": max_err / rep.abs_eb,
-        "t_fallback_count": int(rep.t_fallback_count), "ambiguous_decisions": int(rep.ambiguous_decisions),
-        "exact_groups": int(rep.exact_groups), "serial_groups": int(rep.serial_groups),
-        "exact_window": int(rep.exact_window), "exact_undecided": int(rep.exact_undecided),
-        "roofline": roofline, "profile": prof, "host_phases_ms": host_phases,
+        "zstd_ms_per_step": zstd_s * 1000 / args.steps, "d2h_ms_per_step": d2h_s * 1000 / args.steps,
+        "zstd_decompress_ms_per_step": dz_s * 1000 / args.steps,
+        "e2e": {"value": e2e_gbs, "unit": "GB/s", "h2d_bytes_per_step": 4 * N, "d2h_bytes_per_step": pre_zstd_len,
+                "ms_per_step": e2e_ms / args.steps,
+                "includes": "C-ABI call from pinned host memory to .asz bytes on the host: H2D, all GPU stages, "
+                            "D2H of the stream, libzstd level 3"},
+        "e2e_decompress": {"value": e2e_dec_gbs, "unit": "GB/s", "h2d_bytes_per_step": pre_zstd_len,
+                           "d2h_bytes_per_step": 4 * N, "ms_per_step": e2e_dec_ms / args.steps},
+        "cr": float(4 * N / asz_len), "pre_zstd_bytes": pre_zstd_len, "bit_exact_roundtrip": bit_exact,
+        "max_err_over_eb": max_err / rep1.abs_eb,
+        "t_fallback_count": int(rep1.t_fallback_count), "ambiguous_decisions": int(rep1.ambiguous_decisions),
+        "reruns": int(rep1.reruns),
+        "exact_groups": int(rep1.exact_groups), "serial_groups": int(rep1.serial_groups),
+        "exact_window": int(rep1.exact_window), "exact_undecided": int(rep1.exact_undecided),
+        "roofline": roofline, "roofline_path": roofline_path, "profile": prof, "host_phases_ms": host_phases,
         "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
         "cpu_baseline": cpu, "clocks": clocks.summary(),
-        "gpu_launches": int(sum(v["launches"] for v in prof.values())) if prof else None,
+        "gpu_launches": int(launches),
     }
     print(json.dumps(out))
     if pg:
@@ -357,6 +415,10 @@ def main():
 
 
 import ctypes as _C  # noqa: E402
+
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernel
+# family, from the committed ncu captures; None until captured.
+TRAFFIC_PER_LAUNCH = {}
 
 
 class PROFILE_ENTRY(_C.Structure):
