@@ -57,7 +57,7 @@ class Report(C.Structure):
         ("layer_num", C.c_uint64), ("slope_max_invalid_ratio", C.c_float), ("slope_fallback_reason", C.c_int32),
         ("ambiguous_decisions", C.c_uint64), ("reruns", C.c_uint64), ("exact_groups", C.c_uint64),
         ("serial_groups", C.c_uint64), ("exact_window", C.c_uint64), ("exact_undecided", C.c_uint64),
-        ("kernel_launches", C.c_uint64),
+        ("wide_groups", C.c_uint64), ("kernel_launches", C.c_uint64),
         ("pivot_stride", C.c_uint32 * 3), ("block_shape", C.c_uint32 * 3), ("block_num", C.c_uint32 * 3),
         ("quintic", C.c_int32), ("plan", C.c_char * (64 * 11 + 1)),
     ]

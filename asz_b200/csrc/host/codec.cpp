@@ -620,7 +620,7 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t list_count[64];
     uint32_t spill_count[64];
     uint32_t all_count;
-    uint32_t why[2];  // fast path hand-offs: [0] errors outside the histogram window, [1] undecided
+    uint32_t why[3];  // fast path: [0] handed off (bins too spread), [1] handed off (undecided), [2] settled window by window
     int32_t qb_range[2 * 64];
     float h1[3 * 64];
     float x[3 * 64];
@@ -1020,11 +1020,12 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         CK(cudaMemcpyAsync(words, &dm->err, sizeof(words), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(lcounts, dm->list_count, sizeof(lcounts), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(scounts, dm->spill_count, sizeof(scounts), cudaMemcpyDeviceToHost, st));
-        uint32_t why[2];
+        uint32_t why[3];
         CK(cudaMemcpyAsync(why, dm->why, sizeof(why), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         R.exact_window = why[0];
         R.exact_undecided = why[1];
+        R.wide_groups = why[2];
         R.exact_groups = 0;
         R.serial_groups = 0;
         for (u64 l = 0; l < L && l < 64; l++) {

@@ -26,6 +26,9 @@ namespace {
 constexpr int kWin = 1024;         // histogram window (quantised-error values) per candidate
 // Counts are 16-bit (a group has < 65536 samples), two per 32-bit word.
 constexpr int kWinWords = kWin / 2;
+// A group whose bins still overflow the window over the exact key ranges is counted in windows of
+// 5 * kWin bins; beyond this many passes (all candidates together) it goes to the exact path.
+constexpr uint32_t kMaxWidePasses = 40;
 
 __device__ __forceinline__ int class_of(uint64_t b, uint64_t nb) { return b == 0 ? 0 : (b == nb - 1 ? 2 : 1); }
 
@@ -185,8 +188,8 @@ __device__ __forceinline__ void block_sums(GroupShared &sh, double (&v)[NV], uin
 }  // namespace
 
 // One CTA per (block, round) group at a time (persistent grid). list_out receives the groups this
-// path could not settle; why[0] counts those whose errors overflow the histogram window, why[1]
-// those with an undecidable comparison.
+// path could not settle; why[0] counts those whose bins span too many windows, why[1] those with an
+// undecidable comparison; why[2] counts the groups settled here by window-by-window counting.
 __global__ void __launch_bounds__(kThreads, 8)
     tsel_fast_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
                      const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
@@ -358,40 +361,96 @@ __global__ void __launch_bounds__(kThreads, 8)
             }
             continue;
         }
-        if (out) {
-            if (tid == 0) {
-                list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
-                atomicAdd(&why[0], 1u);
-            }
-            continue;
-        }
         const float nf = __ull2float_rn((uint64_t)n), r = __fdiv_rn(1.0f, nf);
         const float *l2 = log2arena + ci.log2_off;
         double H[5];
         uint32_t mq[5];
-#pragma unroll
-        for (int c = 0; c < 5; c++) {
-            double h = 0.0;
-            uint32_t k = 0;
-            for (int i = tid; i < kWinWords; i += kThreads) {
-                uint32_t w = sh.hist[c][i];
-                if (w) {
-                    uint32_t c0 = w & 0xffffu, c1 = w >> 16;
-                    if (c0) {
-                        float p = __fmul_rn(__ull2float_rn((uint64_t)c0), r);
-                        h = __fma_rn(-(double)p, (double)l2[c0], h);
-                        k++;
-                    }
-                    if (c1) {
-                        float p = __fmul_rn(__ull2float_rn((uint64_t)c1), r);
-                        h = __fma_rn(-(double)p, (double)l2[c1], h);
-                        k++;
-                    }
-                    sh.hist[c][i] = 0;
-                }
+        if (out) {
+            // The bins of some candidate span more than the window even over the exact key ranges.
+            // Count them window by window instead: per candidate, passes over the samples with all
+            // five histogram regions used as one window of 5 * kWin bins.
+            constexpr int kWide = 5 * kWin;
+            int64_t q0c[5];
+            uint32_t passes = 0;
+            for (int c = 0; c < 5; c++) {
+                const float t2 = __fadd_rn(cand[c], cand[c]);
+                q0c[c] = lround_f(__fmul_rn(cand_err(afmin, bfmin, t2, rg.stat_eb), neg_eb));
+                const int64_t q1 = lround_f(__fmul_rn(cand_err(afmax, bfmax, t2, rg.stat_eb), neg_eb));
+                const uint64_t pc = ((uint64_t)q1 - (uint64_t)q0c[c]) / kWide + 1;
+                passes += pc < (1u << 20) ? (uint32_t)pc : (1u << 20);
             }
-            H[c] = h;
-            mq[c] = k;
+            if (passes > kMaxWidePasses) {
+                if (tid == 0) {
+                    list_out[atomicAdd(list_count, 1u)] = (uint32_t)g;
+                    atomicAdd(&why[0], 1u);
+                }
+                continue;
+            }
+            uint32_t *flat = &sh.hist[0][0];
+            for (int c = 0; c < 5; c++) {
+                const float t2 = __fadd_rn(cand[c], cand[c]);
+                const int64_t q1 = lround_f(__fmul_rn(cand_err(afmax, bfmax, t2, rg.stat_eb), neg_eb));
+                double h = 0.0;
+                uint32_t k = 0;
+                for (int64_t lo = q0c[c];; lo += kWide) {
+                    for (uint32_t s = tid; s < n; s += kThreads) {
+                        float af, bf;
+                        bool nz;
+                        sample_keys(rec, orig, fast_sample_pos(sg, s, n1, n2), rg.dist, rg.neg_2_stat_eb, af, bf, nz);
+                        const int64_t q = lround_f(__fmul_rn(cand_err(af, bf, t2, rg.stat_eb), neg_eb));
+                        const uint64_t bin = (uint64_t)q - (uint64_t)lo;
+                        if (bin < (uint64_t)kWide) atomicAdd(&flat[bin >> 1], 1u << (16 * (bin & 1)));
+                    }
+                    __syncthreads();
+                    for (int i = tid; i < kWide / 2; i += kThreads) {
+                        const uint32_t w = flat[i];
+                        if (w) {
+                            const uint32_t c0 = w & 0xffffu, c1 = w >> 16;
+                            if (c0) {
+                                const float p = __fmul_rn(__ull2float_rn((uint64_t)c0), r);
+                                h = __fma_rn(-(double)p, (double)l2[c0], h);
+                                k++;
+                            }
+                            if (c1) {
+                                const float p = __fmul_rn(__ull2float_rn((uint64_t)c1), r);
+                                h = __fma_rn(-(double)p, (double)l2[c1], h);
+                                k++;
+                            }
+                            flat[i] = 0;
+                        }
+                    }
+                    __syncthreads();
+                    if (q1 - lo < kWide) break;
+                }
+                H[c] = h;
+                mq[c] = k;
+            }
+            if (tid == 0) atomicAdd(&why[2], 1u);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                double h = 0.0;
+                uint32_t k = 0;
+                for (int i = tid; i < kWinWords; i += kThreads) {
+                    uint32_t w = sh.hist[c][i];
+                    if (w) {
+                        uint32_t c0 = w & 0xffffu, c1 = w >> 16;
+                        if (c0) {
+                            float p = __fmul_rn(__ull2float_rn((uint64_t)c0), r);
+                            h = __fma_rn(-(double)p, (double)l2[c0], h);
+                            k++;
+                        }
+                        if (c1) {
+                            float p = __fmul_rn(__ull2float_rn((uint64_t)c1), r);
+                            h = __fma_rn(-(double)p, (double)l2[c1], h);
+                            k++;
+                        }
+                        sh.hist[c][i] = 0;
+                    }
+                }
+                H[c] = h;
+                mq[c] = k;
+            }
         }
         {
             uint32_t none = 0;

@@ -404,6 +404,7 @@ def main():
         "reruns": int(rep1.reruns),
         "exact_groups": int(rep1.exact_groups), "serial_groups": int(rep1.serial_groups),
         "exact_window": int(rep1.exact_window), "exact_undecided": int(rep1.exact_undecided),
+        "wide_groups": int(rep1.wide_groups),
         "roofline": roofline, "roofline_path": roofline_path, "profile": prof, "host_phases_ms": host_phases,
         "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
         "cpu_baseline": cpu, "clocks": clocks.summary(),

@@ -96,6 +96,7 @@ typedef struct asz_report {
     uint64_t serial_groups;       /* groups too large for the shared-memory exact kernel (serial kernel) */
     uint64_t exact_window;        /* of exact_groups: errors spread wider than the fast path's histogram */
     uint64_t exact_undecided;     /* of exact_groups: a comparison the fast path's bounds could not settle */
+    uint64_t wide_groups;         /* groups the fast path settled by counting their bins window by window */
     uint64_t kernel_launches;     /* this library's kernels launched by the call (CUB scans not counted) */
     uint32_t pivot_stride[3], block_shape[3], block_num[3];
     int32_t quintic;

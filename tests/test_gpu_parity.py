@@ -84,6 +84,20 @@ def test_c2_like_128_cubic2_plan(gpu_ctx, family):
     assert rep.t_fallback_count > 0
 
 
+@pytest.mark.parametrize("rel_eb,path", [(1e-4, "windows"), (2e-5, "exact")])
+def test_wide_bin_ranges(gpu_ctx, rel_eb, path):
+    """White noise at a small error bound: the quantised errors of many (block, round) groups span
+    more than the fast path's histogram window, so they are counted window by window (or, when
+    too spread, handed to the exact path)."""
+    rng = np.random.default_rng(5)
+    f = rng.random((24, 24, 384)).astype(np.float32)
+    rep = _check_against_oracle(gpu_ctx, f, rel_eb, ",".join(["cubic2_012"] * 6), "cubic", 3)
+    if path == "windows":
+        assert rep.wide_groups > 0
+    else:
+        assert rep.exact_window > 0
+
+
 def test_device_resident_input(gpu_ctx):
     import torch
 
