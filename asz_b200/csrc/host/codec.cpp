@@ -621,6 +621,8 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t spill_count[64];
     uint32_t all_count;
     uint32_t why[3];  // fast path: [0] handed off (bins too spread), [1] handed off (undecided), [2] settled window by window
+    uint32_t dec_err;      // batched Huffman decoding: error bits
+    uint32_t dec_changed;  // batched Huffman decoding: a chunk start moved in the last pass
     int32_t qb_range[2 * 64];
     float h1[3 * 64];
     float x[3 * 64];
@@ -1277,70 +1279,107 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
 
 namespace {
 
-int gpu_decode(asz_ctx *ctx, const HuffParsed &hp, uint64_t count, const uint8_t *d_base, uint64_t base_off, void *d_out,
-               bool wide, cudaStream_t st) {
-    if (hp.single) {
-        if (hp.single_count != count) return fail(ctx, ASZ_E_DATA, "Huffman payload length does not match its value count");
-        if (wide) CK(launch_fill<int64_t>((int64_t *)d_out, count, (int64_t)hp.offset, st));
-        else CK(launch_fill<int32_t>((int32_t *)d_out, count, (int32_t)hp.offset, st));
-        return ASZ_OK;
+// Zero bytes after the stream for the decoder's read-ahead.
+constexpr u64 kDecodePad = 64;
+
+// One stream to decode: its parsed code, the values it must produce and where they go.
+struct DecodeJob {
+    const HuffParsed *hp;
+    u64 count;
+    void *out;
+    bool wide;
+};
+
+// Decode every stream of a .asz in one batched launch per pass (k_huff.cu). The stream bytes are
+// on the device at d_base (256-byte aligned, padded by kDecodePad). Errors of the payloads are
+// left in dm->dec_err for the caller to read with its final synchronisation.
+int gpu_decode_all(asz_ctx *ctx, const std::vector<DecodeJob> &jobs, const uint8_t *d_base, MiscLayout *dm, cudaStream_t st) {
+    const u64 C = 1024;  // chunk bits
+    std::vector<DecStream> ds;
+    std::vector<uint32_t> tile_stream;
+    std::vector<LutEntry> luts;
+    std::vector<uint32_t> childs;
+    u64 nchunks = 0;
+    uint32_t max_lut_bits = 1;
+    for (const DecodeJob &j : jobs) {
+        const HuffParsed &hp = *j.hp;
+        if (!j.count) continue;
+        if (hp.single) {
+            if (hp.single_count != j.count) return fail(ctx, ASZ_E_DATA, "Huffman payload length does not match its value count");
+            if (j.wide) CK(launch_fill<int64_t>((int64_t *)j.out, j.count, (int64_t)hp.offset, st));
+            else CK(launch_fill<int32_t>((int32_t *)j.out, j.count, (int32_t)hp.offset, st));
+            continue;
+        }
+        DecStream d{};
+        d.bit_begin = hp.payload_off * 8;
+        d.bit_end = d.bit_begin + hp.payload_bits;
+        d.chunk0 = nchunks;
+        d.nchunks = std::max<u64>(1, (hp.payload_bits + C - 1) / C);
+        d.tile0 = tile_stream.size();
+        d.lut_off = luts.size();
+        d.child_off = childs.size();
+        d.count = j.count;
+        d.offset = hp.offset;
+        d.out = j.out;
+        d.lut_bits = hp.lut_bits;
+        d.wide = j.wide ? 1 : 0;
+        luts.insert(luts.end(), hp.lut.begin(), hp.lut.end());
+        childs.insert(childs.end(), hp.child.begin(), hp.child.end());
+        const u64 tiles = (d.nchunks + kDecodeTile - 1) / kDecodeTile;
+        tile_stream.insert(tile_stream.end(), tiles, (uint32_t)ds.size());
+        nchunks += d.nchunks;
+        max_lut_bits = std::max(max_lut_bits, hp.lut_bits);
+        ds.push_back(d);
     }
-    // Tables.
-    const u64 lut_bytes = hp.lut.size() * sizeof(LutEntry), child_bytes = hp.child.size() * sizeof(uint32_t);
-    CK(ctx->codes.reserve(lut_bytes + child_bytes + 16));
-    CK(cudaMemcpyAsync(ctx->codes.p, hp.lut.data(), lut_bytes, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync((uint8_t *)ctx->codes.p + lut_bytes, hp.child.data(), child_bytes, cudaMemcpyHostToDevice, st));
-    DecodeTables dt{(const LutEntry *)ctx->codes.p, (const uint32_t *)((uint8_t *)ctx->codes.p + lut_bytes), hp.lut_bits};
-    const u64 abs_off = base_off + hp.payload_off;
-    const uint8_t *aligned = d_base + (abs_off & ~3ull);
-    const u64 bit_begin = (abs_off & 3ull) * 8, bit_end = bit_begin + hp.payload_bits;
-    const u64 C = 4096;
-    const u64 nch = std::max<u64>(1, (hp.payload_bits + C - 1) / C);
-    CK(ctx->chunks.reserve(4 * nch * 8 + 64));
-    u64 *d_start = ctx->chunks.as<u64>(), *d_end = d_start + nch, *d_cnt = d_end + nch, *d_off = d_cnt + nch;
-    uint32_t *d_flag = (uint32_t *)(d_off + nch);
-    std::vector<u64> start(nch);
-    for (u64 k = 0; k < nch; k++) start[k] = bit_begin + k * C;
-    CK(cudaMemcpyAsync(d_start, start.data(), nch * 8, cudaMemcpyHostToDevice, st));
-    MiscLayout *dm = ctx->misc.as<MiscLayout>();
-    CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+    CK(cudaMemsetAsync(&dm->dec_err, 0, 4, st));
+    if (ds.empty()) return ASZ_OK;
+    if (childs.empty()) childs.push_back(0);
+    // Tables and descriptors in one upload.
+    const u64 ds_bytes = ds.size() * sizeof(DecStream), ts_bytes = tile_stream.size() * 4, lut_bytes = luts.size() * sizeof(LutEntry),
+              ch_bytes = childs.size() * 4;
+    auto al = [](u64 x) { return (x + 255) & ~255ull; };
+    const u64 o_ts = al(ds_bytes), o_lut = o_ts + al(ts_bytes), o_ch = o_lut + al(lut_bytes), total = o_ch + al(ch_bytes);
+    std::vector<uint8_t> blob(total);
+    std::memcpy(blob.data(), ds.data(), ds_bytes);
+    std::memcpy(blob.data() + o_ts, tile_stream.data(), ts_bytes);
+    std::memcpy(blob.data() + o_lut, luts.data(), lut_bytes);
+    std::memcpy(blob.data() + o_ch, childs.data(), ch_bytes);
+    CK(ctx->codes.reserve(total));
+    uint8_t *dc = ctx->codes.as<uint8_t>();
+    CK(cudaMemcpyAsync(dc, blob.data(), total, cudaMemcpyHostToDevice, st));
+    const DecStream *d_ds = (const DecStream *)dc;
+    const uint32_t *d_ts = (const uint32_t *)(dc + o_ts);
+    const LutEntry *d_lut = (const LutEntry *)(dc + o_lut);
+    const uint32_t *d_ch = (const uint32_t *)(dc + o_ch);
+    // Per-chunk arrays: start, end, count, off (count + 1 entries for the scan).
+    CK(ctx->chunks.reserve(4 * (nchunks + 1) * 8 + 64));
+    u64 *d_start = ctx->chunks.as<u64>(), *d_end = d_start + nchunks + 1, *d_cnt = d_end + nchunks + 1, *d_off = d_cnt + nchunks + 1;
+    CK(cudaMemsetAsync(d_cnt + nchunks, 0, 8, st));
+    const uint32_t nst = (uint32_t)ds.size();
+    const u64 ntiles = tile_stream.size();
     for (u64 it = 0;; it++) {
         {
-            ProfScope ps(ctx, "huff_decode_sync", (hp.payload_bits + 7) / 8);
-            CK(launch_decode_sync(aligned, bit_begin, bit_end, C, nch, dt, d_start, d_end, d_cnt, &dm->err, st));
+            ProfScope ps(ctx, "huff_decode_sync", 0);
+            CK(launch_decode_sync(d_base, C, d_ds, d_ts, ntiles, max_lut_bits, d_lut, d_ch, it == 0 ? 1 : 0, d_start, d_end, d_cnt,
+                                  &dm->dec_err, st));
         }
-        CK(cudaMemsetAsync(d_flag, 0, 4, st));
-        CK(launch_decode_restart(nch, d_end, d_start, d_flag, st));
-        uint32_t flag;
-        CK(cudaMemcpyAsync(&flag, d_flag, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemsetAsync(&dm->dec_changed, 0, 4, st));
+        CK(launch_decode_restart(d_ds, nst, nchunks, d_end, d_start, &dm->dec_changed, st));
+        uint32_t changed;
+        CK(cudaMemcpyAsync(&changed, &dm->dec_changed, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        if (!flag) break;
-        if (it > nch + 2) return fail(ctx, ASZ_E_DATA, "Huffman payload does not synchronise");
+        if (!changed) break;
+        // Every pass that moves a start fixes at least one more chunk, so this ends.
+        if (it > nchunks + 2) return fail(ctx, ASZ_E_DATA, "Huffman payload does not synchronise");
     }
     size_t tb = 0;
-    CK(launch_scan_u64(d_cnt, d_off, nch, nullptr, tb, st));
+    CK(launch_scan_u64(d_cnt, d_off, nchunks + 1, nullptr, tb, st));
     CK(ctx->cubtmp.reserve(tb));
     tb = ctx->cubtmp.cap;
-    CK(launch_scan_u64(d_cnt, d_off, nch, ctx->cubtmp.p, tb, st));
-    u64 last[3];
-    CK(cudaMemcpyAsync(&last[0], d_off + nch - 1, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&last[1], d_cnt + nch - 1, 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&last[2], d_end + nch - 1, 8, cudaMemcpyDeviceToHost, st));
-    uint32_t errw;
-    CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (errw) return fail(ctx, ASZ_E_DATA, "corrupt Huffman payload");
-    if (last[2] != bit_end) return fail(ctx, ASZ_E_DATA, "Huffman payload ends inside a code");
-    if (last[0] + last[1] != count)
-        return fail(ctx, ASZ_E_DATA, last[0] + last[1] < count ? "Huffman payload contains too few values"
-                                                               : "Huffman payload contains too many values");
-    ProfScope ps_w(ctx, "huff_decode_write", (hp.payload_bits + 7) / 8 + count * (wide ? 8 : 4));
-    if (wide)
-        CK(launch_decode_write<int64_t>(aligned, bit_begin, bit_end, C, nch, dt, hp.offset, d_start, d_off, (int64_t *)d_out,
-                                        count, &dm->err, st));
-    else
-        CK(launch_decode_write<int32_t>(aligned, bit_begin, bit_end, C, nch, dt, hp.offset, d_start, d_off, (int32_t *)d_out,
-                                        count, &dm->err, st));
+    CK(launch_scan_u64(d_cnt, d_off, nchunks + 1, ctx->cubtmp.p, tb, st));
+    CK(launch_decode_check(d_ds, nst, d_off, d_end, &dm->dec_err, st));
+    ProfScope ps_w(ctx, "huff_decode_write", 0);
+    CK(launch_decode_write(d_base, C, d_ds, d_ts, ntiles, max_lut_bits, d_lut, d_ch, d_start, d_off, &dm->dec_err, st));
     return ASZ_OK;
 }
 
@@ -1369,9 +1408,9 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     unsigned long long raw = ZSTD_getFrameContentSize(in, len);
     if (raw == ZSTD_CONTENTSIZE_ERROR || raw == ZSTD_CONTENTSIZE_UNKNOWN || raw > (1ull << 40))
         return fail(ctx, ASZ_E_DATA, "ZSTD_decompress error in decompress()");
-    CK(ctx->raw_in.reserve(raw + 16));
+    CK(ctx->raw_in.reserve(raw + kDecodePad));
     uint8_t *const bsp = ctx->raw_in.p;
-    std::memset(bsp + raw, 0, 16);
+    std::memset(bsp + raw, 0, kDecodePad);
     size_t got;
     {
         HostScope hs(ctx, "host:zstd");
@@ -1418,6 +1457,10 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         if (!counts[s]) continue;
         std::string e;
         if (!parse_stream(bsp, raw, pos, hp[s], e)) return fail(ctx, ASZ_E_DATA, e);
+        // Every code is at least one bit, and a single-symbol stream still has to fit the field's
+        // bookkeeping: larger counts are corrupt (and would overflow the output sizing).
+        if (hp[s].single ? counts[s] > (1ull << 40) : counts[s] > hp[s].payload_bits)
+            return fail(ctx, ASZ_E_DATA, "compressed stream has an impossible value count");
     }
     const float abs_eb = rel_eb * (mx - mn);
     Geometry G;
@@ -1430,9 +1473,9 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         if (counts[l + 2] < G.rounds[l].qb_total) return fail(ctx, ASZ_E_DATA, "compressed stream has too few QBs");
     // Device: stream bytes, t codes, QB streams.
     CK(ctx->misc.reserve(sizeof(MiscLayout)));
-    CK(ctx->pre.reserve(raw + 16));
+    CK(ctx->pre.reserve(raw + kDecodePad));
     auto t0 = clk::now();
-    CK(cudaMemcpyAsync(ctx->pre.p, bsp, raw + 16, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->pre.p, bsp, raw + kDecodePad, cudaMemcpyHostToDevice, st));
     R.h2d_s += secs(t0, clk::now());
     std::vector<u64> qoff(L + 1);
     u64 qtot = 0;
@@ -1443,13 +1486,12 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     CK(ctx->tint.reserve(std::max<u64>(counts[0], 1) * 8));
     CK(ctx->qb.reserve(std::max<u64>(qtot, 1) * 4));
     std::optional<HostScope> hs_dec(std::in_place, ctx, "host:huffman_decode");
-    if (counts[0]) {
-        rc = gpu_decode(ctx, hp[0], counts[0], ctx->pre.as<uint8_t>(), 0, ctx->tint.p, true, st);
-        if (rc) return rc;
-    }
-    for (u64 s = 0; s <= L; s++) {
-        if (!counts[s + 1]) continue;
-        rc = gpu_decode(ctx, hp[s + 1], counts[s + 1], ctx->pre.as<uint8_t>(), 0, ctx->qb.as<int32_t>() + qoff[s], false, st);
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    {
+        std::vector<DecodeJob> jobs;
+        jobs.push_back({&hp[0], counts[0], ctx->tint.p, true});
+        for (u64 s = 0; s <= L; s++) jobs.push_back({&hp[s + 1], counts[s + 1], ctx->qb.as<int32_t>() + qoff[s], false});
+        rc = gpu_decode_all(ctx, jobs, ctx->pre.as<uint8_t>(), dm, st);
         if (rc) return rc;
     }
     hs_dec.reset();
@@ -1465,7 +1507,6 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     CK(ctx->axis.reserve(std::max<size_t>(G.ent.size(), 1) * sizeof(AxisEntry)));
     const AxisEntry *d_ent = ctx->axis.as<AxisEntry>();
     CK(cudaMemcpyAsync(ctx->axis.p, G.ent.data(), G.ent.size() * sizeof(AxisEntry), cudaMemcpyHostToDevice, st));
-    MiscLayout *dm = ctx->misc.as<MiscLayout>();
     CK(cudaMemsetAsync(&dm->err, 0, 4, st));
     {
         ProfScope ps(ctx, "pivot_decompress", G.pivots * 8);
@@ -1476,10 +1517,16 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_ent, ctx->tint.as<int64_t>(),
                                    ctx->qb.as<int32_t>() + qoff[l + 1], d_out, &dm->err, st));
     }
-    uint32_t errw;
+    uint32_t errw, decw;
     CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&decw, &dm->dec_err, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     hs_rec.reset();
+    // Payload errors first: the reconstruction ran on whatever was decoded (bounded, no faults).
+    if (decw & (8u | 16u)) return fail(ctx, ASZ_E_DATA, "corrupt Huffman payload");
+    if (decw & 128u) return fail(ctx, ASZ_E_DATA, "Huffman payload ends inside a code");
+    if (decw & 32u) return fail(ctx, ASZ_E_DATA, "Huffman payload contains too few values");
+    if (decw & 64u) return fail(ctx, ASZ_E_DATA, "Huffman payload contains too many values");
     if (errw) return fail(ctx, ASZ_E_DEVICE, "reconstruction kernels reported an internal error");
     R.core_s = secs(t_core, clk::now());
     if (!out_on_device) {

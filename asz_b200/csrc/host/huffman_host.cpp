@@ -287,6 +287,11 @@ bool parse_stream(const uint8_t *buf, uint64_t len, uint64_t &pos, HuffParsed &o
         o.payload_off = pos;
         return true;
     }
+    // Compare in bits first: a corrupt length near 2^64 must not wrap when rounded up to bytes.
+    if (w > (len - pos) * 8) {
+        err = "truncated Huffman payload";
+        return false;
+    }
     o.payload_bits = w;
     o.payload_off = pos;
     uint64_t bytes = (w + 7) >> 3;

@@ -71,98 +71,221 @@ __global__ void encode_kernel(const T *__restrict__ s, uint64_t n, int64_t offse
 // Longer codes continue through child[2*node+bit] (a value >= 0x80000000 marks a leaf whose
 // symbol index is the low bits).
 
-__device__ __forceinline__ uint64_t peek64(const uint8_t *__restrict__ p, uint64_t bit) {
-    // Little-endian 64-bit window starting at `bit`; the buffer is padded by 16 bytes.
-    const uint64_t byte = bit >> 3;
-    const uint32_t *w = (const uint32_t *)(p + (byte & ~3ull));
-    uint64_t lo = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
-    uint64_t hi = (uint64_t)w[2];
-    uint32_t sh = (uint32_t)((byte & 3) * 8 + (bit & 7));
-    return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-}
+// Bit reader with read-ahead: `buf` holds the next `nb` payload bits (LSB-first) and is topped up
+// to at least 32 bits (the longest code) before each codeword from a queue of 32-bit words. The
+// queue is fed by 16-byte loads issued one block ahead, so a load's latency overlaps the decoding
+// of the ~128 bits before it is needed. `payload` is 16-byte aligned; reads run at most 48 bytes
+// past the current position and the stream buffer is padded for that.
+struct BitReader {
+    const uint4 *p;
+    uint64_t idx;      // next 16-byte block to request
+    uint4 nxt;         // requested block
+    uint64_t c0, c1;   // current block, words consumed from the low end
+    uint32_t cw;       // words left in (c0, c1)
+    uint64_t buf;
+    uint32_t nb;
 
-// Decode one codeword at `bit`; returns its symbol index and advances `bit`.
-__device__ __forceinline__ uint32_t decode_one(const uint8_t *__restrict__ p, uint64_t &bit, DecodeTables dt) {
-    uint64_t win = peek64(p, bit);
-    LutEntry e = dt.lut[win & ((1u << dt.lut_bits) - 1)];
+    __device__ __forceinline__ void load_cur(const uint4 &v) {
+        c0 = (uint64_t)v.x | ((uint64_t)v.y << 32);
+        c1 = (uint64_t)v.z | ((uint64_t)v.w << 32);
+        cw = 4;
+    }
+    __device__ __forceinline__ uint32_t take() {
+        const uint32_t w = (uint32_t)c0;
+        c0 = (c0 >> 32) | (c1 << 32);
+        c1 >>= 32;
+        if (--cw == 0) {
+            load_cur(nxt);
+            nxt = __ldg(p + idx++);
+        }
+        return w;
+    }
+    __device__ __forceinline__ void init(const uint8_t *payload, uint64_t bit) {
+        p = reinterpret_cast<const uint4 *>(payload);
+        idx = bit >> 7;
+        load_cur(__ldg(p + idx));
+        nxt = __ldg(p + idx + 1);
+        idx += 2;
+        for (uint32_t i = (uint32_t)((bit >> 5) & 3); i; i--) take();
+        const uint32_t skip = (uint32_t)(bit & 31);
+        buf = (uint64_t)(take() >> skip);
+        nb = 32 - skip;
+        refill();
+    }
+    __device__ __forceinline__ void refill() {
+        if (nb < 32) {
+            buf |= (uint64_t)take() << nb;
+            nb += 32;
+        }
+    }
+    __device__ __forceinline__ void drop(uint32_t n) {
+        buf >>= n;
+        nb -= n;
+    }
+};
+
+// Decode one codeword through the shared-memory table `lut`; returns the symbol index, or
+// 0xffffffff for a path that leaves the tree. Advances `bit` by the code length.
+__device__ __forceinline__ uint32_t decode_sym(BitReader &br, uint64_t &bit, const LutEntry *lut, uint32_t lut_bits,
+                                               const uint32_t *__restrict__ child) {
+    br.refill();
+    const LutEntry e = lut[br.buf & ((1u << lut_bits) - 1)];
     if (e.len) {
+        br.drop(e.len);
         bit += e.len;
         return e.sym;
     }
     uint32_t node = e.sym;
-    uint32_t used = dt.lut_bits;
-    win >>= dt.lut_bits;
-    // Codes are at most 32 bits, so the 64-bit window always holds the rest.
+    uint32_t used = lut_bits;
+    uint64_t b = br.buf >> lut_bits;
+    // Codes are at most 32 bits and the buffer holds at least 32.
     while (true) {
-        uint32_t c = dt.child[2 * node + (uint32_t)(win & 1)];
-        win >>= 1;
+        const uint32_t c = __ldg(child + 2 * node + (uint32_t)(b & 1));
+        b >>= 1;
         used++;
         if (c & 0x80000000u) {
+            br.drop(used);
             bit += used;
             return c & 0x7fffffffu;
         }
         node = c;
-        if (used > 40) {  // impossible for a validated tree; stop instead of running on
+        if (used >= 32) {  // impossible for a validated tree; stop instead of running on
+            br.drop(used);
             bit += used;
             return 0xffffffffu;
         }
     }
 }
 
-// Pass A: each chunk decodes from start[k] until it reaches the next chunk's start bit and
-// records where it stopped (end[k]) and how many symbols it produced (count[k]).
-// Bit positions are absolute from the 4-byte-aligned `payload` base: the stream occupies
-// [bit_begin, bit_end) and chunk k covers [bit_begin + k*chunk_bits, bit_begin + (k+1)*chunk_bits).
-__global__ void decode_sync_kernel(const uint8_t *__restrict__ payload, uint64_t bit_begin, uint64_t bit_end,
-                                   uint64_t chunk_bits, uint64_t nchunks, DecodeTables dt, const uint64_t *__restrict__ start,
-                                   uint64_t *__restrict__ end, uint64_t *__restrict__ count, uint32_t *err_word) {
-    uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (k >= nchunks) return;
-    uint64_t bit = start[k];
-    const uint64_t lim = min(bit_begin + (k + 1) * chunk_bits, bit_end);
-    uint64_t c = 0;
-    while (bit < lim) {
-        uint32_t s = decode_one(payload, bit, dt);
-        if (s == 0xffffffffu) {
-            atomicOr(err_word, 8u);
-            break;
-        }
-        c++;
-    }
-    end[k] = bit;
-    count[k] = c;
+// ---------------------------------------------------------------------------------------------
+// Batched decoding of every stream of a .asz in one launch per pass. Chunks of chunk_bits bits
+// are numbered globally (stream after stream); tiles of blockDim.x chunks never cross a stream,
+// so a CTA stages one stream's lookup table for a tile. Bit positions are absolute from the
+// 16-byte aligned stream buffer `base`.
+
+__device__ __forceinline__ void stage_lut(LutEntry *lut_sh, const LutEntry *__restrict__ lut, uint32_t lut_bits) {
+    for (uint32_t i = threadIdx.x; i < (1u << lut_bits); i += blockDim.x) lut_sh[i] = lut[i];
 }
 
-// After a pass: the next start of chunk k+1 is end[k]. Flags whether anything moved.
-__global__ void decode_restart_kernel(uint64_t nchunks, const uint64_t *__restrict__ end, uint64_t *__restrict__ start,
-                                      uint32_t *changed) {
-    uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (k == 0 || k >= nchunks) return;
-    uint64_t s = end[k - 1];
-    if (s != start[k]) {
-        start[k] = s;
-        *changed = 1u;
+// Pass A over all tiles: chunk k decodes from its start until it reaches the next chunk's first
+// bit, recording where it stopped (end[k]) and how many values it produced (count[k]). On the
+// first pass the start is the chunk's first bit; later passes start where chunk k-1 ended.
+__global__ void __launch_bounds__(256)
+    decode_sync_kernel(const uint8_t *__restrict__ base, uint64_t chunk_bits, const DecStream *__restrict__ streams,
+                       const uint32_t *__restrict__ tile_stream, uint64_t ntiles, const LutEntry *__restrict__ luts,
+                       const uint32_t *__restrict__ childs, int first_pass, uint64_t *__restrict__ start,
+                       uint64_t *__restrict__ end, uint64_t *__restrict__ count, uint32_t *err_word) {
+    extern __shared__ LutEntry lut_sh[];
+    uint32_t staged = 0xffffffffu;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t si = tile_stream[tile];
+        const DecStream d = streams[si];
+        if (si != staged) {
+            __syncthreads();
+            stage_lut(lut_sh, luts + d.lut_off, d.lut_bits);
+            __syncthreads();
+            staged = si;
+        }
+        const uint64_t kl = (tile - d.tile0) * blockDim.x + threadIdx.x;
+        if (kl >= d.nchunks) continue;
+        const uint64_t k = d.chunk0 + kl;
+        uint64_t bit = first_pass ? d.bit_begin + kl * chunk_bits : start[k];
+        if (first_pass) start[k] = bit;
+        const uint64_t lim = min(d.bit_begin + (kl + 1) * chunk_bits, d.bit_end);
+        uint64_t c = 0;
+        if (bit < lim) {
+            BitReader br;
+            br.init(base, bit);
+            while (bit < lim) {
+                const uint32_t sym = decode_sym(br, bit, lut_sh, d.lut_bits, childs + d.child_off);
+                if (sym == 0xffffffffu) {
+                    atomicOr(err_word, 8u);
+                    break;
+                }
+                c++;
+            }
+        }
+        end[k] = bit;
+        count[k] = c;
     }
 }
 
-// Pass B: write symbols (value = index + offset) at out[off[k] ...].
-template <class T>
-__global__ void decode_write_kernel(const uint8_t *__restrict__ payload, uint64_t bit_begin, uint64_t bit_end,
-                                    uint64_t chunk_bits, uint64_t nchunks, DecodeTables dt, int64_t offset,
-                                    const uint64_t *__restrict__ start, const uint64_t *__restrict__ off, T *__restrict__ out,
-                                    uint64_t nout, uint32_t *err_word) {
-    uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (k >= nchunks) return;
-    uint64_t bit = start[k];
-    const uint64_t lim = min(bit_begin + (k + 1) * chunk_bits, bit_end);
-    uint64_t o = off[k];
-    while (bit < lim) {
-        uint32_t s = decode_one(payload, bit, dt);
-        if (s == 0xffffffffu || o >= nout) {
-            atomicOr(err_word, 16u);
-            break;
+__device__ __forceinline__ uint32_t stream_of_chunk(const DecStream *__restrict__ streams, uint32_t nstreams, uint64_t k) {
+    uint32_t lo = 0, hi = nstreams;  // last stream with chunk0 <= k
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (streams[mid].chunk0 <= k) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// After a pass: the start of chunk k (not the first of its stream) becomes end[k-1]. Flags
+// whether anything moved.
+__global__ void decode_restart_kernel(const DecStream *__restrict__ streams, uint32_t nstreams, uint64_t nchunks,
+                                      const uint64_t *__restrict__ end, uint64_t *__restrict__ start, uint32_t *changed) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nchunks; k += (uint64_t)gridDim.x * blockDim.x) {
+        if (streams[stream_of_chunk(streams, nstreams, k)].chunk0 == k) continue;
+        const uint64_t s = end[k - 1];
+        if (s != start[k]) {
+            start[k] = s;
+            *changed = 1u;
         }
-        out[o++] = (T)((int64_t)s + offset);
+    }
+}
+
+// Per stream, once the starts are stable: the values decoded must equal the stream's count and
+// the last chunk must end exactly at the payload's last bit. off[] is the exclusive scan of
+// count[] over all chunks (nchunks + 1 entries).
+__global__ void decode_check_kernel(const DecStream *__restrict__ streams, uint32_t nstreams, const uint64_t *__restrict__ off,
+                                    const uint64_t *__restrict__ end, uint32_t *err_word) {
+    const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
+    if (si >= nstreams) return;
+    const DecStream d = streams[si];
+    const uint64_t got = off[d.chunk0 + d.nchunks] - off[d.chunk0];
+    if (got < d.count) atomicOr(err_word, 32u);
+    if (got > d.count) atomicOr(err_word, 64u);
+    if (end[d.chunk0 + d.nchunks - 1] != d.bit_end) atomicOr(err_word, 128u);
+}
+
+// Pass B over all tiles: write the values (symbol index + offset) of chunk k at its offset in its
+// stream's output (int64 for the t stream, int32 for QB streams).
+__global__ void __launch_bounds__(256)
+    decode_write_kernel(const uint8_t *__restrict__ base, uint64_t chunk_bits, const DecStream *__restrict__ streams,
+                        const uint32_t *__restrict__ tile_stream, uint64_t ntiles, const LutEntry *__restrict__ luts,
+                        const uint32_t *__restrict__ childs, const uint64_t *__restrict__ start,
+                        const uint64_t *__restrict__ off, uint32_t *err_word) {
+    extern __shared__ LutEntry lut_sh[];
+    uint32_t staged = 0xffffffffu;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t si = tile_stream[tile];
+        const DecStream d = streams[si];
+        if (si != staged) {
+            __syncthreads();
+            stage_lut(lut_sh, luts + d.lut_off, d.lut_bits);
+            __syncthreads();
+            staged = si;
+        }
+        const uint64_t kl = (tile - d.tile0) * blockDim.x + threadIdx.x;
+        if (kl >= d.nchunks) continue;
+        const uint64_t k = d.chunk0 + kl;
+        uint64_t bit = start[k];
+        const uint64_t lim = min(d.bit_begin + (kl + 1) * chunk_bits, d.bit_end);
+        if (bit >= lim) continue;
+        uint64_t o = off[k] - off[d.chunk0];
+        BitReader br;
+        br.init(base, bit);
+        while (bit < lim) {
+            const uint32_t sym = decode_sym(br, bit, lut_sh, d.lut_bits, childs + d.child_off);
+            if (sym == 0xffffffffu || o >= d.count) {
+                atomicOr(err_word, 16u);
+                break;
+            }
+            const int64_t v = (int64_t)sym + d.offset;
+            if (d.wide) static_cast<int64_t *>(d.out)[o] = v;
+            else static_cast<int32_t *>(d.out)[o] = (int32_t)v;
+            o++;
+        }
     }
 }
 
@@ -205,28 +328,41 @@ cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void 
     return cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, (int64_t)n, st);
 }
 
-cudaError_t launch_decode_sync(const uint8_t *payload, uint64_t bit_begin, uint64_t bit_end, uint64_t chunk_bits,
-                               uint64_t nchunks, DecodeTables dt, const uint64_t *start, uint64_t *end, uint64_t *count,
-                               uint32_t *err, cudaStream_t st) {
-    decode_sync_kernel<<<(unsigned)((nchunks + 127) / 128), 128, 0, st>>>(payload, bit_begin, bit_end, chunk_bits, nchunks,
-                                                                           dt, start, end, count, err);
+// Persistent decode grid: up to 6 CTAs of 256 threads per SM (a table takes up to 32 KB).
+static unsigned decode_grid(uint64_t ntiles) { return (unsigned)(ntiles < 148 * 6 ? (ntiles ? ntiles : 1) : 148 * 6); }
+
+cudaError_t launch_decode_sync(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
+                               uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
+                               int first_pass, uint64_t *start, uint64_t *end, uint64_t *count, uint32_t *err, cudaStream_t st) {
+    const size_t sh = ((size_t)1 << max_lut_bits) * sizeof(LutEntry);
+    decode_sync_kernel<<<decode_grid(ntiles), kDecodeTile, sh, st>>>(base, chunk_bits, streams, tile_stream, ntiles, luts,
+                                                                      childs, first_pass, start, end, count, err);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_decode_restart(uint64_t nchunks, const uint64_t *end, uint64_t *start, uint32_t *changed,
-                                  cudaStream_t st) {
-    decode_restart_kernel<<<(unsigned)((nchunks + 255) / 256), 256, 0, st>>>(nchunks, end, start, changed);
+cudaError_t launch_decode_restart(const DecStream *streams, uint32_t nstreams, uint64_t nchunks, const uint64_t *end,
+                                  uint64_t *start, uint32_t *changed, cudaStream_t st) {
+    const uint64_t b = (nchunks + 255) / 256;
+    decode_restart_kernel<<<(unsigned)(b < 148 * 8 ? (b ? b : 1) : 148 * 8), 256, 0, st>>>(streams, nstreams, nchunks, end, start,
+                                                                                         changed);
     count_launch();
     return cudaGetLastError();
 }
 
-template <class T>
-cudaError_t launch_decode_write(const uint8_t *payload, uint64_t bit_begin, uint64_t bit_end, uint64_t chunk_bits,
-                                uint64_t nchunks, DecodeTables dt, int64_t offset, const uint64_t *start, const uint64_t *off,
-                                T *out, uint64_t nout, uint32_t *err, cudaStream_t st) {
-    decode_write_kernel<T><<<(unsigned)((nchunks + 127) / 128), 128, 0, st>>>(payload, bit_begin, bit_end, chunk_bits,
-                                                                               nchunks, dt, offset, start, off, out, nout, err);
+cudaError_t launch_decode_check(const DecStream *streams, uint32_t nstreams, const uint64_t *off, const uint64_t *end,
+                                uint32_t *err, cudaStream_t st) {
+    decode_check_kernel<<<(nstreams + 63) / 64, 64, 0, st>>>(streams, nstreams, off, end, err);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_write(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
+                                uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
+                                const uint64_t *start, const uint64_t *off, uint32_t *err, cudaStream_t st) {
+    const size_t sh = ((size_t)1 << max_lut_bits) * sizeof(LutEntry);
+    decode_write_kernel<<<decode_grid(ntiles), kDecodeTile, sh, st>>>(base, chunk_bits, streams, tile_stream, ntiles, luts, childs,
+                                                                       start, off, err);
     count_launch();
     return cudaGetLastError();
 }
@@ -246,12 +382,6 @@ template cudaError_t launch_encode<int32_t>(const int32_t *, uint64_t, int64_t, 
                                             uint32_t *, cudaStream_t);
 template cudaError_t launch_encode<int64_t>(const int64_t *, uint64_t, int64_t, const CodeEntry *, uint64_t *, void *, size_t &,
                                             uint32_t *, cudaStream_t);
-template cudaError_t launch_decode_write<int32_t>(const uint8_t *, uint64_t, uint64_t, uint64_t, uint64_t, DecodeTables,
-                                                  int64_t, const uint64_t *, const uint64_t *, int32_t *, uint64_t, uint32_t *,
-                                                  cudaStream_t);
-template cudaError_t launch_decode_write<int64_t>(const uint8_t *, uint64_t, uint64_t, uint64_t, uint64_t, DecodeTables,
-                                                  int64_t, const uint64_t *, const uint64_t *, int64_t *, uint64_t, uint32_t *,
-                                                  cudaStream_t);
 template cudaError_t launch_fill<int32_t>(int32_t *, uint64_t, int32_t, cudaStream_t);
 template cudaError_t launch_fill<int64_t>(int64_t *, uint64_t, int64_t, cudaStream_t);
 

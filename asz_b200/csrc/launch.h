@@ -33,11 +33,19 @@ struct LutEntry {
     uint32_t len;
 };
 
-struct DecodeTables {
-    const LutEntry *lut;
-    const uint32_t *child;
-    uint32_t lut_bits;
+// One stream of a batched decode (see k_huff.cu). Chunks of the stream are chunk0 .. chunk0 +
+// nchunks - 1 in the global numbering; its tiles start at tile0.
+struct DecStream {
+    uint64_t bit_begin, bit_end;   // payload bits, absolute from the stream buffer base
+    uint64_t chunk0, nchunks, tile0;
+    uint64_t lut_off, child_off;   // entries into the batched table arenas
+    uint64_t count;                // values the stream must produce
+    int64_t offset;                // added to each symbol index
+    void *out;                     // int64 values when wide, else int32
+    uint32_t lut_bits, wide;
 };
+
+constexpr uint32_t kDecodeTile = 256;  // chunks per tile (threads per decode CTA)
 
 cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st);
 cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
@@ -88,15 +96,16 @@ template <class T>
 cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntry *tab, uint64_t *bitoff, void *tmp,
                           size_t &tmp_bytes, uint32_t *out, cudaStream_t st);
 cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st);
-cudaError_t launch_decode_sync(const uint8_t *payload, uint64_t bit_begin, uint64_t bit_end, uint64_t chunk_bits,
-                               uint64_t nchunks, DecodeTables dt, const uint64_t *start, uint64_t *end, uint64_t *count,
-                               uint32_t *err, cudaStream_t st);
-cudaError_t launch_decode_restart(uint64_t nchunks, const uint64_t *end, uint64_t *start, uint32_t *changed,
-                                  cudaStream_t st);
-template <class T>
-cudaError_t launch_decode_write(const uint8_t *payload, uint64_t bit_begin, uint64_t bit_end, uint64_t chunk_bits,
-                                uint64_t nchunks, DecodeTables dt, int64_t offset, const uint64_t *start, const uint64_t *off,
-                                T *out, uint64_t nout, uint32_t *err, cudaStream_t st);
+cudaError_t launch_decode_sync(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
+                               uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
+                               int first_pass, uint64_t *start, uint64_t *end, uint64_t *count, uint32_t *err, cudaStream_t st);
+cudaError_t launch_decode_restart(const DecStream *streams, uint32_t nstreams, uint64_t nchunks, const uint64_t *end,
+                                  uint64_t *start, uint32_t *changed, cudaStream_t st);
+cudaError_t launch_decode_check(const DecStream *streams, uint32_t nstreams, const uint64_t *off, const uint64_t *end,
+                                uint32_t *err, cudaStream_t st);
+cudaError_t launch_decode_write(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
+                                uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
+                                const uint64_t *start, const uint64_t *off, uint32_t *err, cudaStream_t st);
 template <class T>
 cudaError_t launch_fill(T *out, uint64_t n, T v, cudaStream_t st);
 

@@ -151,3 +151,43 @@ def test_corrupt_streams_fail_cleanly(gpu_ctx):
     assert len(raw) > 0
     dec, _ = gpu_ctx.decompress(blob, data.shape, case["rel_eb"], p)
     assert np.array_equal(dec.view(np.uint32), out.view(np.uint32))
+
+
+def _zstd3(raw: bytes) -> bytes:
+    import ctypes as C
+    z = C.CDLL("libzstd.so.1")
+    z.ZSTD_compressBound.restype = C.c_size_t
+    z.ZSTD_compressBound.argtypes = [C.c_size_t]
+    z.ZSTD_compress.restype = C.c_size_t
+    z.ZSTD_compress.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int]
+    cap = z.ZSTD_compressBound(len(raw))
+    buf = C.create_string_buffer(cap)
+    n = z.ZSTD_compress(buf, cap, raw, len(raw), 3)
+    return buf.raw[:n]
+
+
+def test_corrupt_payload_bits(gpu_ctx):
+    """Bit flips inside the Huffman payloads (re-wrapped in a valid zstd frame): the decoder either
+    reports a corrupt stream or decodes some other valid stream, never faults, and the context
+    keeps working."""
+    import asz_b200.api as api
+    case = golden_cases()[0]
+    data, blob, out = load_golden(case)
+    p = api.default_params(block_pivot_ratio=case["block_pivot_ratio"])
+    raw = O.compress(data, case["rel_eb"], case["plan"], case["family"] == "quintic",
+                     O.default_params(block_pivot_ratio=case["block_pivot_ratio"])).pre_zstd
+    rng = np.random.default_rng(3)
+    errors = 0
+    for _ in range(24):
+        b = bytearray(raw)
+        for _ in range(int(rng.integers(1, 4))):
+            i = int(rng.integers(len(b) // 2, len(b)))
+            b[i] ^= 1 << int(rng.integers(0, 8))
+        try:
+            gpu_ctx.decompress(_zstd3(bytes(b)), data.shape, case["rel_eb"], p)
+        except api.AszError:
+            errors += 1
+    assert errors > 0
+    dec, _ = gpu_ctx.decompress(blob, data.shape, case["rel_eb"], p)
+    assert np.array_equal(dec.view(np.uint32), out.view(np.uint32))
+
