@@ -58,6 +58,8 @@ class Report(C.Structure):
         ("ambiguous_decisions", C.c_uint64), ("reruns", C.c_uint64), ("exact_groups", C.c_uint64),
         ("serial_groups", C.c_uint64), ("exact_window", C.c_uint64), ("exact_undecided", C.c_uint64),
         ("wide_groups", C.c_uint64), ("kernel_launches", C.c_uint64),
+        ("plan_stats_s", C.c_double), ("plan_sample_s", C.c_double), ("plan_lossless_s", C.c_double),
+        ("plan_search_layers", C.c_uint32), ("plan_best_dist", C.c_float * 64),
         ("pivot_stride", C.c_uint32 * 3), ("block_shape", C.c_uint32 * 3), ("block_num", C.c_uint32 * 3),
         ("quintic", C.c_int32), ("plan", C.c_char * (64 * 11 + 1)),
     ]

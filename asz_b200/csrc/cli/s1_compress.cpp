@@ -44,6 +44,28 @@ int main(int argc, char *argv[]) try {
            r.default_slope);
     printf("Get default slope time: %f s\n", r.default_slope_s);
     printf("default_slope=%f\n", r.default_slope);
+    if (!a.have_plan) {
+        // generate_config's lines (generate_config.tpp:654, 672-673): layer i's winner is the plan's
+        // i-th predictor from the end.
+        std::vector<std::string> preds;
+        {
+            std::string pl = r.plan;
+            size_t b = 0;
+            while (b < pl.size()) {
+                size_t e = pl.find(',', b);
+                preds.push_back(pl.substr(b, e == std::string::npos ? std::string::npos : e - b));
+                if (e == std::string::npos) break;
+                b = e + 1;
+            }
+        }
+        for (uint32_t i = 0; i < r.plan_search_layers && i < preds.size(); i++)
+            printf("best_layer_predictor=%s, best_dist=%f\n", preds[preds.size() - 1 - i].c_str(), r.plan_best_dist[i]);
+        // A layer with no candidate ends the search after printing its empty choice (-1e8 start score).
+        if (r.plan_search_layers < p.max_layer_num) printf("best_layer_predictor=, best_dist=%f\n", -1e8f);
+        printf("Generate config breakdown: statistics=%f s,sample prediction=%f s,lossless estimation=%f s\n", r.plan_stats_s,
+               r.plan_sample_s, r.plan_lossless_s);
+        printf("Generate config time: %f s\n", r.plan_s);
+    }
     // print_config (generate_config.tpp:6-49).
     printf("predictor_vec={");
     {

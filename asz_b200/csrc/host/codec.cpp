@@ -149,7 +149,7 @@ struct asz_ctx {
     std::string err;
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
-        classes, axis, pre, chunks, out, proxies, tlist, spill, iota;
+        classes, axis, pre, chunks, out, proxies, tlist, spill, iota, plan_qb, plan_e, plan_aux, plan_pay;
     int tsel_mode = 0;  // 0: certified fast path + exact path for the rest; 1: exact path for all groups
     // Cached glibc log2f tables, keyed by sample count.
     std::map<uint32_t, uint32_t> log2_off;
@@ -583,7 +583,8 @@ void asz_destroy(asz_ctx *c) {
     cudaSetDevice(c->device);
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
-                      &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota})
+                      &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
+                      &c->plan_pay})
         b->release();
     c->pre_zstd.release();
     c->raw_in.release();
@@ -727,7 +728,7 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
         {
             ProfScope ps_slope(ctx, "slope", 0);
             CK(launch_slope_exact(dm->boxes, dm->evals, ne, d_in, dims[1] * dims[2], dims[2], ctx->log2arena.as<float>(),
-                                  R * R, dm->h1, dm->x, dm->m, &dm->err, exact_cap(), ctx->stream));
+                                  R * R, dm->h1, dm->x, dm->m, &dm->err, exact_cap(), 3, ctx->stream));
         }
         uint32_t e1 = 0;
         CK(cudaMemcpyAsync(&e1, &dm->err, 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -740,7 +741,7 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
     if (serial) {
         ProfScope ps_slope(ctx, "slope_serial", 0);
         CK(launch_slope_v0(fg, dm->boxes, dm->evals, ne, d_in, ctx->log2arena.as<float>(), R * R, ctx->scratch.as<uint8_t>(),
-                           sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, ctx->stream));
+                           sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, 3, ctx->stream));
     }
     std::vector<float> h1(3 * ne), x(3 * ne);
     uint32_t m[3], errw;
@@ -815,6 +816,341 @@ struct StreamOut {
     u64 hist_off = 0;
 };
 
+// ---------------------------------------------------------------------------------------------
+// Plan search: param_c::generate_config (c_codes/asz_core/generate_config.tpp:444-678).
+// Per layer, from the finest: for each candidate predictor, the best t on its direction's
+// whole-field AB map (exact map order on the device, glibc log10f here), then a sampled open-loop
+// compression of the original data (device), whose QBs are Huffman-coded (device) and compressed
+// with libzstd level 3 (host threads); the candidate with the best psnr - slope * bit rate wins.
+// The float steps follow the reference build's emitted code: pow in double with the products
+// rounded to float, 0.5f/x for the 1/(2x) factors, fmaf(-slope, h1, psnr) for the t choice,
+// bit rate = zstd_bytes * (8 / samples), psnr = log10f(range^2 / (mse / samples)) * 10, and a
+// separately rounded slope * bit rate in the final score.
+
+struct PlanSearchOut {
+    std::vector<std::string> plan;
+    std::vector<float> dists;  // winning score per layer, finest first
+    double stats_s = 0, sample_s = 0, lossless_s = 0;
+};
+
+int plan_search(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const asz_params &p, float abs_eb, float mn, float mx,
+                float slope, PlanSearchOut &out) {
+    static const char *all9[9] = {"cubic0_120", "cubic0_021", "cubic0_012", "cubic1_120", "cubic1_021",
+                                  "cubic1_012", "cubic2_120", "cubic2_021", "cubic2_012"};
+    static const char *last3[3] = {"cubic0_012", "cubic1_012", "cubic2_012"};
+    static const int nest[3][3] = {{1, 2, 0}, {0, 2, 1}, {0, 1, 2}};  // loop axes per order digit, outer to inner
+    cudaStream_t st = ctx->stream;
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    const std::vector<float> cand_t = candidate_t(p);
+    if (cand_t.size() > 21) return fail(ctx, ASZ_E_UNSUPPORTED, "too many t candidates for the plan search");
+    const float R = mx - mn;
+    FieldGeom fg{};
+    for (int a = 0; a < 3; a++) fg.n[a] = dims[a];
+    u64 ps[3] = {1, 1, 1};
+    out = PlanSearchOut();
+    for (u64 layer = 0; layer < p.max_layer_num; layer++) {
+        const float layer_eb = (float)((double)abs_eb * std::pow((double)p.eb_ratio, (double)layer));
+        const float neg_2_layer_eb = 0.5f / layer_eb;
+        const float stat_eb = layer_eb * p.stat_eb_ratio;
+        const float neg_2_stat_eb = 0.5f / stat_eb;
+        const float lslope = (float)((double)slope * std::pow((double)p.slope_ratio, (double)layer));
+        std::vector<std::string> cands;
+        if (layer < p.full_predictor_search_layer_num) cands.assign(all9, all9 + 9);
+        else cands.assign(last3, last3 + 3);
+        // ---- Best t per direction on its AB map.
+        auto t_stats = clk::now();
+        float best_t[3] = {0.25f, 0.25f, 0.25f};
+        {
+            bool need[3] = {false, false, false};
+            for (auto &c : cands) need[c[5] - '0'] = true;
+            SampleBox boxes[3];
+            int box_dir[3];
+            uint32_t nb = 0, cap = 1;
+            for (int d = 0; d < 3; d++) {
+                if (!need[d] || !(dims[d] > 3 * ps[d])) continue;
+                u64 ps2[3] = {ps[0], ps[1], ps[2]};
+                ps2[d] *= 2;
+                SampleBox &b = boxes[nb];
+                u64 lo[3] = {0, 0, 0}, hi[3] = {dims[0], dims[1], dims[2]};
+                lo[d] = 3 * ps2[d] / 2;
+                hi[d] = dims[d] - 3 * ps2[d] / 2;
+                u64 vol = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+                float q = (float)vol / (float)(ps2[0] * ps2[1] * ps2[2] * p.h1_block_sampling_num);
+                u64 ss = (u64)std::cbrt((double)q);
+                if (ss == 0) ss = 1;
+                u64 n = 1;
+                for (int a = 0; a < 3; a++) {
+                    b.lo[a] = lo[a];
+                    b.hi[a] = hi[a];
+                    b.step[a] = ps2[a] * ss;
+                    n *= hi[a] > lo[a] ? (hi[a] - lo[a] + b.step[a] - 1) / b.step[a] : 0;
+                }
+                u64 dist = ps2[d];
+                for (int a = d + 1; a < 3; a++) dist *= dims[a];
+                b.dist = dist / 2;
+                b.neg_2_stat_eb = neg_2_stat_eb;
+                b.stat_eb = stat_eb;
+                if (n > 0xffffffffull) return fail(ctx, ASZ_E_UNSUPPORTED, "plan-search AB map too large");
+                b.n = (uint32_t)n;
+                b.log2_off = n ? log2_table(ctx, (uint32_t)n) : 0;
+                cap = std::max<uint32_t>(cap, (uint32_t)n);
+                box_dir[nb++] = d;
+            }
+            if (nb) {
+                const uint32_t ne = (uint32_t)cand_t.size();
+                ProxyEval evals[64];
+                for (uint32_t k = 0; k < ne; k++) evals[k] = ProxyEval{cand_t[k], layer_eb};
+                int rc = upload_log2(ctx);
+                if (rc) return rc;
+                CK(cudaMemcpyAsync(dm->boxes, boxes, sizeof(SampleBox) * nb, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(dm->evals, evals, sizeof(ProxyEval) * ne, cudaMemcpyHostToDevice, st));
+                CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+                CK(cudaMemsetAsync(dm->m, 0, sizeof(dm->m), st));
+                bool serial = cap > exact_cap();
+                if (!serial) {
+                    {
+                        ProfScope ps_(ctx, "plan_abmap", 0);
+                        CK(launch_slope_exact(dm->boxes, dm->evals, ne, d_in, dims[1] * dims[2], dims[2], ctx->log2arena.as<float>(),
+                                              R * R, dm->h1, dm->x, dm->m, &dm->err, exact_cap(), nb, st));
+                    }
+                    uint32_t e1 = 0;
+                    CK(cudaMemcpyAsync(&e1, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    if (e1) {
+                        serial = true;
+                        CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+                    }
+                }
+                if (serial) {
+                    uint32_t bcap, tcap;
+                    u64 sstride;
+                    scratch_dims(cap, bcap, tcap, sstride);
+                    CK(ctx->scratch.reserve(3 * sstride));
+                    ProfScope ps_(ctx, "plan_abmap_serial", 0);
+                    CK(launch_slope_v0(fg, dm->boxes, dm->evals, ne, d_in, ctx->log2arena.as<float>(), R * R,
+                                       ctx->scratch.as<uint8_t>(), sstride, cap, bcap, tcap, dm->h1, dm->x, dm->m, &dm->err, nb,
+                                       st));
+                }
+                std::vector<float> h1(nb * ne), x(nb * ne);
+                uint32_t m[3], errw;
+                CK(cudaMemcpyAsync(h1.data(), dm->h1, 4 * nb * ne, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(x.data(), dm->x, 4 * nb * ne, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(m, dm->m, 12, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (errw) return fail(ctx, ASZ_E_DEVICE, "plan-search AB-map kernel reported an internal error");
+                for (uint32_t bi = 0; bi < nb; bi++) {
+                    if (m[bi] == 0) continue;  // empty map: t stays 1/4
+                    auto score = [&](uint32_t k) {
+                        const float psnr = 10.0f * log10f(x[bi * ne + k]);
+                        return std::fma(-lslope, h1[bi * ne + k], psnr);
+                    };
+                    uint32_t k0 = ne;
+                    for (uint32_t k = 0; k < ne; k++)
+                        if (cand_t[k] == 0.25f) k0 = k;
+                    float bt = 0.25f, best;
+                    if (k0 < ne) {
+                        best = score(k0);
+                    } else {
+                        // 1/4 outside the candidate range: evaluate it separately.
+                        return fail(ctx, ASZ_E_UNSUPPORTED, "plan search needs t = 1/4 among the t candidates");
+                    }
+                    for (uint32_t k = 0; k < ne; k++) {
+                        if (cand_t[k] == 0.25f) continue;
+                        const float cur = score(k);
+                        if (cur > best) bt = cand_t[k];
+                        best = cur > best ? cur : best;
+                    }
+                    best_t[box_dir[bi]] = bt;
+                }
+            }
+        }
+        out.stats_s += secs(t_stats, clk::now());
+        // ---- Sampled open-loop compression of every candidate (one launch), and its error sums.
+        auto t_sample = clk::now();
+        const uint32_t nc = (uint32_t)cands.size();
+        std::vector<PlanCand> pc(nc);
+        u64 total = 0;
+        for (uint32_t c = 0; c < nc; c++) {
+            const int dir = cands[c][5] - '0', order = cands[c][9] - '0';
+            PlanCand &q = pc[c];
+            u64 ps2[3] = {ps[0], ps[1], ps[2]};
+            ps2[dir] *= 2;
+            for (int a = 0; a < 3; a++) {
+                q.st[a] = ps2[a] * (a == order ? 1 : p.generate_config_sample_stride);
+                q.lo[a] = a == dir ? ps2[dir] / 2 : 0;
+                q.cnt[a] = dims[a] > q.lo[a] ? (dims[a] - q.lo[a] + q.st[a] - 1) / q.st[a] : 0;
+                q.ax[a] = nest[order][a];
+            }
+            q.off = total;
+            q.hs = ps2[dir] / 2;
+            u64 dist = q.hs;
+            for (int a = dir + 1; a < 3; a++) dist *= dims[a];
+            q.dist = dist;
+            q.right = dims[dir];
+            q.t = best_t[dir];
+            q.eb = layer_eb;
+            q.neg_2_eb = neg_2_layer_eb;
+            q.dir = dir;
+            total += q.cnt[0] * q.cnt[1] * q.cnt[2];
+        }
+        std::vector<u64> num(nc);
+        for (uint32_t c = 0; c < nc; c++) num[c] = pc[c].cnt[0] * pc[c].cnt[1] * pc[c].cnt[2];
+        CK(ctx->plan_qb.reserve(std::max<u64>(total, 1) * 4));
+        CK(ctx->plan_e.reserve(std::max<u64>(total, 1) * 4));
+        const u64 aux_cands = 0, aux_range = (nc * sizeof(PlanCand) + 255) & ~255ull, aux_mse = aux_range + 256;
+        CK(ctx->plan_aux.reserve(aux_mse + 256));
+        uint8_t *aux = ctx->plan_aux.as<uint8_t>();
+        CK(cudaMemcpyAsync(aux + aux_cands, pc.data(), nc * sizeof(PlanCand), cudaMemcpyHostToDevice, st));
+        std::vector<int32_t> rinit(2 * nc);
+        for (uint32_t c = 0; c < nc; c++) {
+            rinit[2 * c] = INT32_MAX;
+            rinit[2 * c + 1] = INT32_MIN;
+        }
+        CK(cudaMemcpyAsync(aux + aux_range, rinit.data(), rinit.size() * 4, cudaMemcpyHostToDevice, st));
+        const PlanCand *d_pc = (const PlanCand *)(aux + aux_cands);
+        int32_t *d_qb = ctx->plan_qb.as<int32_t>();
+        {
+            ProfScope ps_(ctx, "plan_sample", total * 8);
+            CK(launch_plan_sample(d_in, dims[1], dims[2], d_pc, nc, total, d_qb, ctx->plan_e.as<float>(), (int32_t *)(aux + aux_range),
+                                  st));
+        }
+        {
+            ProfScope ps_(ctx, "plan_mse", total * 4);
+            CK(launch_plan_mse(d_pc, nc, ctx->plan_e.as<float>(), (float *)(aux + aux_mse), st));
+        }
+        std::vector<int32_t> ranges(2 * nc);
+        std::vector<float> mse(nc);
+        CK(cudaMemcpyAsync(ranges.data(), aux + aux_range, ranges.size() * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(mse.data(), aux + aux_mse, nc * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        out.sample_s += secs(t_sample, clk::now());
+        // ---- Huffman code of each candidate's QBs (device histogram and encoding), zstd on the host.
+        auto t_lossless = clk::now();
+        std::vector<u64> hist_off(nc, 0);
+        u64 hist_total = 0;
+        for (uint32_t c = 0; c < nc; c++) {
+            if (!num[c]) continue;
+            const u64 range = (u64)((int64_t)ranges[2 * c + 1] - (int64_t)ranges[2 * c]) + 1;
+            if (range > (1ull << 27)) return fail(ctx, ASZ_E_UNSUPPORTED, "QB range too wide for the dense histogram");
+            hist_off[c] = hist_total;
+            hist_total += range;
+        }
+        CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
+        CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
+        unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
+        for (uint32_t c = 0; c < nc; c++) {
+            if (!num[c]) continue;
+            const u64 range = (u64)((int64_t)ranges[2 * c + 1] - (int64_t)ranges[2 * c]) + 1;
+            ProfScope ps_(ctx, "plan_histogram", num[c] * 4);
+            CK(launch_histogram<int32_t>(d_qb + pc[c].off, num[c], ranges[2 * c], range, d_hist + hist_off[c], st));
+        }
+        std::vector<u64> hist(hist_total);
+        if (hist_total) CK(cudaMemcpyAsync(hist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<HuffCode> codes(nc);
+        std::vector<int64_t> sym_lo(nc, 0);
+        std::vector<std::string> code_err(nc);
+        std::vector<char> code_ok(nc, 1);
+        {
+            auto build_one = [&](uint32_t c) {
+                if (!num[c]) return;
+                const u64 range = (u64)((int64_t)ranges[2 * c + 1] - (int64_t)ranges[2 * c]) + 1;
+                const u64 *h = hist.data() + hist_off[c];
+                u64 a = 0, b = range;
+                while (a < b && h[a] == 0) a++;
+                while (b > a && h[b - 1] == 0) b--;
+                std::vector<u64> hh(h + a, h + b);
+                sym_lo[c] = (int64_t)ranges[2 * c] + (int64_t)a;
+                code_ok[c] = build_code(hh, sym_lo[c], (int64_t)ranges[2 * c] + (int64_t)b - 1, num[c], false, codes[c], code_err[c]);
+            };
+            std::vector<std::thread> pool;
+            for (uint32_t c = 1; c < nc; c++)
+                if (num[c]) pool.emplace_back(build_one, c);
+            build_one(0);
+            for (auto &t : pool) t.join();
+        }
+        for (uint32_t c = 0; c < nc; c++)
+            if (!code_ok[c]) return fail(ctx, ASZ_E_UNSUPPORTED, code_err[c]);
+        // Encode all candidates into one payload arena.
+        std::vector<u64> word_off(nc, 0), code_off(nc, 0);
+        u64 words = 0, ncode = 0, max_count = 0;
+        for (uint32_t c = 0; c < nc; c++) {
+            if (!num[c]) continue;
+            word_off[c] = words;
+            words += (codes[c].bits + 31) / 32 + 2;
+            code_off[c] = ncode;
+            ncode += codes[c].table.size();
+            max_count = std::max(max_count, num[c]);
+        }
+        std::vector<CodeEntry> ctab(std::max<u64>(ncode, 1));
+        for (uint32_t c = 0; c < nc; c++)
+            if (num[c]) std::copy(codes[c].table.begin(), codes[c].table.end(), ctab.begin() + code_off[c]);
+        CK(ctx->codes.reserve(ctab.size() * sizeof(CodeEntry)));
+        CK(cudaMemcpyAsync(ctx->codes.p, ctab.data(), ctab.size() * sizeof(CodeEntry), cudaMemcpyHostToDevice, st));
+        CK(ctx->plan_pay.reserve(std::max<u64>(words, 1) * 4));
+        CK(cudaMemsetAsync(ctx->plan_pay.p, 0, std::max<u64>(words, 1) * 4, st));
+        CK(ctx->bitoff.reserve(std::max<u64>(max_count, 1) * 8));
+        size_t tmp_bytes = 0;
+        CK(launch_encode<int32_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp_bytes, nullptr, st));
+        CK(ctx->cubtmp.reserve(tmp_bytes));
+        for (uint32_t c = 0; c < nc; c++) {
+            if (!num[c] || codes[c].maxval == 1) continue;
+            size_t tb = ctx->cubtmp.cap;
+            ProfScope ps_(ctx, "plan_encode", num[c] * 4);
+            CK(launch_encode<int32_t>(d_qb + pc[c].off, num[c], sym_lo[c], ctx->codes.as<CodeEntry>() + code_off[c],
+                                      ctx->bitoff.as<u64>(), ctx->cubtmp.p, tb, ctx->plan_pay.as<uint32_t>() + word_off[c], st));
+        }
+        std::vector<uint32_t> pay(std::max<u64>(words, 1));
+        CK(cudaMemcpyAsync(pay.data(), ctx->plan_pay.p, std::max<u64>(words, 1) * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<u64> zlen(nc, 0);
+        std::vector<char> z_ok(nc, 1);
+        {
+            auto zstd_one = [&](uint32_t c) {
+                if (!num[c]) return;
+                const HuffCode &hc = codes[c];
+                std::vector<uint8_t> bs(hc.save_size() + hc.encode_size());
+                write_tree(hc, bs.data());
+                write_len_word(hc, bs.data() + hc.save_size());
+                if (hc.maxval != 1) std::memcpy(bs.data() + hc.save_size() + 8, pay.data() + word_off[c], (hc.bits + 7) >> 3);
+                std::vector<uint8_t> z(ZSTD_compressBound(bs.size()));
+                size_t zl = ZSTD_compress(z.data(), z.size(), bs.data(), bs.size(), 3);
+                if (ZSTD_isError(zl)) z_ok[c] = 0;
+                else zlen[c] = zl;
+            };
+            std::vector<std::thread> pool;
+            for (uint32_t c = 1; c < nc; c++)
+                if (num[c]) pool.emplace_back(zstd_one, c);
+            zstd_one(0);
+            for (auto &t : pool) t.join();
+        }
+        for (uint32_t c = 0; c < nc; c++)
+            if (!z_ok[c]) return fail(ctx, ASZ_E_DATA, "ZSTD_compress failed in the plan search");
+        out.lossless_s += secs(t_lossless, clk::now());
+        // ---- Choose the layer's predictor.
+        int best = -1;
+        float best_dist = 0;
+        for (uint32_t c = 0; c < nc; c++) {
+            if (!num[c]) continue;
+            const float nf = (float)num[c];
+            const float br = (float)zlen[c] * (8.0f / nf);
+            const float mse_avg = mse[c] / nf;
+            const float psnr = log10f(R * R / mse_avg) * 10.0f;
+            const float dist = psnr - lslope * br;
+            if (best < 0 || dist > best_dist) {
+                best = (int)c;
+                best_dist = dist;
+            }
+        }
+        if (best < 0) break;
+        ps[cands[best][5] - '0'] *= 2;
+        out.plan.insert(out.plan.begin(), cands[best]);
+        out.dists.push_back(best_dist);
+    }
+    return ASZ_OK;
+}
+
 }  // namespace
 
 extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
@@ -832,17 +1168,18 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     if (rc) return rc;
     rc = validate_dims(ctx, dims, rel_eb);
     if (rc) return rc;
-    if (!plan_text) return fail(ctx, ASZ_E_UNSUPPORTED, "automatic plan search is not available; pass a predictor plan");
     Plan plan;
     std::string perr;
-    if (!parse_plan(plan_text, plan, perr)) return fail(ctx, ASZ_E_ARG, perr);
-    if (plan.pred.size() > 63) return fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    if (plan_text) {
+        if (!parse_plan(plan_text, plan, perr)) return fail(ctx, ASZ_E_ARG, perr);
+        if (plan.pred.size() > 63) return fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    }
     if (p.predictor_family == ASZ_FAMILY_AUTO)
         return fail(ctx, ASZ_E_UNSUPPORTED, "automatic predictor-family selection is not available; pass a family");
     const bool quintic = p.predictor_family == ASZ_FAMILY_QUINTIC;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
     const u64 N = dims[0] * dims[1] * dims[2];
-    const u64 L = plan.pred.size();
+    
     cudaStream_t st = ctx->stream;
     asz_report R{};
 
@@ -880,6 +1217,28 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     }
     if (rc) return rc;
     R.default_slope_s = secs(t_slope, clk::now());
+    if (!plan_text) {
+        // Plan search (s1_compress.cpp:30-47 with no --predictor-plan).
+        auto t_plan = clk::now();
+        PlanSearchOut ps;
+        {
+            HostScope hs(ctx, "host:plan_search");
+            rc = plan_search(ctx, d_in, dims, p, abs_eb, mn, mx, slope, ps);
+        }
+        if (rc) return rc;
+        R.plan_s = secs(t_plan, clk::now());
+        R.plan_stats_s = ps.stats_s;
+        R.plan_sample_s = ps.sample_s;
+        R.plan_lossless_s = ps.lossless_s;
+        R.plan_search_layers = (uint32_t)std::min<size_t>(ps.dists.size(), 64);
+        for (uint32_t i = 0; i < R.plan_search_layers; i++) R.plan_best_dist[i] = ps.dists[i];
+        if (ps.plan.empty()) return fail(ctx, ASZ_E_DATA, "plan search found no layer");
+        std::string txt;
+        for (size_t i = 0; i < ps.plan.size(); i++) txt += (i ? "," : "") + ps.plan[i];
+        if (!parse_plan(txt.c_str(), plan, perr)) return fail(ctx, ASZ_E_DEVICE, perr);
+        if (plan.pred.size() > 63) return fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    }
+    const u64 L = plan.pred.size();
 
     auto t_core = clk::now();
     std::optional<HostScope> hs_prep(std::in_place, ctx, "host:prepare");

@@ -355,15 +355,15 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
     }
 }
 
-// Default-slope proxies: three AB maps (one per axis) over the original field, each evaluated
-// for every (t, eb) pair. One thread per map.
+// Proxies of whole-field AB maps over the original data (the default slope's three axis maps, or
+// the plan search's per-direction maps), each evaluated for every (t, eb) pair. One thread per map.
 __global__ void slope_v0_kernel(FieldGeom fg, const SampleBox *__restrict__ boxes, const ProxyEval *__restrict__ evals,
                                 uint32_t n_evals, const float *__restrict__ orig, const float *__restrict__ log2arena,
                                 float R2, uint8_t *scratch, uint64_t scratch_stride, uint32_t cap, uint32_t bcap,
                                 uint32_t tcap, float *__restrict__ h1_out, float *__restrict__ x_out,
-                                uint32_t *__restrict__ m_out, uint32_t *__restrict__ err_word) {
+                                uint32_t *__restrict__ m_out, uint32_t *__restrict__ err_word, uint32_t nboxes) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= 3) return;
+    if (g >= nboxes) return;
     SampleBox box = boxes[g];
     Scratch s = carve(scratch + g * scratch_stride, cap, bcap, tcap);
     FieldRef fr{orig, orig, fg.n[1] * fg.n[2], fg.n[2]};
@@ -401,9 +401,9 @@ cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
 cudaError_t launch_slope_v0(const FieldGeom &fg, const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals,
                             const float *orig, const float *log2arena, float R2, uint8_t *scratch, uint64_t scratch_stride,
                             uint32_t cap, uint32_t bcap, uint32_t tcap, float *h1, float *x, uint32_t *m_out, uint32_t *err,
-                            cudaStream_t st) {
+                            uint32_t nboxes, cudaStream_t st) {
     slope_v0_kernel<<<1, 32, 0, st>>>(fg, boxes, evals, n_evals, orig, log2arena, R2, scratch, scratch_stride, cap, bcap, tcap,
-                                      h1, x, m_out, err);
+                                      h1, x, m_out, err, nboxes);
     count_launch();
     return cudaGetLastError();
 }

@@ -562,11 +562,12 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
 
 cudaError_t launch_slope_exact(const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals, const float *orig,
                                uint64_t n1n2, uint64_t n2, const float *log2arena, float R2, float *h1, float *x,
-                               uint32_t *m_out, uint32_t *err, uint32_t cap, cudaStream_t st) {
+                               uint32_t *m_out, uint32_t *err, uint32_t cap, uint32_t nboxes, cudaStream_t st) {
+    if (nboxes == 0) return cudaSuccess;
     uint32_t smem = exact_smem_bytes(cap);
     cudaError_t e = cudaFuncSetAttribute(slope_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    slope_exact_kernel<<<3, kThreads, smem, st>>>(boxes, evals, n_evals, orig, n1n2, n2, log2arena, R2, h1, x, m_out, err,
+    slope_exact_kernel<<<nboxes, kThreads, smem, st>>>(boxes, evals, n_evals, orig, n1n2, n2, log2arena, R2, h1, x, m_out, err,
                                                   smem, cap);
     count_launch();
     return cudaGetLastError();

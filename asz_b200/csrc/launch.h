@@ -47,6 +47,18 @@ struct DecStream {
 
 constexpr uint32_t kDecodeTile = 256;  // chunks per tile (threads per decode CTA)
 
+// One candidate predictor of a plan-search layer (generate_config.tpp:526-604): its sample lattice
+// (start, stride and count per axis; loop nest ax[0] outer .. ax[2] inner), stencil geometry along
+// the prediction axis, t and error bound, and its offset in the layer's sample arrays.
+struct PlanCand {
+    uint64_t lo[3], st[3], cnt[3];
+    uint64_t off;
+    uint64_t hs, dist, right;
+    float t, eb, neg_2_eb;
+    int32_t dir;
+    int32_t ax[3];
+};
+
 cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st);
 cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
                                    cudaStream_t st);
@@ -81,13 +93,16 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
                               uint32_t *amb_count, const uint32_t *overrides, uint32_t n_overrides, float *proxies,
                               const uint32_t *list, const uint32_t *list_count, uint32_t *spill, uint32_t *spill_count,
                               uint32_t cap, unsigned grid, cudaStream_t st);
+cudaError_t launch_plan_sample(const float *d, uint64_t n1, uint64_t n2, const PlanCand *cands, uint32_t ncands, uint64_t total,
+                               int32_t *qb, float *e, int32_t *qb_range, cudaStream_t st);
+cudaError_t launch_plan_mse(const PlanCand *cands, uint32_t ncands, const float *e, float *mse, cudaStream_t st);
 cudaError_t launch_slope_exact(const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals, const float *orig,
                                uint64_t n1n2, uint64_t n2, const float *log2arena, float R2, float *h1, float *x,
-                               uint32_t *m_out, uint32_t *err, uint32_t cap, cudaStream_t st);
+                               uint32_t *m_out, uint32_t *err, uint32_t cap, uint32_t nboxes, cudaStream_t st);
 cudaError_t launch_slope_v0(const FieldGeom &fg, const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals,
                             const float *orig, const float *log2arena, float R2, uint8_t *scratch, uint64_t scratch_stride,
                             uint32_t cap, uint32_t bcap, uint32_t tcap, float *h1, float *x, uint32_t *m_out, uint32_t *err,
-                            cudaStream_t st);
+                            uint32_t nboxes, cudaStream_t st);
 
 template <class T>
 cudaError_t launch_histogram(const T *s, uint64_t n, int64_t offset, uint64_t range, unsigned long long *hist,

@@ -98,6 +98,12 @@ typedef struct asz_report {
     uint64_t exact_undecided;     /* of exact_groups: a comparison the fast path's bounds could not settle */
     uint64_t wide_groups;         /* groups the fast path settled by counting their bins window by window */
     uint64_t kernel_launches;     /* this library's kernels launched by the call (CUB scans not counted) */
+    /* Plan search (no plan given): "Generate config breakdown" phases (seconds), and per layer
+     * from the finest the winning score ("best_layer_predictor=..., best_dist=..."); the winning
+     * predictors are the plan read from its end. */
+    double plan_stats_s, plan_sample_s, plan_lossless_s;
+    uint32_t plan_search_layers;
+    float plan_best_dist[64];
     uint32_t pivot_stride[3], block_shape[3], block_num[3];
     int32_t quintic;
     char plan[64 * 11 + 1];       /* comma-separated predictor plan actually used */

@@ -723,6 +723,157 @@ vector<std::string> parse_plan(const char *s) {
     return out;
 }
 
+
+// dot_sample_compress (generate_config.tpp:227-254) on the original data, in the form GCC emits:
+// the edge stencils below, the interior as in dot_compress, the residual quantised in float
+// (diff * neg_2_eb), and the squared error accumulated with one fmaf per sample.
+static inline void dot_sample(vector<qb_t> &qv, float &mse, const float *d, u64 i, u64 hs, u64 right, u64 pos, u64 dist,
+                              float t, float eb, float neg_2_eb) {
+    float pred;
+    const float xm1 = d[pos - dist];
+    if (i <= hs) {
+        if (i + hs >= right) pred = xm1;
+        else if (i + 3 * hs >= right) pred = (d[pos + dist] + xm1) * 0.5f;
+        else pred = std::fmaf(d[pos + dist], 6.0f, std::fmaf(xm1, 3.0f, -d[pos + 3 * dist])) * 0.125f;
+    } else {
+        const float xm3 = d[pos - 3 * dist];
+        if (i + hs >= right) pred = std::fmaf(xm1, 3.0f, -xm3) * 0.5f;
+        else if (i + 3 * hs >= right) pred = (std::fmaf(xm1, 6.0f, d[pos + dist] * 3.0f) - xm3) * 0.125f;
+        else {
+            float s1 = d[pos + dist] + xm1, s3 = xm3 + d[pos + 3 * dist];
+            float p1 = (float)((double)s3 * (0.25 - (double)t));
+            pred = (float)std::fma(0.25 + (double)t, (double)s1, (double)p1);
+        }
+    }
+    const float diff = pred - d[pos];
+    const qb_t qb = (qb_t)lround_f(diff * neg_2_eb);
+    qv.push_back(qb);
+    const float q2 = (float)(qb_t)((uint32_t)qb * 2u);
+    const float e = std::fmaf(-eb, q2, diff);
+    mse = std::fmaf(e, e, mse);
+}
+
+// block_sample_compress_cubicD_ORDER (generate_config.tpp:256-438) over the whole field: the
+// innermost loop (axis = the order digit) runs at the lattice stride, the outer two at
+// sample_stride times it; the prediction axis starts at its half stride.
+static void sample_compress(vector<qb_t> &qv, float &mse, const float *d, const field &f, int dir, int order,
+                            const u64 ps2[3], u64 S, float t, float eb, float neg_2_eb) {
+    u64 st[3], lo[3];
+    for (int a = 0; a < 3; a++) {
+        st[a] = ps2[a] * (a == order ? 1 : S);
+        lo[a] = a == dir ? ps2[dir] / 2 : 0;
+    }
+    const u64 hs = ps2[dir] / 2;
+    u64 dist = hs;
+    for (int a = dir + 1; a < 3; a++) dist *= f.n[a];
+    static const int nest[3][3] = {{1, 2, 0}, {0, 2, 1}, {0, 1, 2}};  // loop axes, outer to inner
+    const int *ax = nest[order];
+    u64 ii[3];
+    for (ii[ax[0]] = lo[ax[0]]; ii[ax[0]] < f.n[ax[0]]; ii[ax[0]] += st[ax[0]])
+        for (ii[ax[1]] = lo[ax[1]]; ii[ax[1]] < f.n[ax[1]]; ii[ax[1]] += st[ax[1]])
+            for (ii[ax[2]] = lo[ax[2]]; ii[ax[2]] < f.n[ax[2]]; ii[ax[2]] += st[ax[2]])
+                dot_sample(qv, mse, d, ii[dir], hs, f.n[dir], f.pos(ii[0], ii[1], ii[2]), dist, t, eb, neg_2_eb);
+}
+
+template <class T> struct huff;
+
+// generate_config (generate_config.tpp:444-678): reverse-greedy plan search from the finest layer.
+static vector<std::string> generate_plan(const float *data, const field &f, float abs_eb, float min_val, float max_val,
+                                         float slope, const params_t &P, vector<float> &dists) {
+    const aszo_params &p = P.p;
+    static const char *all9[9] = {"cubic0_120", "cubic0_021", "cubic0_012", "cubic1_120", "cubic1_021",
+                                  "cubic1_012", "cubic2_120", "cubic2_021", "cubic2_012"};
+    static const char *last3[3] = {"cubic0_012", "cubic1_012", "cubic2_012"};
+    u64 ps[3] = {1, 1, 1};
+    vector<std::string> plan;
+    dists.clear();
+    for (u64 layer = 0; layer < p.max_layer_num; layer++) {
+        // As emitted: pow in double, products rounded to float, 0.5f/x for the 1/(2x) factors.
+        const float layer_eb = (float)((double)abs_eb * std::pow((double)p.eb_ratio, (double)layer));
+        const float neg_2_layer_eb = 0.5f / layer_eb;
+        const float stat_eb = layer_eb * p.stat_eb_ratio;
+        const float neg_2_stat_eb = 0.5f / stat_eb;
+        const float lslope = (float)((double)slope * std::pow((double)p.slope_ratio, (double)layer));
+        vector<std::string> cands;
+        if (layer < p.full_predictor_search_layer_num) cands.assign(all9, all9 + 9);
+        else cands.assign(last3, last3 + 3);
+        ab_map maps[3];
+        bool ready[3] = {false, false, false};
+        vector<float> br(cands.size()), psnr(cands.size());
+        vector<u64> num(cands.size(), 0);
+        for (size_t c = 0; c < cands.size(); c++) {
+            const int dir = cands[c][5] - '0', order = cands[c][9] - '0';
+            ab_map &m = maps[dir];
+            if (!ready[dir] && f.n[dir] > 3 * ps[dir]) {
+                u64 ps2[3] = {ps[0], ps[1], ps[2]};
+                ps2[dir] *= 2;
+                std::array<std::array<u64, 2>, 3> loc = {{{0, f.n[0]}, {0, f.n[1]}, {0, f.n[2]}}};
+                loc[dir] = {3 * ps2[dir] / 2, f.n[dir] - 3 * ps2[dir] / 2};
+                u64 dist = ps2[dir];
+                for (int a = dir + 1; a < 3; a++) dist *= f.n[a];
+                dist /= 2;
+                std::array<u64, 3> stride = {ps2[0], ps2[1], ps2[2]};
+                get_ab_map(m, data, f, loc, stride, dist, neg_2_stat_eb, p.h1_block_sampling_num);
+            }
+            ready[dir] = true;
+            // Best t on the map: score fmaf(-slope, h1, psnr), strictly better replaces.
+            float best_t = 0.25f;
+            if (!m.empty()) {
+                float h1, ps_;
+                get_h1_psnr(h1, ps_, m, 0.25f, layer_eb, stat_eb, min_val, max_val);
+                float best = std::fmaf(-lslope, h1, ps_);
+                for (float t : P.candidate_t) {
+                    if (t == 0.25f) continue;
+                    get_h1_psnr(h1, ps_, m, t, layer_eb, stat_eb, min_val, max_val);
+                    float cur = std::fmaf(-lslope, h1, ps_);
+                    if (cur > best) best_t = t;
+                    best = cur > best ? cur : best;
+                }
+            }
+            // Sampled compression with that t, then Huffman + zstd level 3 of its QBs.
+            u64 ps2[3] = {ps[0], ps[1], ps[2]};
+            ps2[dir] *= 2;
+            vector<qb_t> qv;
+            float mse = 0;
+            sample_compress(qv, mse, data, f, dir, order, ps2, p.generate_config_sample_stride, best_t, layer_eb,
+                            neg_2_layer_eb);
+            if (!qv.empty()) {
+                huff<qb_t> h;
+                h.build(qv.data(), qv.size());
+                vector<uint8_t> hb(h.save_size() + h.encode_size());
+                uint8_t *w = h.save(hb.data());
+                w = h.encode(qv.data(), qv.size(), w);
+                if (w != hb.data() + hb.size()) throw std::runtime_error("Huffman encoded size mismatch");
+                vector<uint8_t> z(ZSTD_compressBound(hb.size()));
+                size_t zl = ZSTD_compress(z.data(), z.size(), hb.data(), hb.size(), 3);
+                if (ZSTD_isError(zl)) throw std::runtime_error(ZSTD_getErrorName(zl));
+                const float nf = (float)qv.size();
+                br[c] = (float)zl * (8.0f / nf);
+                const float mse_avg = mse / nf;
+                const float R = max_val - min_val;
+                psnr[c] = log10f(R * R / mse_avg) * 10.0f;
+                num[c] = qv.size();
+            }
+        }
+        // Best predictor: score psnr - slope*br (two roundings), strictly better replaces.
+        int best = -1;
+        float best_dist = 0;
+        for (size_t c = 0; c < cands.size(); c++) {
+            if (!num[c]) continue;
+            const float dist = psnr[c] - lslope * br[c];
+            if (best < 0 || dist > best_dist) {
+                best = (int)c;
+                best_dist = dist;
+            }
+        }
+        if (best < 0) break;
+        ps[cands[best][5] - '0'] *= 2;
+        plan.insert(plan.begin(), cands[best]);
+        dists.push_back(best_dist);
+    }
+    return plan;
+}
+
 void set_err(char *err, const char *m) {
     if (err) snprintf(err, 256, "%s", m);
 }
@@ -745,6 +896,9 @@ void aszo_default_params(aszo_params *p) {
     p->default_slope_fallback = 1000;
     p->default_slope_eb_span = 1.5f;
     p->insufficient_sample_t = 4.0f / 16;
+    p->max_layer_num = 14;
+    p->full_predictor_search_layer_num = 4;
+    p->generate_config_sample_stride = 5;
 }
 
 int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
@@ -755,8 +909,7 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
         C.f = {{dims[0], dims[1], dims[2]}};
         C.P.init(*p);
         C.quintic = quintic != 0;
-        C.plan = parse_plan(plan);
-        if (C.plan.size() > 63) throw std::invalid_argument("predictor plan cannot contain more than 63 layers");
+        if (plan) C.plan = parse_plan(plan);
         C.data = data;
         u64 N = C.f.size();
         auto mm = std::minmax_element(data, data + N);
@@ -765,6 +918,17 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
         if (C.min_val == C.max_val) throw std::runtime_error("max_val==min_val");
         C.abs_eb = rel_eb * (C.max_val - C.min_val);
         C.default_slope_v = default_slope(data, C.f, C.abs_eb, C.min_val, C.max_val, C.P);
+        vector<float> dists;
+        if (!plan) C.plan = generate_plan(data, C.f, C.abs_eb, C.min_val, C.max_val, C.default_slope_v, C.P, dists);
+        if (C.plan.size() > 63) throw std::invalid_argument("predictor plan cannot contain more than 63 layers");
+        if (C.plan.empty()) throw std::runtime_error("plan search found no layer");
+        {
+            std::string pl;
+            for (size_t i = 0; i < C.plan.size(); i++) pl += (i ? "," : "") + C.plan[i];
+            snprintf(out->plan, sizeof(out->plan), "%s", pl.c_str());
+            out->search_layers = (uint32_t)std::min<size_t>(dists.size(), 64);
+            for (size_t i = 0; i < out->search_layers; i++) out->best_dist[i] = dists[i];
+        }
         C.geometry();
         C.compress_core();
         // Stream assembly: compress.tpp:233-291.

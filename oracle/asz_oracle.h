@@ -28,6 +28,9 @@ typedef struct aszo_params {
     float stat_eb_ratio;
     float default_slope_invalid_ratio_threshold, default_slope_fallback, default_slope_eb_span;
     float insufficient_sample_t;
+    uint64_t max_layer_num;                   /* plan search (generate_config.tpp:444-678) */
+    uint64_t full_predictor_search_layer_num;
+    uint64_t generate_config_sample_stride;
 } aszo_params;
 
 void aszo_default_params(aszo_params *p);
@@ -46,9 +49,13 @@ typedef struct aszo_result {
     uint64_t asz_len;
     float min_val, max_val, abs_eb, default_slope;
     uint64_t t_fallback_count;
+    char plan[64 * 11 + 1];  /* plan used (searched when none was given) */
+    uint32_t search_layers;  /* plan search: layers that chose a predictor */
+    float best_dist[64];     /* plan search: the winning score of each of those layers */
 } aszo_result;
 
-/* Compress with a given plan ("cubic2_012,cubic1_120,..."), quintic = force_quintic.
+/* Compress with a given plan ("cubic2_012,cubic1_120,..."), quintic = force_quintic. A NULL plan
+ * runs the reference's plan search (param_c::generate_config).
  * Returns 0 or a negative error code; err (256 bytes) receives a message. */
 int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p,
                   const char *plan, int quintic, aszo_result *out, char *err);

@@ -27,6 +27,8 @@ class Params(C.Structure):
         ("stat_eb_ratio", C.c_float), ("default_slope_invalid_ratio_threshold", C.c_float),
         ("default_slope_fallback", C.c_float), ("default_slope_eb_span", C.c_float),
         ("insufficient_sample_t", C.c_float),
+        ("max_layer_num", C.c_uint64), ("full_predictor_search_layer_num", C.c_uint64),
+        ("generate_config_sample_stride", C.c_uint64),
     ]
 
 
@@ -39,6 +41,7 @@ class _Result(C.Structure):
         ("asz", C.POINTER(C.c_uint8)), ("asz_len", C.c_uint64),
         ("min_val", C.c_float), ("max_val", C.c_float), ("abs_eb", C.c_float),
         ("default_slope", C.c_float), ("t_fallback_count", C.c_uint64),
+        ("plan", C.c_char * (64 * 11 + 1)), ("search_layers", C.c_uint32), ("best_dist", C.c_float * 64),
     ]
 
 
@@ -94,20 +97,23 @@ class Compressed:
     abs_eb: float
     default_slope: float
     t_fallback_count: int
+    plan: str = ""
+    best_dist: tuple = ()
 
 
 def _dims(shape):
     return (C.c_uint64 * 3)(*[int(s) for s in shape])
 
 
-def compress(data: np.ndarray, rel_eb: float, plan: str, quintic: bool = False, params: Params | None = None) -> Compressed:
+def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic: bool = False, params: Params | None = None) -> Compressed:
+    """Compress with `plan`, or run the reference's plan search when plan is None."""
     lib = liboracle()
     data = np.ascontiguousarray(data, dtype=np.float32)
     p = params or default_params()
     res = _Result()
     err = C.create_string_buffer(256)
     rc = lib.aszo_compress(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p),
-                           plan.encode(), int(quintic), C.byref(res), err)
+                           plan.encode() if plan is not None else None, int(quintic), C.byref(res), err)
     if rc != 0:
         raise RuntimeError(err.value.decode())
     try:
@@ -118,7 +124,8 @@ def compress(data: np.ndarray, rel_eb: float, plan: str, quintic: bool = False, 
         pre = C.string_at(res.pre_zstd, res.pre_zstd_len)
         asz = C.string_at(res.asz, res.asz_len)
         return Compressed(qb, t, rec, pre, asz, res.min_val, res.max_val, res.abs_eb, res.default_slope,
-                          int(res.t_fallback_count))
+                          int(res.t_fallback_count), res.plan.decode(),
+                          tuple(res.best_dist[i] for i in range(res.search_layers)))
     finally:
         lib.aszo_free_result(C.byref(res))
 

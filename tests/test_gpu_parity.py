@@ -84,6 +84,38 @@ def test_c2_like_128_cubic2_plan(gpu_ctx, family):
     assert rep.t_fallback_count > 0
 
 
+def test_plan_search_against_oracle(gpu_ctx):
+    """No plan given: the device plan search picks the reference's plan (checked with the oracle's
+    restatement), and the whole compression then matches."""
+    import asz_b200.api as api
+    from asz_b200 import fields
+    rng = np.random.default_rng(77)
+    for i in range(12):
+        shape = tuple(int(x) for x in rng.integers(7, 48, size=3))
+        f = fields.grf_field(shape, rng.uniform(1.5, 5), rng).astype(np.float32)
+        if i % 3 == 1:
+            f[: shape[0] // 3] = 0.0
+        eb = float(10 ** rng.uniform(-5, -1.5))
+        family = ["cubic", "quintic"][int(rng.integers(0, 2))]
+        bpr = int(rng.integers(1, 6))
+        o = O.compress(f, eb, None, family == "quintic", O.default_params(block_pivot_ratio=bpr))
+        blob, rep = gpu_ctx.compress(f, eb, None, family, api.default_params(block_pivot_ratio=bpr))
+        assert rep.plan.decode() == o.plan
+        assert [rep.plan_best_dist[k] for k in range(rep.plan_search_layers)] == list(o.best_dist)
+        assert blob == o.asz
+
+
+def test_plan_search_c1_like(gpu_ctx):
+    """A C1-shaped field (smaller depth) through the plan search, against the oracle."""
+    import asz_b200.api as api
+    from asz_b200 import fields
+    f = fields.c1_field(seed=3, shape=(24, 120, 100))
+    o = O.compress(f, 1e-3, None, False, O.default_params(block_pivot_ratio=3))
+    blob, rep = gpu_ctx.compress(f, 1e-3, None, "cubic", api.default_params(block_pivot_ratio=3))
+    assert rep.plan.decode() == o.plan
+    assert blob == o.asz
+
+
 @pytest.mark.parametrize("rel_eb,path", [(1e-4, "windows"), (2e-5, "exact")])
 def test_wide_bin_ranges(gpu_ctx, rel_eb, path):
     """White noise at a small error bound: the quantised errors of many (block, round) groups span
@@ -135,6 +167,26 @@ def test_cli_drop_in(case):
         assert r.returncode == 0, r.stderr
         assert np.array_equal(np.fromfile(o, np.float32), out.ravel())
         assert "Decompression time:" in r.stdout and "CR= " in r.stdout
+
+
+def test_cli_plan_search():
+    """s1_compress without --predictor-plan: the searched plan's .asz (checked with the oracle) and the
+    plan-search stdout lines."""
+    case = golden_cases()[0]
+    data, _, _ = load_golden(case)
+    dims = [str(s) for s in data.shape]
+    bpr = case["block_pivot_ratio"]
+    want = O.compress(data, case["rel_eb"], None, case["family"] == "quintic", O.default_params(block_pivot_ratio=bpr))
+    with tempfile.TemporaryDirectory() as wd:
+        inp, z = os.path.join(wd, "in.f32"), os.path.join(wd, "x.asz")
+        data.tofile(inp)
+        r = subprocess.run([os.path.join(BIN, "s1_compress"), "-f", "-i", inp, "-z", z, "-3", *dims, "-M", "REL",
+                            repr(case["rel_eb"]), "--predictor-family", case["family"], "--block-pivot-ratio", str(bpr)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert open(z, "rb").read() == want.asz
+        for line in ("best_layer_predictor=", "Generate config breakdown: statistics=", "Generate config time:"):
+            assert line in r.stdout
 
 
 def test_corrupt_streams_fail_cleanly(gpu_ctx):

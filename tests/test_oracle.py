@@ -57,6 +57,30 @@ def test_oracle_matches_reference_binary_random():
             assert np.array_equal(O.decompress(asz, shape, eb, p).view(np.uint32), dec.view(np.uint32))
 
 
+@pytest.mark.skipif(not _ref_available(), reason="reference binaries not built (make -C oracle ref)")
+def test_oracle_plan_search_matches_reference_binary():
+    """The plan search (no --predictor-plan): the searched plan and the .asz bytes."""
+    import re
+
+    from asz_b200 import fields
+    rng = np.random.default_rng(4242)
+    for _ in range(10):
+        shape = tuple(int(x) for x in rng.integers(7, 40, size=3))
+        f = fields.grf_field(shape, rng.uniform(1.5, 5), rng).astype(np.float32)
+        eb = float(10 ** rng.uniform(-5, -1.5))
+        fam = ["cubic", "quintic"][int(rng.integers(0, 2))]
+        bpr = int(rng.integers(1, 6))
+        with tempfile.TemporaryDirectory() as wd:
+            asz, _, out = O.run_reference_compress(f, eb, wd, plan=None, family=fam,
+                                                   extra=["--block-pivot-ratio", str(bpr)], dump=False)
+        c = O.compress(f, eb, None, fam == "quintic", O.default_params(block_pivot_ratio=bpr))
+        ref_plan = re.search(r'predictor_vec=\{([^}]*)\}', out).group(1).replace('"', '')
+        assert c.plan == ref_plan
+        assert c.asz == asz
+        ref_dists = [float(x) for x in re.findall(r"best_layer_predictor=cubic\d_\d+, best_dist=([-0-9.e+]+)", out)]
+        assert np.allclose(ref_dists, c.best_dist, rtol=0, atol=1e-6)
+
+
 def test_huffman_known_answer():
     # Symbols [0,0,1]: heap pops leaf 1 (freq 1) then leaf 0 (freq 2) -> codes 1:'0', 0:'1'.
     enc = O.huffman_encode(np.array([0, 0, 1], np.int32))
