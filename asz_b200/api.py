@@ -60,6 +60,12 @@ class Report(C.Structure):
         ("wide_groups", C.c_uint64), ("kernel_launches", C.c_uint64),
         ("plan_stats_s", C.c_double), ("plan_sample_s", C.c_double), ("plan_lossless_s", C.c_double),
         ("plan_search_layers", C.c_uint32), ("plan_best_dist", C.c_float * 64),
+        ("family_selected", C.c_int32), ("family_fallback", C.c_int32),
+        ("fam_suffix_layers", C.c_uint64), ("fam_blocks", C.c_uint64), ("fam_sampled_points", C.c_uint64),
+        ("fam_budget", C.c_uint64), ("fam_probe_bpr", C.c_uint64), ("fam_points", C.c_uint64),
+        ("fam_cubic_mse", C.c_longdouble), ("fam_quintic_mse", C.c_longdouble), ("fam_cubic_psnr", C.c_longdouble),
+        ("fam_quintic_psnr", C.c_longdouble), ("fam_cubic_h1", C.c_longdouble), ("fam_quintic_h1", C.c_longdouble),
+        ("fam_score_gain", C.c_longdouble),
         ("pivot_stride", C.c_uint32 * 3), ("block_shape", C.c_uint32 * 3), ("block_num", C.c_uint32 * 3),
         ("quintic", C.c_int32), ("plan", C.c_char * (64 * 11 + 1)),
     ]

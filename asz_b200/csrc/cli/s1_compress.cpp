@@ -66,6 +66,23 @@ int main(int argc, char *argv[]) try {
                r.plan_sample_s, r.plan_lossless_s);
         printf("Generate config time: %f s\n", r.plan_s);
     }
+    if (r.family_selected) {
+        // select_predictor_family's lines (predictor_family.tpp:236-250).
+        if (r.family_fallback)
+            printf("Predictor family selection: selector=h1, suffix_layers=%lu, blocks=0, sampled_block_points=0, "
+                   "sample_point_budget=%lu, probe_block_pivot_ratio=%lu, fallback=point_budget, family=cubic\n",
+                   (unsigned long)r.fam_suffix_layers, (unsigned long)r.fam_budget, (unsigned long)r.fam_probe_bpr);
+        else
+            printf("Predictor family selection: selector=h1, suffix_layers=%lu, blocks=%lu, sampled_block_points=%lu, "
+                   "sample_point_budget=%lu, probe_block_pivot_ratio=%lu, points=%lu, cubic_mse=%.12Le, quintic_mse=%.12Le, "
+                   "cubic_psnr=%.12Le, quintic_psnr=%.12Le, cubic_h1=%.12Le, quintic_h1=%.12Le, six_score_gain=%.12Le, "
+                   "family=%s\n",
+                   (unsigned long)r.fam_suffix_layers, (unsigned long)r.fam_blocks, (unsigned long)r.fam_sampled_points,
+                   (unsigned long)r.fam_budget, (unsigned long)r.fam_probe_bpr, (unsigned long)r.fam_points, r.fam_cubic_mse,
+                   r.fam_quintic_mse, r.fam_cubic_psnr, r.fam_quintic_psnr, r.fam_cubic_h1, r.fam_quintic_h1, r.fam_score_gain,
+                   r.quintic ? "quintic" : "cubic");
+        printf("Predictor family selection time: %f s\n", r.family_s);
+    }
     // print_config (generate_config.tpp:6-49).
     printf("predictor_vec={");
     {

@@ -75,6 +75,10 @@ struct AxisEntry {
 
 struct FieldGeom {
     uint64_t n[3];
+    // Frame origin: blocks and the pivot lattice start here (0 for a whole field). Positions below
+    // it are a read-only halo that keeps its input values (the predictor-family probe's local
+    // contexts, predictor_family.tpp:40-60).
+    uint64_t origin[3];
     uint64_t block_shape[3];
     uint64_t block_num[3];
     uint64_t pivot_stride[3];
@@ -84,5 +88,9 @@ struct FieldGeom {
 };
 
 ASZ_HD uint64_t owner_block(uint64_t i, uint64_t shape) { return i == 0 ? 0 : (i - 1) / shape; }
+
+// Block of coordinate i in a frame starting at h: a block's upper face belongs to it, its lower face
+// to the block below (only the frame's first face at h == 0 starts block 0).
+ASZ_HD uint64_t owner_block_at(uint64_t i, uint64_t h, uint64_t shape) { return i <= h ? 0 : (i - h - 1) / shape; }
 
 }  // namespace asz

@@ -20,17 +20,18 @@ ASZ_HD Target locate(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, ui
     const uint64_t kk[3] = {k0, k1, k2};
     uint64_t ii[3], bb[3], jj[3], cc[3];
     for (int a = 0; a < 3; a++) {
-        ii[a] = a == rg.dir ? rg.hs + 2 * rg.hs * kk[a] : rg.stride[a] * kk[a];
-        bb[a] = owner_block(ii[a], fg.block_shape[a]);
-        uint64_t start = bb[a] * fg.block_shape[a] +
-                         (a == rg.dir ? rg.hs : (bb[a] == 0 ? 0 : rg.stride[a]));
+        const uint64_t h = fg.origin[a];
+        ii[a] = a == rg.dir ? h + rg.hs + 2 * rg.hs * kk[a] : (h == 0 ? rg.stride[a] * kk[a] : h + rg.stride[a] * (kk[a] + 1));
+        bb[a] = owner_block_at(ii[a], h, fg.block_shape[a]);
+        const uint64_t b0 = h + bb[a] * fg.block_shape[a];
+        uint64_t start = b0 + (a == rg.dir ? rg.hs : (b0 == 0 ? 0 : rg.stride[a]));
         jj[a] = (ii[a] - start) / rg.stride[a];
         cc[a] = at.count[rg.axis_off[a] + bb[a]];
     }
     Target t;
     t.pos = (ii[0] * fg.n[1] + ii[1]) * fg.n[2] + ii[2];
     t.i = ii[rg.dir];
-    const uint64_t r = (bb[rg.dir] + 1) * fg.block_shape[rg.dir] + 1;
+    const uint64_t r = fg.origin[rg.dir] + (bb[rg.dir] + 1) * fg.block_shape[rg.dir] + 1;
     t.right = r < fg.n[rg.dir] ? r : fg.n[rg.dir];
     // QB base of the block: per-axis prefix sums of the raster-ordered box sizes.
     uint64_t base = at.prefix[rg.axis_off[0] + bb[0]] * rg.total[1] * rg.total[2] +
@@ -60,16 +61,20 @@ ASZ_HD uint32_t stencil_case(uint64_t i, uint64_t hs, uint64_t right, bool quint
 // The per-axis part of locate() for lattice index k along axis a.
 ASZ_HD AxisEntry axis_entry(const FieldGeom &fg, const RoundGeom &rg, AxisTables at, int a, uint64_t k) {
     AxisEntry e{};
-    const uint64_t ii = a == rg.dir ? rg.hs + 2 * rg.hs * k : rg.stride[a] * k;
-    const uint64_t bb = owner_block(ii, fg.block_shape[a]);
-    const uint64_t start = bb * fg.block_shape[a] + (a == rg.dir ? rg.hs : (bb == 0 ? 0 : rg.stride[a]));
+    const uint64_t h = fg.origin[a];
+    // Target lattice: odd multiples of hs past the origin along the round axis; on the other axes
+    // the stride lattice from the origin, without the origin's face when it is not the field's.
+    const uint64_t ii = a == rg.dir ? h + rg.hs + 2 * rg.hs * k : (h == 0 ? rg.stride[a] * k : h + rg.stride[a] * (k + 1));
+    const uint64_t bb = owner_block_at(ii, h, fg.block_shape[a]);
+    const uint64_t b0 = h + bb * fg.block_shape[a];
+    const uint64_t start = b0 + (a == rg.dir ? rg.hs : (b0 == 0 ? 0 : rg.stride[a]));
     e.ii = (uint32_t)ii;
     e.bb = (uint32_t)bb;
     e.jj = (uint32_t)((ii - start) / rg.stride[a]);
     e.cc = (uint32_t)at.count[rg.axis_off[a] + bb];
     e.pre = at.prefix[rg.axis_off[a] + bb];
     if (a == rg.dir) {
-        const uint64_t r = (bb + 1) * fg.block_shape[a] + 1;
+        const uint64_t r = b0 + fg.block_shape[a] + 1;
         e.stencil = stencil_case(ii, rg.hs, r < fg.n[a] ? r : fg.n[a], fg.quintic != 0);
     }
     return e;

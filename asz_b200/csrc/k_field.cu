@@ -85,7 +85,8 @@ __global__ void pivot_compress_kernel(PivotGeom pg, const float *__restrict__ in
     int32_t lo = INT32_MAX, hi = INT32_MIN;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t k2 = k % pg.cnt[2], k1 = (k / pg.cnt[2]) % pg.cnt[1], k0 = k / (pg.cnt[1] * pg.cnt[2]);
-        uint64_t pos = k0 * pg.stride[0] * pg.n1n2 + k1 * pg.stride[1] * pg.n2 + k2 * pg.stride[2];
+        uint64_t pos = (pg.origin[0] + k0 * pg.stride[0]) * pg.n1n2 + (pg.origin[1] + k1 * pg.stride[1]) * pg.n2 +
+                       pg.origin[2] + k2 * pg.stride[2];
         int32_t q = (int32_t)lround_d(__dmul_rn((double)in[pos], pg.rp));
         qb[k] = q;
         rec[pos] = __double2float_rn(__dmul_rn((double)q, pg.peb2));
@@ -106,7 +107,8 @@ __global__ void pivot_decompress_kernel(PivotGeom pg, const int32_t *__restrict_
     const uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t k2 = k % pg.cnt[2], k1 = (k / pg.cnt[2]) % pg.cnt[1], k0 = k / (pg.cnt[1] * pg.cnt[2]);
-        uint64_t pos = k0 * pg.stride[0] * pg.n1n2 + k1 * pg.stride[1] * pg.n2 + k2 * pg.stride[2];
+        uint64_t pos = (pg.origin[0] + k0 * pg.stride[0]) * pg.n1n2 + (pg.origin[1] + k1 * pg.stride[1]) * pg.n2 +
+                       pg.origin[2] + k2 * pg.stride[2];
         rec[pos] = __double2float_rn(__dmul_rn((double)qb[k], pg.peb2));
     }
 }
@@ -228,10 +230,13 @@ __device__ __forceinline__ LineMap line_map(uint32_t tpl_log2) {
 // Compress round: quantise the residual and write the reconstruction in place.
 // compress.tpp:35-37 as emitted: axis 0 multiplies by the hoisted 0.5*(1/eb) (inlined loop),
 // axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
-__global__ void __launch_bounds__(256)
+// kProbe: every axis divides, as the diagnostics instantiation that the predictor-family probe runs
+// does (one out-of-line clone for all axes), and pred_out receives each target's prediction.
+template <bool kProbe>
+__global__ void __launch_bounds__(256, 5)
     round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
                           const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
-                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word) {
+                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out) {
     const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd), r0 = __dmul_rn(rinv, 0.5);
     const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
     const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
@@ -260,7 +265,8 @@ __global__ void __launch_bounds__(256)
             const float pred = predict_case(rec, pos, rg.dist, sc, t);
             const double pd = (double)pred;
             const double diff = __dsub_rn(pd, (double)in[pos]);
-            const double q = dir == 0 ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+            const double q = dir == 0 && !kProbe ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+            if (kProbe) pred_out[pos] = pred;
             const int32_t v = (int32_t)lround_d(q);
             qb[qi] = v;
             rec[pos] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
@@ -372,10 +378,16 @@ static unsigned round_grid(const RoundGeom &rg, uint32_t tpl_log2) {
 }
 
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
-                                  const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, cudaStream_t st) {
+                                  const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, int div_all,
+                                  float *pred_out, cudaStream_t st) {
     if (rg.targets == 0) return cudaSuccess;
     const uint32_t lg = tpl_log2_for(rg.tcount[2]);
-    round_compress_kernel<<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err);
+    if (div_all)
+        round_compress_kernel<true><<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
+                                                                        pred_out);
+    else
+        round_compress_kernel<false><<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
+                                                                         nullptr);
     count_launch();
     return cudaGetLastError();
 }
@@ -427,5 +439,29 @@ namespace asz {
 uint64_t &launch_counter() {
     thread_local uint64_t count = 0;
     return count;
+}
+}  // namespace asz
+
+// Copy of the box [lo, lo + m) of a C-order field of shape n into a dense buffer of shape m (the
+// predictor-family probe's local contexts).
+namespace asz {
+namespace {
+__global__ void copy_box_kernel(const float *__restrict__ in, uint64_t n1, uint64_t n2, uint64_t lo0, uint64_t lo1, uint64_t lo2,
+                                uint64_t m0, uint64_t m1, uint64_t m2, float *__restrict__ out) {
+    const uint64_t total = m0 * m1 * m2;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i2 = k % m2, r = k / m2, i1 = r % m1, i0 = r / m1;
+        out[k] = in[((lo0 + i0) * n1 + lo1 + i1) * n2 + lo2 + i2];
+    }
+}
+}  // namespace
+
+cudaError_t launch_copy_box(const float *in, const uint64_t n[3], const uint64_t lo[3], const uint64_t m[3], float *out,
+                            cudaStream_t st) {
+    const uint64_t total = m[0] * m[1] * m[2];
+    if (total == 0) return cudaSuccess;
+    copy_box_kernel<<<grid_for(total, 256, 148 * 8), 256, 0, st>>>(in, n[1], n[2], lo[0], lo[1], lo[2], m[0], m[1], m[2], out);
+    count_launch();
+    return cudaGetLastError();
 }
 }  // namespace asz

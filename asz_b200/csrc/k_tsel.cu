@@ -271,8 +271,8 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
     if (!fb) {
         SampleBox box;
         for (int a = 0; a < 3; a++) {
-            uint64_t lo = bb[a] * fg.block_shape[a];
-            uint64_t hi = min((bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
+            uint64_t lo = fg.origin[a] + bb[a] * fg.block_shape[a];
+            uint64_t hi = min(fg.origin[a] + (bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
             if (a != d && lo != 0) lo += rg.stride[a];
             if (a == d) {
                 lo += 3 * rg.stride[a] / 2;

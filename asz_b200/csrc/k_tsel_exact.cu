@@ -433,8 +433,8 @@ __global__ void __launch_bounds__(kThreads)
         const int d = rg.dir;
         ExactGroup eg;
         for (int a = 0; a < 3; a++) {
-            uint64_t lo = bb[a] * fg.block_shape[a];
-            uint64_t hi = min((bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
+            uint64_t lo = fg.origin[a] + bb[a] * fg.block_shape[a];
+            uint64_t hi = min(fg.origin[a] + (bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
             if (a != d && lo != 0) lo += rg.stride[a];
             if (a == d) {
                 lo += 3 * rg.stride[a] / 2;

@@ -18,6 +18,7 @@ inline void count_launch() { ++launch_counter(); }
 struct PivotGeom {
     uint64_t cnt[3];      // pivots per axis
     uint64_t stride[3];
+    uint64_t origin[3];   // first pivot (the frame origin)
     uint64_t n1n2, n2;
     double rp;            // 0.5 / (double)pivot_eb
     double peb2;          // 2 * (double)pivot_eb
@@ -68,7 +69,8 @@ cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, floa
 // One round over every target; `ent` holds the per-axis AxisEntry tables (RoundGeom::ent_off).
 // Requires tcount[0] * tcount[1] < 2^32 and tcount[2] < 2^32 (checked by the host).
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
-                                  const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, cudaStream_t st);
+                                  const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, int div_all,
+                                  float *pred_out, cudaStream_t st);
 cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const AxisEntry *ent,
                                     const int64_t *t_int, const int32_t *qb, float *rec, uint32_t *err, cudaStream_t st);
 
@@ -93,6 +95,8 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
                               uint32_t *amb_count, const uint32_t *overrides, uint32_t n_overrides, float *proxies,
                               const uint32_t *list, const uint32_t *list_count, uint32_t *spill, uint32_t *spill_count,
                               uint32_t cap, unsigned grid, cudaStream_t st);
+cudaError_t launch_copy_box(const float *in, const uint64_t n[3], const uint64_t lo[3], const uint64_t m[3], float *out,
+                            cudaStream_t st);
 cudaError_t launch_plan_sample(const float *d, uint64_t n1, uint64_t n2, const PlanCand *cands, uint32_t ncands, uint64_t total,
                                int32_t *qb, float *e, int32_t *qb_range, cudaStream_t st);
 cudaError_t launch_plan_mse(const PlanCand *cands, uint32_t ncands, const float *e, float *mse, cudaStream_t st);

@@ -104,6 +104,12 @@ typedef struct asz_report {
     double plan_stats_s, plan_sample_s, plan_lossless_s;
     uint32_t plan_search_layers;
     float plan_best_dist[64];
+    /* Predictor-family selection (family ASZ_FAMILY_AUTO), the figures of its stdout line
+     * (predictor_family.tpp:236-248): prediction MSE, PSNR and H1 per family, and the score. */
+    int32_t family_selected, family_fallback;
+    uint64_t fam_suffix_layers, fam_blocks, fam_sampled_points, fam_budget, fam_probe_bpr, fam_points;
+    long double fam_cubic_mse, fam_quintic_mse, fam_cubic_psnr, fam_quintic_psnr, fam_cubic_h1, fam_quintic_h1,
+        fam_score_gain;
     uint32_t pivot_stride[3], block_shape[3], block_num[3];
     int32_t quintic;
     char plan[64 * 11 + 1];       /* comma-separated predictor plan actually used */
@@ -180,6 +186,11 @@ int asz_error_stats_noalloc(const float *x, const float *y, uint64_t n, double v
  * of every target equals its position in the reference's block-major loops
  * (compress.tpp:53-88). Returns the number of violations (0), or a negative error code. */
 int64_t asz_check_geometry(const uint64_t dims[3], const char *plan, uint64_t block_pivot_ratio, int quintic);
+/* The same for a frame whose blocks and pivot lattice start at `origin` (the predictor-family
+ * probe's local contexts, predictor_family.tpp:40-60): positions below the origin, and the
+ * origin's faces off the pivot lattice, keep their input values and are never written. */
+int64_t asz_check_geometry_frame(const uint64_t dims[3], const uint64_t origin[3], const char *plan,
+                                 uint64_t block_pivot_ratio, int quintic);
 
 /* Host-side run of the device's std::unordered_map order emulation (no GPU involved), for
  * checking it against the real container: keys are (a[i], b[i]) pairs with the reference's

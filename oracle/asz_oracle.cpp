@@ -34,6 +34,7 @@
 #include <stack>
 #include <stdexcept>
 #include <string>
+#include <random>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -724,6 +725,228 @@ vector<std::string> parse_plan(const char *s) {
 }
 
 
+
+// ---------------------------------------------------------------------------------------------
+// Predictor-family selection: param_c::select_predictor_family and predictor_family_detail
+// (predictor_family.tpp:1-252), with the long-double steps as the reference build emits them on
+// x87: log2 and log10 through fyl2x, divisions by a count as a multiplication by its reciprocal,
+// no infinity test in the score (finite-math), and floor through frndint.
+
+static inline long double x87_fyl2x(long double x, long double y) {  // y * log2(x)
+    long double r;
+    __asm__("fyl2x" : "=t"(r) : "0"(x), "u"(y) : "st(1)");
+    return r;
+}
+static inline long double x87_lg2() {
+    long double r;
+    __asm__("fldlg2" : "=t"(r));
+    return r;
+}
+
+struct fam_result {
+    u64 point_count = 0;
+    long double prediction_mse = 0, reconstruction_mse = 0, reconstruction_psnr = 0, h1 = 0;
+};
+
+// entropy() (predictor_family.tpp:116-131).
+static long double fam_entropy(const vector<qb_t> &qbs) {
+    if (qbs.empty()) return 0;
+    std::unordered_map<qb_t, u64> freq;
+    for (qb_t q : qbs) freq[q]++;
+    const long double r = 1.0L / (long double)qbs.size();
+    long double h1 = 0;
+    for (const auto &kv : freq) {
+        const long double pr = (long double)kv.second * r;
+        h1 = h1 - pr * x87_fyl2x(pr, 1.0L);
+    }
+    return h1;
+}
+
+// evaluate() (predictor_family.tpp:133-215) for one family on the target blocks.
+static fam_result fam_evaluate(const codec &probe, const float *data, const vector<std::array<u64, 3>> &targets, bool quintic) {
+    const u64 L = probe.plan.size();
+    const float seed_eb = probe.abs_eb * probe.P.p.pivot_eb_ratio;
+    vector<vector<qb_t>> layer_qbs(L);
+    vector<long double> pred_sse(L, 0), rec_sse(L, 0);
+    vector<u64> counts(L, 0);
+    for (const auto &tb : targets) {
+        std::array<u64, 3> cbb, tend, cb, ce, hb;
+        for (int a = 0; a < 3; a++) {
+            cbb[a] = tb[a] ? tb[a] - 1 : 0;
+            tend[a] = tb[a] + 1;
+            cb[a] = cbb[a] * probe.block_shape[a];
+            ce[a] = std::min(tend[a] * probe.block_shape[a] + 1, probe.f.n[a]);
+            const u64 left_halo = 5 * (probe.pivot_stride[a] / 2);
+            hb[a] = cb[a] > left_halo ? cb[a] - left_halo : 0;
+        }
+        codec local;
+        local.f = {{ce[0] - hb[0], ce[1] - hb[1], ce[2] - hb[2]}};
+        vector<float> ldata(local.f.size());
+        for (u64 i0 = hb[0]; i0 < ce[0]; i0++)
+            for (u64 i1 = hb[1]; i1 < ce[1]; i1++)
+                std::memcpy(&ldata[local.f.pos(i0 - hb[0], i1 - hb[1], 0)], &data[probe.f.pos(i0, i1, hb[2])],
+                            local.f.n[2] * sizeof(float));
+        local.data = ldata.data();
+        local.cd = ldata;
+        local.P = probe.P;
+        local.quintic = quintic;
+        local.plan = probe.plan;
+        local.pivot_stride = probe.pivot_stride;
+        local.block_shape = probe.block_shape;
+        local.min_val = probe.min_val;
+        local.max_val = probe.max_val;
+        local.abs_eb = probe.abs_eb;
+        local.default_slope_v = probe.default_slope_v;
+        // Seed pivots on the context (global lattice), as in the whole-field compressor.
+        const double peb = seed_eb, rp = 0.5 / peb, peb2 = peb + peb;
+        for (u64 i0 = cb[0]; i0 < ce[0]; i0 += probe.pivot_stride[0])
+            for (u64 i1 = cb[1]; i1 < ce[1]; i1 += probe.pivot_stride[1])
+                for (u64 i2 = cb[2]; i2 < ce[2]; i2 += probe.pivot_stride[2]) {
+                    const u64 pos = local.f.pos(i0 - hb[0], i1 - hb[1], i2 - hb[2]);
+                    const qb_t qb = (qb_t)lround_d((double)ldata[pos] * rp);
+                    local.cd[pos] = (float)((double)qb * peb2);
+                }
+        vector<long double> lp(L, 0), lr(L, 0);
+        vector<u64> lc(L, 0);
+        vector<qb_t> context_qbs;
+        for (u64 b0 = cbb[0]; b0 < tend[0]; b0++)
+            for (u64 b1 = cbb[1]; b1 < tend[1]; b1++)
+                for (u64 b2 = cbb[2]; b2 < tend[2]; b2++) {
+                    const bool target = b0 == tb[0] && b1 == tb[1] && b2 == tb[2];
+                    const u64 bb[3] = {b0, b1, b2};
+                    std::array<std::array<u64, 2>, 3> loc;
+                    for (int a = 0; a < 3; a++)
+                        loc[a] = {bb[a] * probe.block_shape[a] - hb[a],
+                                  std::min((bb[a] + 1) * probe.block_shape[a] + 1, probe.f.n[a]) - hb[a]};
+                    std::array<u64, 3> stride = probe.pivot_stride;
+                    for (u64 l = 0; l < L; l++) {
+                        const int dir = probe.plan[l][5] - '0', order = probe.plan[l][9] - '0';
+                        const float leb = local.layer_eb(L, l);
+                        const float slope =
+                            (float)((double)probe.default_slope_v * std::pow((double)probe.P.p.slope_ratio, (double)((int64_t)L - (int64_t)l - 1)));
+                        bool fb = false;
+                        const float t = local.select_t(dir, loc, stride, leb, slope, fb);
+                        vector<qb_t> &qv = target ? layer_qbs[l] : context_qbs;
+                        if (!target) context_qbs.clear();
+                        u64 base = qv.size();
+                        qv.resize(base + local.layer_qb_count(loc, stride, dir));
+                        // dot_compress<true>: the division form on every axis, and the diagnostics.
+                        const double ebd = leb, eb2 = ebd + ebd;
+                        local.for_targets(loc, stride, dir, order, base, [&](u64 i, u64 hs, u64 right, u64 pos, u64 dist, u64 qi) {
+                            const float pred = local.predict(i, hs, right, pos, dist, t);
+                            const double pd = pred, diff = pd - (double)ldata[pos];
+                            const qb_t qb = (qb_t)lround_d((diff * 0.5) / ebd);
+                            qv[qi] = qb;
+                            local.cd[pos] = (float)std::fma(-(double)qb, eb2, pd);
+                            if (target) {
+                                const long double pe = (long double)pred - (long double)ldata[pos];
+                                const long double re = (long double)local.cd[pos] - (long double)ldata[pos];
+                                lp[l] = lp[l] + pe * pe;
+                                lr[l] = lr[l] + re * re;
+                                lc[l]++;
+                            }
+                        });
+                        stride[dir] /= 2;
+                    }
+                }
+        for (u64 l = 0; l < L; l++) {
+            pred_sse[l] = pred_sse[l] + lp[l];
+            rec_sse[l] = rec_sse[l] + lr[l];
+            counts[l] += lc[l];
+        }
+    }
+    fam_result r;
+    long double wh1 = 0, ptot = 0, rtot = 0;
+    for (u64 l = 0; l < L; l++) {
+        if (counts[l] != layer_qbs[l].size()) throw std::runtime_error("predictor-family target count mismatch");
+        r.point_count += counts[l];
+        ptot = ptot + pred_sse[l];
+        rtot = rtot + rec_sse[l];
+        wh1 = wh1 + fam_entropy(layer_qbs[l]) * (long double)counts[l];
+    }
+    if (r.point_count == 0) throw std::runtime_error("predictor-family sample contains no target points");
+    const long double rc = 1.0L / (long double)r.point_count;
+    r.prediction_mse = ptot * rc;
+    r.reconstruction_mse = rtot * rc;
+    const long double range = (long double)probe.max_val - (long double)probe.min_val;
+    r.reconstruction_psnr = r.reconstruction_mse == 0 ? (long double)INFINITY
+                                                      : x87_fyl2x(range * range / r.reconstruction_mse, x87_lg2()) * 10.0L;
+    r.h1 = wh1 * rc;
+    return r;
+}
+
+// select_predictor_family (predictor_family.tpp:217-251). Fills the result's family fields.
+static bool select_family(const codec &C, float rel_eb, aszo_result *out) {
+    const aszo_params &p = C.P.p;
+    codec probe;
+    probe.f = C.f;
+    probe.P = C.P;
+    probe.P.p.h1_block_sampling_num = 256;  // not copied to the probe (copy_settings, :17-37)
+    probe.min_val = C.min_val;
+    probe.max_val = C.max_val;
+    probe.abs_eb = C.abs_eb;
+    probe.default_slope_v = C.default_slope_v;
+    const u64 suffix = std::min<u64>(p.predictor_family_suffix_layers, C.plan.size());
+    probe.plan.assign(C.plan.end() - suffix, C.plan.end());
+    probe.P.p.block_pivot_ratio = rel_eb <= p.predictor_family_fine_eb_threshold ? p.predictor_family_fine_probe_block_pivot_ratio
+                                                                                : p.predictor_family_coarse_probe_block_pivot_ratio;
+    probe.geometry();
+    // make_stratified_targets (:65-86).
+    const u64 total = probe.block_num[0] * probe.block_num[1] * probe.block_num[2];
+    const u64 sc = std::min<u64>(p.predictor_family_sample_blocks, total);
+    std::mt19937_64 rng(0);
+    vector<std::array<u64, 3>> cands;
+    for (u64 s = 0; s < sc; s++) {
+        const u64 sb = (u64)((unsigned __int128)s * total / sc), se = (u64)((unsigned __int128)(s + 1) * total / sc);
+        u64 index = sb + rng() % (se - sb);
+        std::array<u64, 3> t;
+        t[2] = index % probe.block_num[2];
+        index /= probe.block_num[2];
+        t[1] = index % probe.block_num[1];
+        t[0] = index / probe.block_num[1];
+        cands.push_back(t);
+    }
+    // Point budget (:232-234): floor via frndint in round-down mode.
+    const long double frac = (long double)C.f.size() * (long double)p.predictor_family_sample_fraction_limit;
+    const u64 fraction_budget = (u64)floorl(frac);
+    const u64 budget = std::min<u64>(p.predictor_family_sample_point_limit, fraction_budget);
+    vector<std::array<u64, 3>> targets;
+    u64 sampled = 0;
+    for (const auto &c : cands) {  // apply_point_budget (:99-114)
+        u64 pts = 1;
+        for (int a = 0; a < 3; a++) {
+            const u64 b = c[a] * probe.block_shape[a], e = std::min((c[a] + 1) * probe.block_shape[a] + 1, probe.f.n[a]);
+            pts *= e - b;
+        }
+        if (sampled <= budget && pts <= budget - sampled) {
+            targets.push_back(c);
+            sampled += pts;
+        }
+    }
+    out->family_selected = 1;
+    out->fam_suffix_layers = suffix;
+    out->fam_budget = budget;
+    out->fam_probe_bpr = probe.P.p.block_pivot_ratio;
+    out->fam_sampled_points = sampled;
+    out->fam_blocks = targets.size();
+    if (targets.empty()) {
+        out->family_fallback = 1;
+        return false;
+    }
+    const fam_result c = fam_evaluate(probe, C.data, targets, false);
+    const fam_result q = fam_evaluate(probe, C.data, targets, true);
+    const long double score = (c.h1 - q.h1) * (long double)C.default_slope_v + (q.reconstruction_psnr - c.reconstruction_psnr);
+    out->fam_points = c.point_count;
+    out->fam_cubic_mse = c.prediction_mse;
+    out->fam_quintic_mse = q.prediction_mse;
+    out->fam_cubic_psnr = c.reconstruction_psnr;
+    out->fam_quintic_psnr = q.reconstruction_psnr;
+    out->fam_cubic_h1 = c.h1;
+    out->fam_quintic_h1 = q.h1;
+    out->fam_score_gain = score;
+    return score > 0;
+}
+
 // dot_sample_compress (generate_config.tpp:227-254) on the original data, in the form GCC emits:
 // the edge stencils below, the interior as in dot_compress, the residual quantised in float
 // (diff * neg_2_eb), and the squared error accumulated with one fmaf per sample.
@@ -899,6 +1122,13 @@ void aszo_default_params(aszo_params *p) {
     p->max_layer_num = 14;
     p->full_predictor_search_layer_num = 4;
     p->generate_config_sample_stride = 5;
+    p->predictor_family_suffix_layers = 6;
+    p->predictor_family_sample_blocks = 8;
+    p->predictor_family_sample_point_limit = 32768;
+    p->predictor_family_sample_fraction_limit = 0.02f;
+    p->predictor_family_coarse_probe_block_pivot_ratio = 3;
+    p->predictor_family_fine_probe_block_pivot_ratio = 4;
+    p->predictor_family_fine_eb_threshold = 1e-4f;
 }
 
 int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
@@ -908,7 +1138,7 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
         codec C;
         C.f = {{dims[0], dims[1], dims[2]}};
         C.P.init(*p);
-        C.quintic = quintic != 0;
+        C.quintic = quintic > 0;
         if (plan) C.plan = parse_plan(plan);
         C.data = data;
         u64 N = C.f.size();
@@ -922,6 +1152,8 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
         if (!plan) C.plan = generate_plan(data, C.f, C.abs_eb, C.min_val, C.max_val, C.default_slope_v, C.P, dists);
         if (C.plan.size() > 63) throw std::invalid_argument("predictor plan cannot contain more than 63 layers");
         if (C.plan.empty()) throw std::runtime_error("plan search found no layer");
+        if (quintic < 0) C.quintic = select_family(C, rel_eb, out);
+        out->quintic = C.quintic ? 1 : 0;
         {
             std::string pl;
             for (size_t i = 0; i < C.plan.size(); i++) pl += (i ? "," : "") + C.plan[i];

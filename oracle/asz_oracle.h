@@ -31,6 +31,13 @@ typedef struct aszo_params {
     uint64_t max_layer_num;                   /* plan search (generate_config.tpp:444-678) */
     uint64_t full_predictor_search_layer_num;
     uint64_t generate_config_sample_stride;
+    uint64_t predictor_family_suffix_layers;  /* family selection (predictor_family.tpp:217-251) */
+    uint64_t predictor_family_sample_blocks;
+    uint64_t predictor_family_sample_point_limit;
+    float predictor_family_sample_fraction_limit;
+    uint64_t predictor_family_coarse_probe_block_pivot_ratio;
+    uint64_t predictor_family_fine_probe_block_pivot_ratio;
+    float predictor_family_fine_eb_threshold;
 } aszo_params;
 
 void aszo_default_params(aszo_params *p);
@@ -52,10 +59,17 @@ typedef struct aszo_result {
     char plan[64 * 11 + 1];  /* plan used (searched when none was given) */
     uint32_t search_layers;  /* plan search: layers that chose a predictor */
     float best_dist[64];     /* plan search: the winning score of each of those layers */
+    int32_t quintic;         /* family used */
+    int32_t family_selected; /* 1: chosen by the selector (family -1) */
+    int32_t family_fallback; /* selector: no block fit the point budget */
+    uint64_t fam_suffix_layers, fam_blocks, fam_sampled_points, fam_budget, fam_probe_bpr, fam_points;
+    long double fam_cubic_mse, fam_quintic_mse, fam_cubic_psnr, fam_quintic_psnr, fam_cubic_h1, fam_quintic_h1,
+        fam_score_gain;
 } aszo_result;
 
-/* Compress with a given plan ("cubic2_012,cubic1_120,..."), quintic = force_quintic. A NULL plan
- * runs the reference's plan search (param_c::generate_config).
+/* Compress with a given plan ("cubic2_012,cubic1_120,..."), quintic = force_quintic (0 or 1), or
+ * -1 to run the reference's predictor-family selector. A NULL plan runs the reference's plan
+ * search (param_c::generate_config).
  * Returns 0 or a negative error code; err (256 bytes) receives a message. */
 int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p,
                   const char *plan, int quintic, aszo_result *out, char *err);

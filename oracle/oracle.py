@@ -29,6 +29,11 @@ class Params(C.Structure):
         ("insufficient_sample_t", C.c_float),
         ("max_layer_num", C.c_uint64), ("full_predictor_search_layer_num", C.c_uint64),
         ("generate_config_sample_stride", C.c_uint64),
+        ("predictor_family_suffix_layers", C.c_uint64), ("predictor_family_sample_blocks", C.c_uint64),
+        ("predictor_family_sample_point_limit", C.c_uint64), ("predictor_family_sample_fraction_limit", C.c_float),
+        ("predictor_family_coarse_probe_block_pivot_ratio", C.c_uint64),
+        ("predictor_family_fine_probe_block_pivot_ratio", C.c_uint64),
+        ("predictor_family_fine_eb_threshold", C.c_float),
     ]
 
 
@@ -42,6 +47,12 @@ class _Result(C.Structure):
         ("min_val", C.c_float), ("max_val", C.c_float), ("abs_eb", C.c_float),
         ("default_slope", C.c_float), ("t_fallback_count", C.c_uint64),
         ("plan", C.c_char * (64 * 11 + 1)), ("search_layers", C.c_uint32), ("best_dist", C.c_float * 64),
+        ("quintic", C.c_int32), ("family_selected", C.c_int32), ("family_fallback", C.c_int32),
+        ("fam_suffix_layers", C.c_uint64), ("fam_blocks", C.c_uint64), ("fam_sampled_points", C.c_uint64),
+        ("fam_budget", C.c_uint64), ("fam_probe_bpr", C.c_uint64), ("fam_points", C.c_uint64),
+        ("fam_cubic_mse", C.c_longdouble), ("fam_quintic_mse", C.c_longdouble), ("fam_cubic_psnr", C.c_longdouble),
+        ("fam_quintic_psnr", C.c_longdouble), ("fam_cubic_h1", C.c_longdouble), ("fam_quintic_h1", C.c_longdouble),
+        ("fam_score_gain", C.c_longdouble),
     ]
 
 
@@ -99,21 +110,25 @@ class Compressed:
     t_fallback_count: int
     plan: str = ""
     best_dist: tuple = ()
+    quintic: bool = False
+    family: dict = None
 
 
 def _dims(shape):
     return (C.c_uint64 * 3)(*[int(s) for s in shape])
 
 
-def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic: bool = False, params: Params | None = None) -> Compressed:
-    """Compress with `plan`, or run the reference's plan search when plan is None."""
+def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic=False, params: Params | None = None) -> Compressed:
+    """Compress with `plan`, or run the reference's plan search when plan is None. quintic: a bool,
+    or None to run the reference's predictor-family selector."""
     lib = liboracle()
     data = np.ascontiguousarray(data, dtype=np.float32)
     p = params or default_params()
     res = _Result()
     err = C.create_string_buffer(256)
     rc = lib.aszo_compress(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p),
-                           plan.encode() if plan is not None else None, int(quintic), C.byref(res), err)
+                           plan.encode() if plan is not None else None, -1 if quintic is None else int(quintic),
+                           C.byref(res), err)
     if rc != 0:
         raise RuntimeError(err.value.decode())
     try:
@@ -125,7 +140,12 @@ def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic: bool = 
         asz = C.string_at(res.asz, res.asz_len)
         return Compressed(qb, t, rec, pre, asz, res.min_val, res.max_val, res.abs_eb, res.default_slope,
                           int(res.t_fallback_count), res.plan.decode(),
-                          tuple(res.best_dist[i] for i in range(res.search_layers)))
+                          tuple(res.best_dist[i] for i in range(res.search_layers)), bool(res.quintic),
+                          {k: getattr(res, k) for k in ("family_selected", "family_fallback", "fam_suffix_layers",
+                                                          "fam_blocks", "fam_sampled_points", "fam_budget",
+                                                          "fam_probe_bpr", "fam_points", "fam_cubic_mse",
+                                                          "fam_quintic_mse", "fam_cubic_psnr", "fam_quintic_psnr",
+                                                          "fam_cubic_h1", "fam_quintic_h1", "fam_score_gain")})
     finally:
         lib.aszo_free_result(C.byref(res))
 

@@ -105,6 +105,37 @@ def test_plan_search_against_oracle(gpu_ctx):
         assert blob == o.asz
 
 
+def test_family_selection_against_oracle(gpu_ctx):
+    """No family given: the device-run probes make the reference's choice (via the oracle's
+    restatement) with the same long-double figures, on fixed and searched plans."""
+    import asz_b200.api as api
+    from asz_b200 import fields
+    rng = np.random.default_rng(131)
+    orders = ["120", "021", "012"]
+    families = set()
+    for i in range(16):
+        shape = tuple(int(x) for x in rng.integers(7, 60, size=3))
+        f = fields.grf_field(shape, rng.uniform(1.5, 5), rng).astype(np.float32)
+        eb = float(10 ** rng.uniform(-5, -1.5))
+        plan = None if i % 4 == 0 else ",".join(
+            f"cubic{rng.integers(0, 3)}_{orders[rng.integers(0, 3)]}" for _ in range(int(rng.integers(1, 10))))
+        bpr = int(rng.integers(1, 6))
+        try:
+            o = O.compress(f, eb, plan, None, O.default_params(block_pivot_ratio=bpr))
+        except RuntimeError as e:
+            with pytest.raises(api.AszError, match="no target points"):
+                gpu_ctx.compress(f, eb, plan, "auto", api.default_params(block_pivot_ratio=bpr))
+            assert "no target points" in str(e)
+            continue
+        blob, rep = gpu_ctx.compress(f, eb, plan, "auto", api.default_params(block_pivot_ratio=bpr))
+        assert bool(rep.quintic) == o.quintic
+        families.add(o.quintic)
+        for k in ("fam_cubic_mse", "fam_quintic_mse", "fam_cubic_psnr", "fam_quintic_psnr", "fam_cubic_h1",
+                  "fam_quintic_h1", "fam_score_gain"):
+            assert getattr(rep, k) == o.family[k], k
+        assert blob == o.asz
+
+
 def test_plan_search_c1_like(gpu_ctx):
     """A C1-shaped field (smaller depth) through the plan search, against the oracle."""
     import asz_b200.api as api
@@ -187,6 +218,22 @@ def test_cli_plan_search():
         assert open(z, "rb").read() == want.asz
         for line in ("best_layer_predictor=", "Generate config breakdown: statistics=", "Generate config time:"):
             assert line in r.stdout
+
+
+def test_cli_fully_automatic():
+    """s1_compress with neither a plan nor a family (the launcher's default), against the oracle."""
+    from asz_b200 import fields
+    f = fields.c1_field(seed=5, shape=(20, 64, 60))
+    want = O.compress(f, 1e-3, None, None, O.default_params(block_pivot_ratio=3))
+    with tempfile.TemporaryDirectory() as wd:
+        inp, z = os.path.join(wd, "in.f32"), os.path.join(wd, "x.asz")
+        f.tofile(inp)
+        r = subprocess.run([os.path.join(BIN, "s1_compress"), "-f", "-i", inp, "-z", z, "-3", *[str(s) for s in f.shape],
+                            "-M", "REL", "0.001", "--block-pivot-ratio", "3"], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert open(z, "rb").read() == want.asz
+        assert "Predictor family selection: selector=h1" in r.stdout
+        assert "Predictor family selection time:" in r.stdout
 
 
 def test_corrupt_streams_fail_cleanly(gpu_ctx):

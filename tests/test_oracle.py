@@ -81,6 +81,46 @@ def test_oracle_plan_search_matches_reference_binary():
         assert np.allclose(ref_dists, c.best_dist, rtol=0, atol=1e-6)
 
 
+@pytest.mark.skipif(not _ref_available(), reason="reference binaries not built (make -C oracle ref)")
+def test_oracle_family_selection_matches_reference_binary():
+    """No --predictor-family: the selector's choice, its printed score, and the .asz bytes (the
+    reference's own error when no target point is sampled)."""
+    import re
+
+    from asz_b200 import fields
+    rng = np.random.default_rng(31)
+    orders = ["120", "021", "012"]
+    seen = set()
+    for i in range(14):
+        shape = tuple(int(x) for x in rng.integers(7, 60, size=3))
+        f = fields.grf_field(shape, rng.uniform(1.5, 5), rng).astype(np.float32)
+        eb = float(10 ** rng.uniform(-5, -1.5))
+        plan = None if i % 4 == 0 else ",".join(
+            f"cubic{rng.integers(0, 3)}_{orders[rng.integers(0, 3)]}" for _ in range(int(rng.integers(1, 10))))
+        bpr = int(rng.integers(1, 6))
+        ref_err = ora_err = None
+        with tempfile.TemporaryDirectory() as wd:
+            try:
+                asz, _, out = O.run_reference_compress(f, eb, wd, plan=plan, family=None,
+                                                       extra=["--block-pivot-ratio", str(bpr)], dump=False)
+            except RuntimeError as e:
+                ref_err = str(e).split("error: ")[-1]
+        try:
+            c = O.compress(f, eb, plan, None, O.default_params(block_pivot_ratio=bpr))
+        except RuntimeError as e:
+            ora_err = str(e)
+        assert ref_err == ora_err
+        if ref_err:
+            continue
+        line = [l for l in out.splitlines() if l.startswith("Predictor family selection:")][0]
+        assert (re.search(r"family=(\w+)", line).group(1) == "quintic") == c.quintic
+        seen.add(c.quintic)
+        m = re.search(r"six_score_gain=([-0-9.e+]+)", line)
+        if m:
+            assert f"{float(c.family['fam_score_gain']):.12e}" == f"{float(m.group(1)):.12e}"
+        assert c.asz == asz
+
+
 def test_huffman_known_answer():
     # Symbols [0,0,1]: heap pops leaf 1 (freq 1) then leaf 0 (freq 2) -> codes 1:'0', 0:'1'.
     enc = O.huffman_encode(np.array([0, 0, 1], np.int32))
