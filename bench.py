@@ -35,6 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SHAPE = (512, 512, 512)
+C1_SHAPE = (100, 500, 500)
 REL_EB = 1e-3
 PLAN = ",".join(["cubic2_012"] * 9)
 FAMILY = "cubic"
@@ -207,6 +208,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shape", default="512,512,512", help="field shape (smaller shapes are for profiler captures)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the plan-search / family-selection measurement")
     args = ap.parse_args()
     shape = tuple(int(v) for v in args.shape.split(","))
     if args.impl == "reference":
@@ -348,6 +350,45 @@ def main():
     ev1.record(stream)
     barrier()
     e2e_dec_ms = ev0.elapsed_time(ev1)
+    # Tuning (config 0's form): a C1-shaped field with the plan search and the family selector,
+    # beside a fixed cyclic plan at the same error bound. Device-resident input.
+    tune = None
+    if not args.no_tune:
+        from asz_b200 import fields
+        c1 = torch.from_numpy(fields.c1_field(seed=7 + rank, shape=C1_SHAPE)).to(dev)
+        c1dims = api._dims(C1_SHAPE)
+        pa = api.default_params(block_pivot_ratio=BPR)  # family left automatic
+        pc = api.default_params(block_pivot_ratio=BPR)
+        pc.predictor_family = api.ASZ_FAMILY_CUBIC
+        tr = api.Report()
+
+        def run(params, plan):
+            rc = L.asz_compress(ctx._c, C.c_void_p(c1.data_ptr()), 1, c1dims, C.c_float(REL_EB), C.byref(params), plan,
+                                C.byref(outp), C.byref(outn), C.byref(tr))
+            if rc:
+                raise api.AszError(rc, L.asz_last_error(ctx._c).decode())
+            L.asz_free(outp)
+            return tr
+
+        run(pa, None)  # warm-up
+        barrier()
+        t0 = time.perf_counter()
+        r = run(pa, None)
+        auto_s = time.perf_counter() - t0
+        _, auto_psnr = ctx.stats()
+        auto = {"plan_search_ms": r.plan_s * 1e3, "family_selection_ms": r.family_s * 1e3, "call_ms": auto_s * 1e3,
+                "zstd_ms": r.zstd_s * 1e3, "cr": float(r.cr), "psnr_db": auto_psnr, "family": "quintic" if r.quintic else "cubic",
+                "layers": int(r.layer_num), "plan": r.plan.decode()}
+        cyc = ",".join(["cubic0_012", "cubic1_012", "cubic2_012"] * 4)
+        run(pc, cyc.encode())
+        t0 = time.perf_counter()
+        r = run(pc, cyc.encode())
+        fixed_s = time.perf_counter() - t0
+        _, fixed_psnr = ctx.stats()
+        fixed = {"call_ms": fixed_s * 1e3, "zstd_ms": r.zstd_s * 1e3, "cr": float(r.cr), "psnr_db": fixed_psnr, "plan": cyc}
+        tune = {"field": "x".join(map(str, C1_SHAPE)) + " k^-11/3 GRF + 20 blobs + 1e-4 noise, REL 1e-3, block_pivot_ratio 3",
+                "auto": auto, "fixed_cyclic": fixed, "timing": "host wall clock around one C-ABI call each"}
+        del c1
     L.asz_set_stream(ctx._c, None)
     # Max over ranks.
     times = torch.tensor([core_ms, dec_ms, e2e_ms, e2e_dec_ms], device=dev)
@@ -408,7 +449,7 @@ def main():
         "roofline": roofline, "roofline_path": roofline_path, "profile": prof, "host_phases_ms": host_phases,
         "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
         "cpu_baseline": cpu, "clocks": clocks.summary(),
-        "gpu_launches": int(launches),
+        "gpu_launches": int(launches), "tune": tune,
     }
     print(json.dumps(out))
     if pg:
