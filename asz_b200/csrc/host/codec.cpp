@@ -152,8 +152,11 @@ struct asz_ctx {
     std::string err;
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
-        classes, axis, pre, chunks, out, proxies, tlist, spill, iota, plan_qb, plan_e, plan_aux, plan_pay, probe_in, probe_pred;
-    int tsel_mode = 0;  // 0: certified fast path + exact path for the rest; 1: exact path for all groups
+        classes, axis, pre, chunks, out, proxies, tlist, spill, iota, plan_qb, plan_e, plan_aux, plan_pay, probe_in, probe_pred,
+        rounds_dev, lines_bail, lines_resume;
+    // 0: certified fast path + exact path for the rest; 1: exact path for all groups; 2: as 0, with
+    // the rounds of all-axis-2 plans fused per column of lines.
+    int tsel_mode = 0;
     // Cached glibc log2f tables, keyed by sample count.
     std::map<uint32_t, uint32_t> log2_off;
     std::vector<float> log2_host;
@@ -469,6 +472,33 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
     }
 }
 
+// Bytes of one column's lines for the fused axis-2 rounds (k_lines.cu), or 0 when the plan does not
+// qualify: every round along axis 2, a whole field, at most 64 blocks along axis 2, and the lines of
+// a column within the kernels' shared-memory budget.
+uint32_t lines_smem_bytes(const Geometry &G) {
+    const FieldGeom &fg = G.fg;
+    if (G.rounds.empty() || G.rounds.size() > 63 || fg.origin[0] || fg.origin[1] || fg.origin[2] || fg.block_num[2] > 64)
+        return 0;
+    for (const RoundGeom &rg : G.rounds)
+        if (rg.dir != 2 || rg.stride[0] != 1 || rg.stride[1] != 1 || rg.tcount[0] != fg.n[0] || rg.tcount[1] != fg.n[1])
+            return 0;
+    const u64 l0 = std::min<u64>(fg.block_shape[0] + 1, fg.n[0]), l1 = std::min<u64>(fg.block_shape[1] + 1, fg.n[1]);
+    const u64 bytes = l0 * l1 * fg.n[2] * sizeof(float);
+    return bytes <= lines_smem_limit() ? (uint32_t)bytes : 0;
+}
+
+// The fused launches of one pass: the interior columns with their smaller line buffer, then the
+// edge columns (or every column in one launch when there is no interior).
+struct LinesLaunch {
+    uint32_t set, bytes;
+};
+std::vector<LinesLaunch> lines_launches(const Geometry &G, uint32_t edge_bytes) {
+    const FieldGeom &fg = G.fg;
+    if (fg.block_num[0] < 2 || fg.block_num[1] < 2) return {{kColumnsAll, edge_bytes}};
+    const u64 inner = fg.block_shape[0] * fg.block_shape[1] * fg.n[2] * sizeof(float);
+    return {{kColumnsInterior, (uint32_t)inner}, {kColumnsEdge, edge_bytes}};
+}
+
 bool kernel_limits_ok(const Geometry &G) {
     for (int a = 0; a < 3; a++)
         if (G.fg.n[a] >= (1ull << 32)) return false;
@@ -596,7 +626,8 @@ void asz_destroy(asz_ctx *c) {
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
                       &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
-                      &c->plan_pay, &c->probe_in, &c->probe_pred})
+                      &c->plan_pay, &c->probe_in, &c->probe_pred, &c->rounds_dev, &c->lines_bail,
+                      &c->lines_resume})
         b->release();
     c->pre_zstd.release();
     c->raw_in.release();
@@ -636,6 +667,7 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t why[3];  // fast path: [0] handed off (bins too spread), [1] handed off (undecided), [2] settled window by window
     uint32_t dec_err;      // batched Huffman decoding: error bits
     uint32_t dec_changed;  // batched Huffman decoding: a chunk start moved in the last pass
+    uint32_t resume_count;  // fused axis-2 compression: columns waiting for the exact path
     int32_t qb_range[2 * 64];
     float h1[3 * 64];
     float x[3 * 64];
@@ -1268,6 +1300,41 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
     int32_t *d_qb = ctx->qb.as<int32_t>();
     float *d_tval = ctx->tval.as<float>();
     int64_t *d_tint = ctx->tint.as<int64_t>();
+    // Every round along axis 2 on a whole field: all rounds fused per column of lines (k_lines.cu).
+    const uint32_t line_bytes = (!a.probe && !a.origin && ctx->tsel_mode == 2) ? lines_smem_bytes(G) : 0;
+    const int tsel_mode = ctx->tsel_mode == 2 ? 0 : ctx->tsel_mode;  // 2: the fast path with fused rounds
+    const u64 ncols = G.fg.block_num[0] * G.fg.block_num[1];
+    const RoundGeom *d_rounds = nullptr;
+    const u64 *d_qoff = nullptr;
+    u64 lines_alg_bytes = 0;
+    if (line_bytes) {
+        const u64 rbytes = L * sizeof(RoundGeom);
+        CK(ctx->rounds_dev.reserve(rbytes + (L + 1) * sizeof(u64)));
+        uint8_t *rd = ctx->rounds_dev.as<uint8_t>();
+        CK(cudaMemcpyAsync(rd, G.rounds.data(), rbytes, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(rd + rbytes, qb_off.data(), (L + 1) * sizeof(u64), cudaMemcpyHostToDevice, st));
+        d_rounds = (const RoundGeom *)rd;
+        d_qoff = (const u64 *)(rd + rbytes);
+        CK(ctx->lines_bail.reserve(std::max<u64>(G.nblocks * L, 1) * sizeof(uint32_t)));
+        CK(ctx->lines_resume.reserve(std::max<u64>(4 * ncols, 1) * sizeof(uint32_t)));
+        // Algorithmic bytes: the field loaded and stored once; per target its original value read
+        // and its QB written; per coefficient sample its original value read.
+        lines_alg_bytes = N * 8;
+        for (u64 l = 0; l < L; l++) {
+            lines_alg_bytes += G.rounds[l].targets * 8;
+            for (int c = 0; c < 27; c++) {
+                const ClassInfo &ci = G.classes[l][c];
+                if (ci.fallback || !ci.n) continue;
+                u64 m = 1;
+                for (int ax = 0; ax < 3; ax++) {
+                    const u64 nb = G.fg.block_num[ax], k = ax == 0 ? c / 9 : ax == 1 ? (c / 3) % 3 : c % 3;
+                    m *= k == 0 ? 1 : k == 1 ? (nb > 2 ? nb - 2 : 0) : (nb >= 2 ? 1 : 0);
+                }
+                lines_alg_bytes += m * ci.n * 4;
+            }
+        }
+    }
+    u64 lines_exact = 0, lines_serial = 0;
     hs_prep.reset();
     std::optional<HostScope> hs_rounds(std::in_place, ctx, "host:rounds");
     while (true) {
@@ -1286,14 +1353,77 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
             ProfScope ps(ctx, "pivot_compress", G.pivots * 12);
             CK(launch_pivot_compress(G.pg, d_in, d_rec, d_qb + qb_off[0], &dm->qb_range[0], st));
         }
-        for (u64 l = 0; l < L; l++) {
+        if (line_bytes) {
+            // Fused pass over all columns. Blocks the certified fast path cannot settle stop their
+            // column at that round; the exact path then settles them round by round, and their
+            // columns resume from there, until no column is left waiting (at most one pass per round).
+            const uint32_t nov = (uint32_t)(overrides.size() / 3);
+            uint32_t *d_bail = ctx->lines_bail.as<uint32_t>();
+            uint32_t *d_res[2] = {ctx->lines_resume.as<uint32_t>(), ctx->lines_resume.as<uint32_t>() + 2 * ncols};
+            uint32_t n_resume = 0;
+            int cur = 0;
+            lines_exact = lines_serial = 0;
+            CK(cudaMemsetAsync(dm->spill_count, 0, sizeof(dm->spill_count), st));
+            for (u64 pass = 0;; pass++) {
+                if (pass > L) return fail(ctx, ASZ_E_DEVICE, "fused rounds did not finish");
+                CK(cudaMemsetAsync(dm->list_count, 0, sizeof(dm->list_count), st));
+                CK(cudaMemsetAsync(&dm->resume_count, 0, 4, st));
+                {
+                    ProfScope ps(ctx, "lines_compress", pass ? 0 : lines_alg_bytes);
+                    std::vector<LinesLaunch> lls = lines_launches(G, line_bytes);
+                    if (pass) lls = {{kColumnsAll, line_bytes}};  // resumptions list column indices
+                    for (const LinesLaunch &ll : lls)
+                        CK(launch_lines_compress(G.fg, d_rounds, d_ent, d_qoff, ctx->classes.as<ClassInfo>(), d_in, d_rec,
+                                                 ctx->log2arena.as<float>(), R2, t_default, d_tval, d_tint, &dm->fb, d_qb,
+                                                 dm->qb_range, ctx->overrides.as<uint32_t>(), nov, dm->why,
+                                                 pass ? d_res[cur] : nullptr, n_resume, d_bail, dm->list_count,
+                                                 d_res[cur ^ 1], &dm->resume_count, &dm->err, ll.set, ll.bytes, st));
+                }
+                uint32_t bails[64], spills[64], nres = 0;
+                CK(cudaMemcpyAsync(bails, dm->list_count, sizeof(bails), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(spills, dm->spill_count, sizeof(spills), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&nres, &dm->resume_count, 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                for (u64 l = 0; l < L; l++) lines_serial += spills[l];
+                if (nres == 0) break;
+                if (nres > ncols) return fail(ctx, ASZ_E_DEVICE, "fused rounds listed too many columns");
+                CK(cudaMemsetAsync(dm->spill_count, 0, sizeof(dm->spill_count), st));
+                for (u64 l = 0; l < L; l++) {
+                    if (!bails[l]) continue;
+                    if (bails[l] > G.nblocks) return fail(ctx, ASZ_E_DEVICE, "fused rounds listed too many blocks");
+                    lines_exact += bails[l];
+                    const RoundGeom &rg = G.rounds[l];
+                    const ClassInfo *cls = ctx->classes.as<ClassInfo>() + 27 * l;
+                    uint32_t *d_spill = ctx->spill.as<uint32_t>(), *d_scount = &dm->spill_count[l];
+                    {
+                        ProfScope ps(ctx, "tsel_exact", 0);
+                        CK(launch_tsel_exact(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default,
+                                             d_tval, d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap,
+                                             &dm->amb_count, ctx->overrides.as<uint32_t>(), nov,
+                                             ctx->proxies.as<float>() + G.nblocks * l * 10, d_bail + G.nblocks * l,
+                                             &dm->list_count[l], d_spill, d_scount, exact_cap(), 148, st));
+                    }
+                    {
+                        ProfScope ps(ctx, "tsel_serial", 0);
+                        CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default,
+                                          ctx->scratch.as<uint8_t>(), sstride, capmax, bcap, tcap, d_tval, d_tint, &dm->fb,
+                                          ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap, &dm->amb_count,
+                                          ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10,
+                                          d_spill, d_scount, slots, &dm->err, st));
+                    }
+                }
+                n_resume = nres;
+                cur ^= 1;
+            }
+        }
+        for (u64 l = 0; l < L && !line_bytes; l++) {
             const RoundGeom &rg = G.rounds[l];
             const ClassInfo *cls = ctx->classes.as<ClassInfo>() + 27 * l;
             const uint32_t nov = (uint32_t)(overrides.size() / 3);
             uint32_t *d_list = ctx->tlist.as<uint32_t>(), *d_lcount = &dm->list_count[l % 64];
             uint32_t *d_spill = ctx->spill.as<uint32_t>(), *d_scount = &dm->spill_count[l % 64];
             CK(cudaMemsetAsync(d_scount, 0, 4, st));
-            if (ctx->tsel_mode == 0) {
+            if (tsel_mode == 0) {
                 // Algorithmic bytes: one read of the 5 operands (4 neighbours + original) per sample.
                 u64 sample_bytes = 0;
                 if (ctx->prof) {
@@ -1351,8 +1481,12 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
         R.exact_groups = 0;
         R.serial_groups = 0;
         for (u64 l = 0; l < L && l < 64; l++) {
-            if (ctx->tsel_mode == 0) R.exact_groups += lcounts[l];
+            if (tsel_mode == 0) R.exact_groups += lcounts[l];
             R.serial_groups += scounts[l];
+        }
+        if (line_bytes) {
+            R.exact_groups = lines_exact;
+            R.serial_groups = lines_serial;
         }
         if (words[0]) return fail(ctx, ASZ_E_DEVICE, "round kernels reported an internal error " + std::to_string(words[0]));
         fb_total = words[1];
@@ -2165,10 +2299,26 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         ProfScope ps(ctx, "pivot_decompress", G.pivots * 8);
         CK(launch_pivot_decompress(G.pg, ctx->qb.as<int32_t>() + qoff[0], d_out, st));
     }
-    for (u64 l = 0; l < L; l++) {
-        ProfScope ps(ctx, "round_decompress", G.rounds[l].targets * 8);
-        CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_ent, ctx->tint.as<int64_t>(),
-                                   ctx->qb.as<int32_t>() + qoff[l + 1], d_out, &dm->err, st));
+    if (const uint32_t line_bytes = ctx->tsel_mode == 2 ? lines_smem_bytes(G) : 0) {
+        // Every round along axis 2: all rounds fused per column of lines (k_lines.cu).
+        const u64 rbytes = L * sizeof(RoundGeom);
+        CK(ctx->rounds_dev.reserve(rbytes + (L + 1) * sizeof(u64)));
+        uint8_t *rd = ctx->rounds_dev.as<uint8_t>();
+        CK(cudaMemcpyAsync(rd, G.rounds.data(), rbytes, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(rd + rbytes, qoff.data(), (L + 1) * sizeof(u64), cudaMemcpyHostToDevice, st));
+        u64 tgt = 0;
+        for (u64 l = 0; l < L; l++) tgt += G.rounds[l].targets;
+        // Algorithmic bytes: the field loaded and stored once, one QB read per target.
+        ProfScope ps(ctx, "lines_decompress", N * 8 + tgt * 4);
+        for (const LinesLaunch &ll : lines_launches(G, line_bytes))
+            CK(launch_lines_decompress(G.fg, (const RoundGeom *)rd, d_ent, (const u64 *)(rd + rbytes),
+                                       ctx->tint.as<int64_t>(), ctx->qb.as<int32_t>(), d_out, &dm->err, ll.set, ll.bytes, st));
+    } else {
+        for (u64 l = 0; l < L; l++) {
+            ProfScope ps(ctx, "round_decompress", G.rounds[l].targets * 8);
+            CK(launch_round_decompress(G.fg, G.rounds[l], (uint32_t)l, d_ent, ctx->tint.as<int64_t>(),
+                                       ctx->qb.as<int32_t>() + qoff[l + 1], d_out, &dm->err, st));
+        }
     }
     uint32_t errw, decw;
     CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
@@ -2487,7 +2637,7 @@ extern "C" int64_t asz_check_hashorder(const int64_t *a, const int64_t *b, uint6
 }
 
 extern "C" int asz_set_tsel_mode(asz_ctx *ctx, int mode) {
-    if (!ctx || mode < 0 || mode > 1) return ASZ_E_ARG;
+    if (!ctx || mode < 0 || mode > 2) return ASZ_E_ARG;
     ctx->tsel_mode = mode;
     return ASZ_OK;
 }

@@ -74,6 +74,29 @@ cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, cons
 cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const AxisEntry *ent,
                                     const int64_t *t_int, const int32_t *qb, float *rec, uint32_t *err, cudaStream_t st);
 
+// Fused rounds for plans whose every round runs along axis 2 (k_lines.cu). rounds and qoff (the
+// stream offsets, pivots first) are device copies of the plan's round table; line_bytes is the
+// size of one column's lines (at most lines_smem_limit()), and the field has at most 64 blocks
+// along axis 2.
+// set selects the columns of a launch (kColumnsAll, or kColumnsInterior: b0 >= 1 and b1 >= 1, at most
+// block_shape[0] * block_shape[1] lines each; kColumnsEdge: the rest); a resumption lists column
+// indices of the same set.
+enum : uint32_t { kColumnsAll = 0, kColumnsInterior = 1, kColumnsEdge = 2 };
+uint32_t lines_smem_limit();
+cudaError_t launch_lines_decompress(const FieldGeom &fg, const RoundGeom *rounds, const AxisEntry *ent, const uint64_t *qoff,
+                                    const int64_t *t_int, const int32_t *qb, float *rec, uint32_t *err, uint32_t set,
+                                    uint32_t line_bytes, cudaStream_t st);
+// A full pass (resume_in == nullptr) or the resumption of the listed (column, round) pairs. Blocks
+// handed to the exact path are listed per round in bail_blocks + round * nblocks (bail_count[round])
+// and their columns in resume_out (resume_count).
+cudaError_t launch_lines_compress(const FieldGeom &fg, const RoundGeom *rounds, const AxisEntry *ent, const uint64_t *qoff,
+                                  const ClassInfo *classes, const float *orig, float *rec, const float *log2arena, float R2,
+                                  float t_default, float *tval, int64_t *t_int, uint32_t *fb_count, int32_t *qb,
+                                  int32_t *qb_range, const uint32_t *overrides, uint32_t n_overrides, uint32_t *why,
+                                  const uint32_t *resume_in, uint32_t n_resume, uint32_t *bail_blocks, uint32_t *bail_count,
+                                  uint32_t *resume_out, uint32_t *resume_count, uint32_t *err, uint32_t set,
+                                  uint32_t line_bytes, cudaStream_t st);
+
 cudaError_t launch_error_stats(const float *x, const float *y, uint64_t n, unsigned int *max_bits, double *sse,
                                cudaStream_t st);
 

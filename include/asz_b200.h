@@ -159,8 +159,10 @@ typedef struct asz_profile_entry {
 int asz_profile_enable(asz_ctx *ctx, int on);
 
 /* Per-block coefficient selection strategy. 0 (default): a certified order-free fast path settles
- * most (block, round) groups and the exact hash-order replay settles the rest. 1: the exact replay
- * for every group. Both give the reference's choices; 1 exists to test the exact path alone. */
+ * most (block, round) groups and the exact hash-order replay settles the rest, one launch per
+ * round. 1: the exact replay for every group. 2: as 0, and plans with every round along axis 2
+ * run all their rounds fused per column of lines held in shared memory (compression and
+ * decompression). All give the reference's choices and bytes. */
 int asz_set_tsel_mode(asz_ctx *ctx, int mode);
 /* Copies up to max entries accumulated since the last reset; returns how many exist. */
 int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset);

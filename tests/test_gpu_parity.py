@@ -84,6 +84,34 @@ def test_c2_like_128_cubic2_plan(gpu_ctx, family):
     assert rep.t_fallback_count > 0
 
 
+@pytest.mark.parametrize("mode", [2, 0], ids=["fused", "per-round"])
+def test_axis2_plans_fused_rounds(gpu_ctx, mode):
+    """Plans with every round along axis 2, with all rounds fused per column of lines (mode 2) and
+    one launch per round (mode 0): random shapes, block ratios (1 to 64 blocks along
+    axis 2), families and error bounds, with noise fields whose groups the fast path hands to the
+    exact path part-way through a column."""
+    from asz_b200 import fields
+    gpu_ctx.set_tsel_mode(mode)
+    rng = np.random.default_rng(2024)
+    handed_off = 0
+    for i in range(16):
+        shape = (int(rng.integers(7, 30)), int(rng.integers(7, 30)), int(rng.integers(16, 400)))
+        if i % 4 == 3:
+            f = rng.random(shape).astype(np.float32)
+            eb = float(10 ** rng.uniform(-5, -4))
+        else:
+            f = fields.grf_field(shape, rng.uniform(1.2, 5), rng).astype(np.float32)
+            eb = float(10 ** rng.uniform(-5, -1.5))
+        layers = int(rng.integers(1, 9))
+        plan = ",".join(f"cubic2_{['120', '021', '012'][int(rng.integers(0, 3))]}" for _ in range(layers))
+        family = ["cubic", "quintic"][i % 2]
+        bpr = int(rng.integers(1, 6))
+        rep = _check_against_oracle(gpu_ctx, f, eb, plan, family, bpr)
+        handed_off += rep.exact_groups
+    gpu_ctx.set_tsel_mode(0)
+    assert handed_off > 0
+
+
 def test_plan_search_against_oracle(gpu_ctx):
     """No plan given: the device plan search picks the reference's plan (checked with the oracle's
     restatement), and the whole compression then matches."""
