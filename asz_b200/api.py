@@ -99,6 +99,9 @@ def lib():
     L.asz_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.asz_compress.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_float, C.POINTER(Params),
                                C.c_char_p, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t), C.POINTER(Report)]
+    L.asz_compress_with_t.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_float,
+                                      C.POINTER(Params), C.c_char_p, C.c_void_p, C.c_uint64,
+                                      C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t), C.POINTER(Report)]
     L.asz_decompress.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.c_float,
                                  C.POINTER(Params), C.c_void_p, C.c_int, C.POINTER(Report)]
     L.asz_free.argtypes = [C.c_void_p]
@@ -245,8 +248,38 @@ class Context:
         self._check(rc)
         return res, rep
 
+    def compress_with_t(self, data, rel_eb: float, plan: str, family: str, params: Params | None, t_int):
+        """Compress with given block-major t codes (NumPy or torch int64, blocks x layers) instead of
+        the coefficient selection; returns (asz bytes, Report)."""
+        p = params if params is not None else default_params()
+        p.predictor_family = _family_code(family)
+        if hasattr(t_int, "detach"):
+            t_int = t_int.detach().cpu().numpy()
+        codes = np.ascontiguousarray(t_int, dtype=np.int64)
+        out = C.POINTER(C.c_uint8)()
+        n = C.c_size_t(0)
+        rep = Report()
+        if _is_cuda_tensor(data):
+            self._use_torch_stream(data)
+            rc = self._L.asz_compress_with_t(self._c, C.c_void_p(data.data_ptr()), 1, _dims(data.shape), C.c_float(rel_eb),
+                                             C.byref(p), plan.encode(), C.c_void_p(codes.ctypes.data), codes.size,
+                                             C.byref(out), C.byref(n), C.byref(rep))
+            self._L.asz_set_stream(self._c, None)
+        else:
+            a = np.ascontiguousarray(data, dtype=np.float32)
+            rc = self._L.asz_compress_with_t(self._c, C.c_void_p(a.ctypes.data), 0, _dims(a.shape), C.c_float(rel_eb),
+                                             C.byref(p), plan.encode(), C.c_void_p(codes.ctypes.data), codes.size,
+                                             C.byref(out), C.byref(n), C.byref(rep))
+        self._check(rc)
+        try:
+            blob = C.string_at(out, n.value)
+        finally:
+            self._L.asz_free(out)
+        return blob, rep
+
     def set_tsel_mode(self, mode: int):
-        """0: certified fast path + exact replay for the rest (default); 1: exact replay everywhere."""
+        """0: certified fast path + exact replay for the rest, one launch per round (default);
+        1: exact replay everywhere; 2: as 0 with the rounds of all-axis-2 plans fused."""
         self._check(self._L.asz_set_tsel_mode(self._c, int(mode)))
 
     def stats(self):

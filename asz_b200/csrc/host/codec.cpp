@@ -165,6 +165,11 @@ struct asz_ctx {
     std::vector<u64> qb_off, qb_len;
     u64 t_len = 0, n_total = 0;
     const float *last_in = nullptr;   // device input of the last compress call
+    // Gradient tuner problem (asz_grad_setup -> asz_grad_gather).
+    Geometry grad_G;
+    const float *grad_in = nullptr;
+    std::vector<uint32_t> grad_off;
+    std::vector<float> grad_meta;
     float last_min = 0, last_max = 0;
     PinnedBuf pre_zstd;   // the last compress call's stream before zstd
     PinnedBuf raw_in;     // decompress: the stream after zstd
@@ -1211,6 +1216,8 @@ struct CoreArgs {
     bool probe;              // predictor-family probe: divide on every axis, predictions to pred_out
     float *pred_out;
     float mn, mx, abs_eb, slope;
+    const int64_t *t_given = nullptr;  // host table of block-major t codes replacing the selection
+    u64 t_len = 0;
 };
 
 struct CoreOut {
@@ -1301,7 +1308,11 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
     float *d_tval = ctx->tval.as<float>();
     int64_t *d_tint = ctx->tint.as<int64_t>();
     // Every round along axis 2 on a whole field: all rounds fused per column of lines (k_lines.cu).
-    const uint32_t line_bytes = (!a.probe && !a.origin && ctx->tsel_mode == 2) ? lines_smem_bytes(G) : 0;
+    if (a.t_given) {
+        if (a.t_len != G.nblocks * L) return fail(ctx, ASZ_E_ARG, "t table length does not match the plan's blocks and rounds");
+        CK(cudaMemcpyAsync(d_tint, a.t_given, a.t_len * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    }
+    const uint32_t line_bytes = (!a.probe && !a.origin && !a.t_given && ctx->tsel_mode == 2) ? lines_smem_bytes(G) : 0;
     const int tsel_mode = ctx->tsel_mode == 2 ? 0 : ctx->tsel_mode;  // 2: the fast path with fused rounds
     const u64 ncols = G.fg.block_num[0] * G.fg.block_num[1];
     const RoundGeom *d_rounds = nullptr;
@@ -1420,6 +1431,14 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
             const RoundGeom &rg = G.rounds[l];
             const ClassInfo *cls = ctx->classes.as<ClassInfo>() + 27 * l;
             const uint32_t nov = (uint32_t)(overrides.size() / 3);
+            if (a.t_given) {
+                // The caller's t codes replace the coefficient selection.
+                CK(launch_tval_from_codes(d_tint, G.nblocks, (uint32_t)L, (uint32_t)l, (float)p.t_precision, d_tval, st));
+                ProfScope ps(ctx, "round_compress", rg.targets * 12);
+                CK(launch_round_compress(G.fg, rg, d_ent, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
+                                         &dm->qb_range[2 * (l + 1)], &dm->err, 0, nullptr, st));
+                continue;
+            }
             uint32_t *d_list = ctx->tlist.as<uint32_t>(), *d_lcount = &dm->list_count[l % 64];
             uint32_t *d_spill = ctx->spill.as<uint32_t>(), *d_scount = &dm->spill_count[l % 64];
             CK(cudaMemsetAsync(d_scount, 0, 4, st));
@@ -1741,8 +1760,9 @@ int select_family(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
     return ASZ_OK;
 }
 
-extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
-                            const asz_params *pp, const char *plan_text, uint8_t **out, size_t *out_len, asz_report *rep) {
+static int compress_entry(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                          const asz_params *pp, const char *plan_text, const int64_t *t_given, uint64_t t_len, uint8_t **out,
+                          size_t *out_len, asz_report *rep) {
     if (!ctx) return ASZ_E_ARG;
     auto t_start = clk::now();
     const uint64_t launches0 = launch_counter();
@@ -1839,7 +1859,7 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
     auto t_core = clk::now();
     CoreOut co;
     {
-        CoreArgs ca{d_in, dims, nullptr, &plan, &p, quintic, false, nullptr, mn, mx, abs_eb, slope};
+        CoreArgs ca{d_in, dims, nullptr, &plan, &p, quintic, false, nullptr, mn, mx, abs_eb, slope, t_given, t_len};
         rc = run_core(ctx, ca, co, R);
         if (rc) return rc;
     }
@@ -1865,6 +1885,10 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
             int64_t c = host_lround_f(t * (float)p.t_precision);
             lo = std::min(lo, c);
             hi = std::max(hi, c);
+        }
+        for (u64 i = 0; t_given && i < t_len; i++) {
+            lo = std::min(lo, t_given[i]);
+            hi = std::max(hi, t_given[i]);
         }
         so[0].lo = lo;
         so[0].hi = hi;
@@ -2058,6 +2082,142 @@ extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, con
         R.total_s = secs(t_start, clk::now());
         *rep = R;
     }
+    return ASZ_OK;
+}
+
+extern "C" int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                            const asz_params *pp, const char *plan_text, uint8_t **out, size_t *out_len, asz_report *rep) {
+    return compress_entry(ctx, in, in_on_device, dims, rel_eb, pp, plan_text, nullptr, 0, out, out_len, rep);
+}
+
+extern "C" int asz_compress_with_t(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                                   const asz_params *pp, const char *plan_text, const int64_t *t_int, uint64_t t_len,
+                                   uint8_t **out, size_t *out_len, asz_report *rep) {
+    if (!ctx) return ASZ_E_ARG;
+    ctx->err.clear();
+    if (!plan_text || !t_int) return fail(ctx, ASZ_E_ARG, "a t table needs a plan and the table");
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    if (p.predictor_family == ASZ_FAMILY_AUTO) return fail(ctx, ASZ_E_ARG, "a t table needs a fixed predictor family");
+    // Codes on the t grid within [t_min, t_max] (s1_compress.cpp:92-98 bound the range).
+    const int64_t lo = (int64_t)std::llround((double)p.t_min * p.t_precision);
+    const int64_t hi = (int64_t)std::llround((double)p.t_max * p.t_precision);
+    for (uint64_t i = 0; i < t_len; i++)
+        if (t_int[i] < lo || t_int[i] > hi) return fail(ctx, ASZ_E_ARG, "t code outside [t_min, t_max] at index " + std::to_string(i));
+    return compress_entry(ctx, in, in_on_device, dims, rel_eb, &p, plan_text, t_int, t_len, out, out_len, rep);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gradient tuner problem: the open-loop AB samples of every (block, round) group (k_grad.cu).
+
+extern "C" int asz_grad_setup(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                              const asz_params *pp, const char *plan_text, asz_grad_problem *out) {
+    if (!ctx) return ASZ_E_ARG;
+    ctx->err.clear();
+    if (!in || !plan_text || !out) return fail(ctx, ASZ_E_ARG, "null argument");
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    int rc = validate(ctx, p, true);
+    if (rc) return rc;
+    rc = validate_dims(ctx, dims, rel_eb);
+    if (rc) return rc;
+    Plan plan;
+    std::string perr;
+    if (!parse_plan(plan_text, plan, perr)) return fail(ctx, ASZ_E_ARG, perr);
+    if (plan.pred.size() > 63) return fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
+    const u64 N = dims[0] * dims[1] * dims[2];
+    cudaStream_t st = ctx->stream;
+    CK(ctx->misc.reserve(sizeof(MiscLayout)));
+    const float *d_in = in;
+    if (!in_on_device) {
+        CK(ctx->in.reserve(N * sizeof(float)));
+        CK(cudaMemcpyAsync(ctx->in.p, in, N * sizeof(float), cudaMemcpyHostToDevice, st));
+        d_in = ctx->in.as<float>();
+    }
+    float mn, mx;
+    rc = compute_range(ctx, d_in, N, mn, mx);
+    if (rc) return rc;
+    if (mn == mx) return fail(ctx, ASZ_E_DATA, "max_val==min_val");
+    const float abs_eb = rel_eb * (mx - mn);
+    const std::vector<float> cand = candidate_t(p);
+    float slope, max_invalid = 0;
+    int reason = 0;
+    rc = default_slope(ctx, d_in, dims, p, abs_eb, mn, mx, cand, slope, max_invalid, reason);
+    if (rc) return rc;
+    Geometry &G = ctx->grad_G;
+    build_geometry(dims, plan, p, abs_eb, slope, p.predictor_family == ASZ_FAMILY_QUINTIC, G);
+    if (!kernel_limits_ok(G)) return fail(ctx, ASZ_E_UNSUPPORTED, "field too large for 32-bit line indexing");
+    const u64 L = plan.pred.size(), groups = G.nblocks * L;
+    ctx->grad_off.assign(groups + 1, 0);
+    ctx->grad_meta.assign(groups * 4, 0.0f);
+    u64 acc = 0;
+    const FieldGeom &fg = G.fg;
+    auto cls_of = [](u64 b, u64 nb) { return b == 0 ? 0 : (b == nb - 1 ? 2 : 1); };
+    for (u64 g = 0; g < G.nblocks; g++) {
+        const u64 b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1], b0 = g / (fg.block_num[1] * fg.block_num[2]);
+        const int c = (cls_of(b0, fg.block_num[0]) * 3 + cls_of(b1, fg.block_num[1])) * 3 + cls_of(b2, fg.block_num[2]);
+        for (u64 l = 0; l < L; l++) {
+            const u64 gid = g * L + l;
+            const ClassInfo &ci = G.classes[l][c];
+            ctx->grad_off[gid] = (uint32_t)acc;
+            acc += ci.fallback ? 0 : ci.n;
+            if (acc > 0xffffffffull) return fail(ctx, ASZ_E_UNSUPPORTED, "more than 2^32 - 1 tuner samples");
+            const RoundGeom &rg = G.rounds[l];
+            float *m = &ctx->grad_meta[gid * 4];
+            m[0] = rg.eb;
+            m[1] = rg.stat_eb;
+            m[2] = rg.neg_2_stat_eb;
+            m[3] = rg.slope;
+        }
+    }
+    ctx->grad_off[groups] = (uint32_t)acc;
+    ctx->grad_in = d_in;
+    asz_grad_problem P{};
+    P.groups = groups;
+    P.samples = acc;
+    P.blocks = G.nblocks;
+    P.layers = L;
+    P.R2 = (mx - mn) * (mx - mn);
+    P.abs_eb = abs_eb;
+    P.default_slope = slope;
+    P.t_min = p.t_min;
+    P.t_max = p.t_max;
+    P.t_precision = p.t_precision;
+    *out = P;
+    return ASZ_OK;
+}
+
+extern "C" int asz_grad_gather(asz_ctx *ctx, float *A, float *B, uint32_t *offsets, float *meta) {
+    if (!ctx) return ASZ_E_ARG;
+    ctx->err.clear();
+    if (!ctx->grad_in || ctx->grad_off.empty()) return fail(ctx, ASZ_E_ARG, "asz_grad_setup has not run");
+    if (!A || !B || !offsets || !meta) return fail(ctx, ASZ_E_ARG, "null argument");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
+    const Geometry &G = ctx->grad_G;
+    const u64 L = G.rounds.size(), groups = G.nblocks * L;
+    cudaStream_t st = ctx->stream;
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    CK(cudaMemcpyAsync(offsets, ctx->grad_off.data(), (groups + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(meta, ctx->grad_meta.data(), groups * 4 * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(ctx->rounds_dev.reserve(L * sizeof(RoundGeom)));
+    CK(cudaMemcpyAsync(ctx->rounds_dev.p, G.rounds.data(), L * sizeof(RoundGeom), cudaMemcpyHostToDevice, st));
+    std::vector<ClassInfo> cls_flat;
+    for (u64 l = 0; l < L; l++) cls_flat.insert(cls_flat.end(), G.classes[l].begin(), G.classes[l].end());
+    CK(ctx->classes.reserve(cls_flat.size() * sizeof(ClassInfo)));
+    CK(cudaMemcpyAsync(ctx->classes.p, cls_flat.data(), cls_flat.size() * sizeof(ClassInfo), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+    {
+        ProfScope ps(ctx, "grad_gather", (u64)ctx->grad_off[groups] * 28);
+        CK(launch_grad_gather(G.fg, ctx->rounds_dev.as<RoundGeom>(), ctx->classes.as<ClassInfo>(), ctx->grad_in, offsets, groups,
+                              A, B, &dm->err, st));
+    }
+    uint32_t errw = 0;
+    CK(cudaMemcpyAsync(&errw, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (errw) return fail(ctx, ASZ_E_DEVICE, "tuner sample lattice does not match the class sample counts");
     return ASZ_OK;
 }
 

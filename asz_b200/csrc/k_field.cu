@@ -252,6 +252,22 @@ cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long lon
     return cudaGetLastError();
 }
 
+// A caller's t codes for round l (block-major table, layer_num per block) as the floats the round
+// kernels read: code / t_precision, exact on the t grid.
+__global__ void tval_from_codes_kernel(const int64_t *__restrict__ t_int, uint64_t nblocks, uint32_t L, uint32_t l,
+                                       float tp, float *__restrict__ tval) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < nblocks; g += (uint64_t)gridDim.x * blockDim.x)
+        tval[g] = __fdiv_rn(__ll2float_rn(t_int[g * L + l]), tp);
+}
+
+cudaError_t launch_tval_from_codes(const int64_t *t_int, uint64_t nblocks, uint32_t L, uint32_t l, float tp, float *tval,
+                                   cudaStream_t st) {
+    if (nblocks == 0) return cudaSuccess;
+    tval_from_codes_kernel<<<grid_for(nblocks, 256, 148 * 8), 256, 0, st>>>(t_int, nblocks, L, l, tp, tval);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *rec, int32_t *qb, int32_t *qb_range,
                                   cudaStream_t st) {
     uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];

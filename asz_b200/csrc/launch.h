@@ -63,6 +63,11 @@ struct PlanCand {
 cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st);
 cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
                                    cudaStream_t st);
+// Open-loop AB samples of every (block, round) group for the gradient tuner (k_grad.cu).
+cudaError_t launch_grad_gather(const FieldGeom &fg, const RoundGeom *rounds, const ClassInfo *classes, const float *x,
+                               const uint32_t *off, uint64_t groups, float *A, float *B, uint32_t *err, cudaStream_t st);
+cudaError_t launch_tval_from_codes(const int64_t *t_int, uint64_t nblocks, uint32_t L, uint32_t l, float tp, float *tval,
+                                   cudaStream_t st);
 cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *rec, int32_t *qb, int32_t *qb_range,
                                   cudaStream_t st);
 cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, float *rec, cudaStream_t st);

@@ -35,16 +35,21 @@ __device__ __forceinline__ int class_of(uint64_t b, uint64_t nb) { return b == 0
 
 // AB keys of one sample from its four neighbours along the round axis and its original value
 // (get_AB_map.tpp:18-21 as emitted), returned as the floats get_h1_psnr converts them to.
-__device__ __forceinline__ void keys_of(float m1, float m3, float p1, float p3, float x0, float neg, float &af, float &bf,
-                                        bool &anz) {
-    float A = __fsub_rn(__fadd_rn(m1, p1), __fadd_rn(m3, p3));
-    float S4 = __fadd_rn(__fadd_rn(p1, p3), __fadd_rn(m1, m3));
-    float B = __double2float_rn(__fma_rn((double)S4, 0.25, -(double)x0));
+// The keys of a sample's A and B (the quantisation step of get_AB_map.tpp:20-21).
+__device__ __forceinline__ void keys_of_ab(float A, float B, float neg, float &af, float &bf, bool &anz) {
     int64_t ak = lround_f(__fmul_rn(A, neg));
     int64_t bk = lround_f(__fmul_rn(B, neg));
     af = __ll2float_rn(ak);
     bf = __ll2float_rn(bk);
     anz = ak != 0;
+}
+
+__device__ __forceinline__ void keys_of(float m1, float m3, float p1, float p3, float x0, float neg, float &af, float &bf,
+                                        bool &anz) {
+    float A = __fsub_rn(__fadd_rn(m1, p1), __fadd_rn(m3, p3));
+    float S4 = __fadd_rn(__fadd_rn(p1, p3), __fadd_rn(m1, m3));
+    float B = __double2float_rn(__fma_rn((double)S4, 0.25, -(double)x0));
+    keys_of_ab(A, B, neg, af, bf, anz);
 }
 
 __device__ __forceinline__ void sample_keys(const float *__restrict__ rec, const float *__restrict__ orig, uint64_t p,

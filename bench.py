@@ -389,6 +389,7 @@ def main():
         tune = {"field": "x".join(map(str, C1_SHAPE)) + " k^-11/3 GRF + 20 blobs + 1e-4 noise, REL 1e-3, block_pivot_ratio 3",
                 "auto": auto, "fixed_cyclic": fixed, "timing": "host wall clock around one C-ABI call each"}
         del c1
+    grad_tune = None if args.no_tune else grad_tune_section(ctx, L, dev, rank, barrier)
     L.asz_set_stream(ctx._c, None)
     # Max over ranks.
     times = torch.tensor([core_ms, dec_ms, e2e_ms, e2e_dec_ms], device=dev)
@@ -449,7 +450,7 @@ def main():
         "roofline": roofline, "roofline_path": roofline_path, "profile": prof, "host_phases_ms": host_phases,
         "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
         "cpu_baseline": cpu, "clocks": clocks.summary(),
-        "gpu_launches": int(launches), "tune": tune,
+        "gpu_launches": int(launches), "tune": tune, "grad_tune": grad_tune,
     }
     print(json.dumps(out))
     if pg:
@@ -457,6 +458,67 @@ def main():
 
 
 import ctypes as _C  # noqa: E402
+
+C4_SHAPE = (256, 256, 256)
+SELECTION_FAMILIES = ("tsel_fast", "tsel_exact", "tsel_serial")
+
+
+def grad_tune_section(ctx, L, dev, rank, barrier):
+    """Per-block t tuning on a C4-recipe field (256^3, per-octant anisotropy): the reference's
+    candidate scan (the library's selection kernels inside a plain compression, device time) against
+    the gradient tuner (open-loop gather + one tune launch, device time), with the resulting
+    compression ratios and errors. Plan from the plan search, block_pivot_ratio 3."""
+    import torch
+
+    from asz_b200 import api, fields, grad
+    x = torch.from_numpy(fields.c4_field(seed=4 + rank, shape=C4_SHAPE)).to(dev)
+    entries = (PROFILE_ENTRY * 64)()
+    out = {"field": "x".join(map(str, C4_SHAPE)) + " per-octant anisotropic GRF (corr. lengths U[2,64], slopes U[2.5,5])",
+           "plan_source": "plan search (no plan given), block_pivot_ratio 3, cubic",
+           "tuner": {"steps": grad.STEPS, "step0": grad.STEP0, "step_cap": grad.STEP_CAP}}
+
+    def profiled(fn):
+        L.asz_profile_enable(ctx._c, 1)
+        L.asz_profile_read(ctx._c, entries, 64, 1)
+        r = fn()
+        n = L.asz_profile_read(ctx._c, entries, 64, 1)
+        L.asz_profile_enable(ctx._c, 0)
+        return r, {entries[i].name.decode(): entries[i].ms for i in range(min(n, 64))}
+
+    for rel_eb in (1e-3, 1e-4):
+        p = api.default_params(block_pivot_ratio=BPR)
+        _, rep0 = ctx.compress(x, rel_eb, None, "cubic", p)
+        plan = rep0.plan.decode()
+        ctx.compress(x, rel_eb, plan, "cubic", p)  # warm-up
+        barrier()
+        (blob, rep), prof = profiled(lambda: ctx.compress(x, rel_eb, plan, "cubic", p))
+        plain_sel_ms = sum(prof.get(k, 0.0) for k in SELECTION_FAMILIES)
+        _, plain_psnr = ctx.stats()
+        plain = {"selection_ms": plain_sel_ms, "cr": 4 * x.numel() / len(blob), "psnr_db": plain_psnr,
+                 "exact_groups": int(rep.exact_groups)}
+        ctx.set_tsel_mode(1)
+        (_, _), prof1 = profiled(lambda: ctx.compress(x, rel_eb, plan, "cubic", p))
+        ctx.set_tsel_mode(0)
+        plain["selection_ms_exact_replay_everywhere"] = sum(prof1.get(k, 0.0) for k in SELECTION_FAMILIES)
+        # Gradient tuner: gather + tune, device time.
+        for _ in range(2):
+            prob, gprof = profiled(lambda: grad.prepare(ctx, x, rel_eb, plan, p))
+            codes, info = grad.tune(prob)
+        gather_ms, tune_ms = gprof.get("grad_gather", 0.0), info.pop("kernel_ms")
+        gblob, grep_ = ctx.compress_with_t(x, rel_eb, plan, "cubic", p, codes)
+        gmax, gpsnr = ctx.stats()
+        g = {"gather_ms": gather_ms, "tune_ms": tune_ms, "selection_ms": gather_ms + tune_ms,
+             "cr": 4 * x.numel() / len(gblob), "psnr_db": gpsnr, "max_err_over_eb": gmax / grep_.abs_eb,
+             "groups": prob.groups, "samples": int(prob.info.samples), **{k: v for k, v in info.items()}}
+        out[f"rel_eb_{rel_eb:g}"] = {
+            "plan": plan, "plain_scan": plain, "gradient": g,
+            "speedup": plain_sel_ms / g["selection_ms"] if g["selection_ms"] else None,
+            "speedup_vs_exact_replay": plain["selection_ms_exact_replay_everywhere"] / g["selection_ms"]
+            if g["selection_ms"] else None,
+            "cr_ratio": g["cr"] / plain["cr"]}
+        del prob
+    del x
+    return out
 
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernel
 # family, from the committed ncu captures; None until captured.

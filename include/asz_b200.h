@@ -135,6 +135,61 @@ int asz_set_stream(asz_ctx *ctx, void *cuda_stream);
 int asz_compress(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
                  const asz_params *p, const char *plan, uint8_t **out, size_t *out_len, asz_report *rep);
 
+/* As asz_compress, with the per-(block, round) coefficients given instead of selected: t_int holds
+ * block-major t codes (for block b = (b0 * block_num1 + b1) * block_num2 + b2 and round l, entry
+ * b * layers + l), each within [t_min, t_max] * t_precision. The stream stores them and every
+ * decoder, the reference's included (decompress.tpp:183-185 reads t as code / t_precision),
+ * reconstructs with them. A plan and a fixed family are required. No counterpart in the reference:
+ * it is the output stage of the gradient tuner (asz_b200/grad.py). */
+int asz_compress_with_t(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                        const asz_params *p, const char *plan, const int64_t *t_int, uint64_t t_len, uint8_t **out,
+                        size_t *out_len, asz_report *rep);
+
+/* ---- Gradient tuner of the per-block coefficients (no counterpart in the reference) ----
+ * A relaxed, differentiable form of the reference's H1-PSNR proxy (get_h_psnr.tpp:6-31) over
+ * open-loop AB samples (get_AB_map.tpp:13-21 read from the original field), one group per
+ * (block, round) indexed block * layers + round like the t stream. The relaxed proxy and its
+ * derivative are defined in asz_b200/csrc/k_grad.cu. Flow: asz_grad_setup sizes the problem,
+ * the caller allocates device buffers of those sizes, asz_grad_gather fills them, then
+ * asz_grad_forward / asz_grad_backward evaluate J(t) and dJ/dt for a t per group (device pointers,
+ * on cuda_stream), and asz_grad_tune runs the whole tuning (projected steps, snap to the t grid,
+ * the reference's exact proxy as the judge against t = 1/4) and writes t codes for
+ * asz_compress_with_t. Status 0 on success, 1 for a bad argument, 7 for a launch error. */
+typedef struct asz_grad_problem {
+    uint64_t groups;       /* blocks * layers */
+    uint64_t samples;      /* AB samples over all groups (A, B buffer length) */
+    uint64_t blocks, layers;
+    float R2;              /* (max - min)^2 of the field */
+    float abs_eb, default_slope;
+    float t_min, t_max;
+    int32_t t_precision;
+} asz_grad_problem;
+
+/* Range, error bound, default slope and plan geometry of a field (plan required); keeps a
+ * reference to `in` (a copy for host input) until the next call. */
+int asz_grad_setup(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
+                   const asz_params *p, const char *plan, asz_grad_problem *out);
+/* Device buffers: A, B (samples floats), offsets (groups + 1 uint32), meta (groups * 4 floats:
+ * layer eb, stat eb, 0.5 / stat eb, layer slope). Runs on the context's stream and waits. */
+int asz_grad_gather(asz_ctx *ctx, float *A, float *B, uint32_t *offsets, float *meta);
+/* J[g] for t[g] (relaxed proxy, lower is better). */
+int asz_grad_forward(const float *A, const float *B, const uint32_t *offsets, const float *meta, float R2,
+                     const float *t, uint64_t groups, float *J, void *cuda_stream);
+/* grad_t[g] = grad_J[g] * dJ[g]/dt[g]. */
+int asz_grad_backward(const float *A, const float *B, const uint32_t *offsets, const float *meta, float R2,
+                      const float *t, const float *grad_J, uint64_t groups, float *grad_t, void *cuda_stream);
+/* steps projected sign-gradient steps from t = 1/4 (step sizes step0 * 2^-k) inside [t_min, t_max],
+ * snapped to codes on the t_precision grid; the reference's proxy (order-free sums, all samples)
+ * keeps code 1/4 * t_precision unless the snapped code scores higher. The steps evaluate J on every
+ * k-th sample of a group, k = ceil(n / step_cap) (step_cap 0 or above 1024: 1024). team: threads
+ * per group (a multiple of 32 up to 512; 0 for the default 256). Writes t_codes[groups] (int64) and, if
+ * non-NULL, t_relaxed[groups]; stats (3 uint32 on the device, zeroed by the caller) count tuned
+ * groups, accepted codes, and groups whose quantised errors spread over more than 262144 bins
+ * (the judge then keeps the default). */
+int asz_grad_tune(const float *A, const float *B, const uint32_t *offsets, const float *meta, float R2, uint64_t groups,
+                  float t_min, float t_max, int32_t t_precision, uint32_t steps, float step0, uint32_t step_cap,
+                  uint32_t team, int64_t *t_codes, float *t_relaxed, uint32_t *stats, void *cuda_stream);
+
 /* Decompress .asz bytes into `out` (prod(dims) floats; host pointer, or device pointer when
  * out_on_device is nonzero). */
 int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const uint64_t dims[3], float rel_eb,

@@ -214,6 +214,7 @@ struct codec {
     vector<vector<qb_t>> qbs;
     vector<i64> t_int;
     u64 t_fallback = 0;
+    const int64_t *t_given = nullptr;  // block-major t codes to use instead of the selection
 
     void geometry() {  // generate_config.tpp:52-68
         pivot_stride = {1, 1, 1};
@@ -384,7 +385,14 @@ struct codec {
                         float slope =
                             (float)((double)default_slope_v * std::pow((double)P.p.slope_ratio, (double)((int)L - (int)l - 1)));
                         bool fb = false;
-                        float t = select_t(dir, loc, stride, leb, slope, fb);
+                        float t;
+                        if (t_given) {
+                            // A caller's t table (block-major codes): the stream stores and the
+                            // decoder uses t_int / t_precision, which any code in range decodes.
+                            t = (float)t_given[t_int.size()] / (float)P.p.t_precision;
+                        } else {
+                            t = select_t(dir, loc, stride, leb, slope, fb);
+                        }
                         if (fb) t_fallback++;
                         t_int.push_back(lround_f(t * (float)P.p.t_precision));
                         // Quantisation: direction 0 multiplies by a hoisted 0.5*(1/eb); directions 1
@@ -400,6 +408,51 @@ struct codec {
                                         out[qi] = qb;
                                         cd[pos] = (float)std::fma(-(double)qb, eb2, pd);
                                     });
+                        stride[dir] /= 2;
+                    }
+                }
+    }
+
+    // The gradient tuner's open-loop samples: for every block (raster order) and round, the AB-map
+    // lattice of select_t (compress.tpp:96-116 region, get_AB_map.tpp:9-17 loops) read from the
+    // ORIGINAL data, recording A = (x-1 + x1) - (x-3 + x3) and B = (float)fma(S4, 0.25, -x) as
+    // get_AB_map.tpp:18-19 computes them; a group that select_t would send to the fallback has none.
+    void grad_samples(vector<float> &A, vector<float> &B, vector<uint64_t> &off) {
+        const u64 L = plan.size();
+        off.assign(1, 0);
+        for (u64 b0 = 0; b0 < block_num[0]; b0++)
+            for (u64 b1 = 0; b1 < block_num[1]; b1++)
+                for (u64 b2 = 0; b2 < block_num[2]; b2++) {
+                    auto loc = block_loc(b0, b1, b2);
+                    std::array<u64, 3> stride = pivot_stride;
+                    for (u64 l = 0; l < L; l++) {
+                        const int dir = plan[l][5] - '0';
+                        if (loc[dir][1] > loc[dir][0] + 3 * stride[dir]) {
+                            std::array<std::array<u64, 2>, 3> sl;
+                            for (int a = 0; a < 3; a++) {
+                                sl[a] = {loc[a][0], loc[a][1]};
+                                if (a != dir && loc[a][0] != 0) sl[a][0] += stride[a];
+                            }
+                            sl[dir][0] += 3 * stride[dir] / 2;
+                            sl[dir][1] -= 3 * stride[dir] / 2;
+                            u64 dist = stride[dir] / 2;
+                            for (int a = dir + 1; a < 3; a++) dist *= f.n[a];
+                            u64 vol = (sl[0][1] - sl[0][0]) * (sl[1][1] - sl[1][0]) * (sl[2][1] - sl[2][0]);
+                            float q = (float)vol / (float)(stride[0] * stride[1] * stride[2] * P.p.h1_block_sampling_num);
+                            u64 ss = (u64)std::cbrt((double)q);
+                            if (ss == 0) ss = 1;
+                            const float *d = data;
+                            for (u64 i0 = sl[0][0]; i0 < sl[0][1]; i0 += stride[0] * ss)
+                                for (u64 i1 = sl[1][0]; i1 < sl[1][1]; i1 += stride[1] * ss)
+                                    for (u64 i2 = sl[2][0]; i2 < sl[2][1]; i2 += stride[2] * ss) {
+                                        u64 p = f.pos(i0, i1, i2);
+                                        float m1 = d[p - dist], m3 = d[p - 3 * dist], p1 = d[p + dist], p3 = d[p + 3 * dist];
+                                        A.push_back((m1 + p1) - (m3 + p3));
+                                        float S4 = (p1 + p3) + (m1 + m3);
+                                        B.push_back((float)std::fma((double)S4, 0.25, -(double)d[p]));
+                                    }
+                        }
+                        off.push_back(A.size());
                         stride[dir] /= 2;
                     }
                 }
@@ -1131,11 +1184,12 @@ void aszo_default_params(aszo_params *p) {
     p->predictor_family_fine_eb_threshold = 1e-4f;
 }
 
-int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
-                  int quintic, aszo_result *out, char *err) {
+static int compress_impl(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
+                         int quintic, const int64_t *t_given, uint64_t t_given_len, aszo_result *out, char *err) {
     try {
         std::memset(out, 0, sizeof(*out));
         codec C;
+        C.t_given = t_given;
         C.f = {{dims[0], dims[1], dims[2]}};
         C.P.init(*p);
         C.quintic = quintic > 0;
@@ -1162,6 +1216,8 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
             for (size_t i = 0; i < out->search_layers; i++) out->best_dist[i] = dists[i];
         }
         C.geometry();
+        if (t_given && t_given_len != C.block_num[0] * C.block_num[1] * C.block_num[2] * C.plan.size())
+            throw std::invalid_argument("t table length does not match the plan's blocks and rounds");
         C.compress_core();
         // Stream assembly: compress.tpp:233-291.
         vector<uint8_t> bs;
@@ -1206,6 +1262,52 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
         out->abs_eb = C.abs_eb;
         out->default_slope = C.default_slope_v;
         out->t_fallback_count = C.t_fallback;
+        return 0;
+    } catch (const std::exception &e) {
+        set_err(err, e.what());
+        return -1;
+    }
+}
+
+int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
+                  int quintic, aszo_result *out, char *err) {
+    return compress_impl(data, dims, rel_eb, p, plan, quintic, nullptr, 0, out, err);
+}
+
+int aszo_compress_with_t(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
+                         int quintic, const int64_t *t_int, uint64_t t_len, aszo_result *out, char *err) {
+    if (!plan || quintic < 0 || !t_int) {
+        set_err(err, "a t table needs a plan and a family");
+        return -1;
+    }
+    return compress_impl(data, dims, rel_eb, p, plan, quintic, t_int, t_len, out, err);
+}
+
+int aszo_grad_samples(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
+                      float *A, float *B, uint64_t *offsets, uint64_t cap, uint64_t *groups, uint64_t *samples, char *err) {
+    try {
+        codec C;
+        C.f = {{dims[0], dims[1], dims[2]}};
+        C.P.init(*p);
+        C.plan = parse_plan(plan);
+        C.data = data;
+        u64 N = C.f.size();
+        auto mm = std::minmax_element(data, data + N);
+        C.min_val = *mm.first;
+        C.max_val = *mm.second;
+        if (C.min_val == C.max_val) throw std::runtime_error("max_val==min_val");
+        C.abs_eb = rel_eb * (C.max_val - C.min_val);
+        C.geometry();
+        vector<float> a, b;
+        vector<uint64_t> off;
+        C.grad_samples(a, b, off);
+        *groups = off.size() - 1;
+        *samples = a.size();
+        if (A && B && offsets && cap >= a.size()) {
+            std::memcpy(A, a.data(), a.size() * 4);
+            std::memcpy(B, b.data(), b.size() * 4);
+            std::memcpy(offsets, off.data(), off.size() * 8);
+        }
         return 0;
     } catch (const std::exception &e) {
         set_err(err, e.what());

@@ -75,6 +75,20 @@ int aszo_compress(const float *data, const uint64_t dims[3], float rel_eb, const
                   const char *plan, int quintic, aszo_result *out, char *err);
 void aszo_free_result(aszo_result *r);
 
+/* As aszo_compress with a given plan and family, but the per-(block, round) t codes come from
+ * t_int (block-major, block_num product x layer_num entries) instead of the coefficient selection.
+ * The stream stores them; the reference's decompressor reads any code as t = code / t_precision. */
+int aszo_compress_with_t(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p,
+                         const char *plan, int quintic, const int64_t *t_int, uint64_t t_len, aszo_result *out,
+                         char *err);
+
+/* The gradient tuner's open-loop AB samples of every (block, round) group (block-major), read
+ * from the original data on get_AB_map's lattice. Sizes come back in groups/samples; the arrays
+ * are filled when they are non-NULL and cap >= samples (offsets: groups + 1 entries). */
+int aszo_grad_samples(const float *data, const uint64_t dims[3], float rel_eb, const aszo_params *p, const char *plan,
+                      float *A, float *B, uint64_t *offsets, uint64_t cap, uint64_t *groups, uint64_t *samples,
+                      char *err);
+
 /* Decompress an .asz produced by the reference or by aszo_compress. */
 int aszo_decompress(const uint8_t *asz, uint64_t asz_len, const uint64_t dims[3], float rel_eb,
                     const aszo_params *p, float *out, char *err);

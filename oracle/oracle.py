@@ -70,7 +70,13 @@ def liboracle():
         lib.aszo_default_params.argtypes = [C.POINTER(Params)]
         lib.aszo_compress.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_float, C.POINTER(Params),
                                       C.c_char_p, C.c_int, C.POINTER(_Result), C.c_char_p]
+        lib.aszo_compress_with_t.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_float, C.POINTER(Params),
+                                             C.c_char_p, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(_Result),
+                                             C.c_char_p]
         lib.aszo_free_result.argtypes = [C.POINTER(_Result)]
+        lib.aszo_grad_samples.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_float, C.POINTER(Params), C.c_char_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
+                                          C.POINTER(C.c_uint64), C.c_char_p]
         lib.aszo_decompress.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.c_float,
                                         C.POINTER(Params), C.c_void_p, C.c_char_p]
         lib.aszo_default_slope.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_float, C.c_float,
@@ -118,17 +124,25 @@ def _dims(shape):
     return (C.c_uint64 * 3)(*[int(s) for s in shape])
 
 
-def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic=False, params: Params | None = None) -> Compressed:
+def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic=False, params: Params | None = None,
+             t_int: np.ndarray | None = None) -> Compressed:
     """Compress with `plan`, or run the reference's plan search when plan is None. quintic: a bool,
-    or None to run the reference's predictor-family selector."""
+    or None to run the reference's predictor-family selector. t_int: block-major per-(block, round)
+    t codes to use instead of the coefficient selection (needs a plan and a family)."""
     lib = liboracle()
     data = np.ascontiguousarray(data, dtype=np.float32)
     p = params or default_params()
     res = _Result()
     err = C.create_string_buffer(256)
-    rc = lib.aszo_compress(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p),
-                           plan.encode() if plan is not None else None, -1 if quintic is None else int(quintic),
-                           C.byref(res), err)
+    if t_int is not None:
+        t_arr = np.ascontiguousarray(t_int, dtype=np.int64)
+        rc = lib.aszo_compress_with_t(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p),
+                                      plan.encode() if plan is not None else None, -1 if quintic is None else int(quintic),
+                                      t_arr.ctypes.data, t_arr.size, C.byref(res), err)
+    else:
+        rc = lib.aszo_compress(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p),
+                               plan.encode() if plan is not None else None, -1 if quintic is None else int(quintic),
+                               C.byref(res), err)
     if rc != 0:
         raise RuntimeError(err.value.decode())
     try:
@@ -148,6 +162,27 @@ def compress(data: np.ndarray, rel_eb: float, plan: str | None, quintic=False, p
                                                           "fam_cubic_h1", "fam_quintic_h1", "fam_score_gain")})
     finally:
         lib.aszo_free_result(C.byref(res))
+
+
+def grad_samples(data: np.ndarray, rel_eb: float, plan: str, params: Params | None = None):
+    """(A, B, offsets) of the gradient tuner's open-loop samples, block-major groups."""
+    lib = liboracle()
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    p = params or default_params()
+    err = C.create_string_buffer(256)
+    g, s = C.c_uint64(), C.c_uint64()
+    rc = lib.aszo_grad_samples(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p), plan.encode(),
+                               None, None, None, 0, C.byref(g), C.byref(s), err)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    A = np.empty(s.value, np.float32)
+    B = np.empty(s.value, np.float32)
+    off = np.empty(g.value + 1, np.uint64)
+    rc = lib.aszo_grad_samples(data.ctypes.data, _dims(data.shape), C.c_float(rel_eb), C.byref(p), plan.encode(),
+                               A.ctypes.data, B.ctypes.data, off.ctypes.data, s.value, C.byref(g), C.byref(s), err)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return A, B, off
 
 
 def decompress(asz: bytes, shape, rel_eb: float, params: Params | None = None) -> np.ndarray:

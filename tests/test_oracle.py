@@ -121,6 +121,32 @@ def test_oracle_family_selection_matches_reference_binary():
         assert c.asz == asz
 
 
+@pytest.mark.skipif(not _ref_available(), reason="reference binaries not built (make -C oracle ref)")
+def test_given_t_tables_decode_with_reference():
+    """Streams compressed with a caller's t table (any code on the t grid in [t_min, t_max], as the
+    gradient tuner writes) decode with the reference's own decompressor to the oracle's
+    reconstruction, and a table equal to the selection's reproduces the selection's bytes."""
+    from asz_b200 import fields
+    rng = np.random.default_rng(808)
+    for i in range(6):
+        shape = tuple(int(x) for x in rng.integers(7, 40, size=3))
+        f = fields.grf_field(shape, rng.uniform(1.5, 5), rng).astype(np.float32)
+        eb = float(10 ** rng.uniform(-4, -2))
+        plan = ",".join(f"cubic{rng.integers(0, 3)}_012" for _ in range(int(rng.integers(1, 7))))
+        bpr = int(rng.integers(1, 5))
+        p = O.default_params(block_pivot_ratio=bpr)
+        quintic = bool(i % 2)
+        sel = O.compress(f, eb, plan, quintic, p)
+        assert O.compress(f, eb, plan, quintic, p, t_int=sel.t_int).asz == sel.asz
+        t = rng.integers(2, 13, size=sel.t_int.shape).astype(np.int64)
+        c = O.compress(f, eb, plan, quintic, p, t_int=t)
+        assert np.array_equal(c.t_int, t)
+        with tempfile.TemporaryDirectory() as wd:
+            dec = O.run_reference_decompress(c.asz, shape, eb, wd, extra=["--block-pivot-ratio", str(bpr)])
+        assert np.array_equal(dec.view(np.uint32), c.recon.view(np.uint32))
+        assert np.abs(dec.astype(np.float64) - f).max() <= 1.01 * c.abs_eb
+
+
 def test_huffman_known_answer():
     # Symbols [0,0,1]: heap pops leaf 1 (freq 1) then leaf 0 (freq 2) -> codes 1:'0', 0:'1'.
     enc = O.huffman_encode(np.array([0, 0, 1], np.int32))
