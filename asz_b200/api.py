@@ -82,6 +82,17 @@ class Report(C.Structure):
         return out
 
 
+class BatchReport(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("total_s", "h2d_s", "prep_s", "tune_s", "rounds_s", "encode_s", "zstd_s",
+                                          "rounds_ms")] + \
+               [(k, C.c_uint64) for k in ("input_bytes", "output_bytes", "kernel_launches")] + \
+               [(k, C.c_uint32) for k in ("tuned_now", "graph_reused", "fields_fallback", "fast_ctas_per_sm",
+                                          "round_ctas_per_sm", "tpl_shift")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def lib():
     """Load libasz_b200.so (raises if it has not been built)."""
     global _LIB
@@ -102,6 +113,9 @@ def lib():
     L.asz_compress_with_t.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_float,
                                       C.POINTER(Params), C.c_char_p, C.c_void_p, C.c_uint64,
                                       C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t), C.POINTER(Report)]
+    L.asz_compress_batch.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_float,
+                                     C.POINTER(Params), C.c_char_p, C.c_void_p, C.POINTER(C.c_size_t),
+                                     C.POINTER(Report), C.POINTER(BatchReport)]
     L.asz_decompress.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.c_float,
                                  C.POINTER(Params), C.c_void_p, C.c_int, C.POINTER(Report)]
     L.asz_free.argtypes = [C.c_void_p]
@@ -276,6 +290,47 @@ class Context:
         finally:
             self._L.asz_free(out)
         return blob, rep
+
+    def compress_batch(self, fields, rel_eb: float, plan: str, family: str = "cubic", params: Params | None = None):
+        """Compress several fields (all NumPy arrays, or all contiguous float32 CUDA tensors on one
+        stream) with one plan; returns (list of asz bytes, list of Report, BatchReport)."""
+        p = params if params is not None else default_params()
+        p.predictor_family = _family_code(family)
+        n = len(fields)
+        ptrs = (C.c_void_p * n)()
+        dims = (C.c_uint64 * (3 * n))()
+        keep = []
+        on_dev = _is_cuda_tensor(fields[0])
+        for i, x in enumerate(fields):
+            if on_dev:
+                import torch
+                if x.dtype != torch.float32 or not x.is_contiguous():
+                    raise ValueError("device inputs must be contiguous float32 tensors")
+                ptrs[i] = x.data_ptr()
+            else:
+                a = np.ascontiguousarray(x, dtype=np.float32)
+                keep.append(a)
+                ptrs[i] = a.ctypes.data
+            for k in range(3):
+                dims[3 * i + k] = int(x.shape[k])
+        outs = (C.POINTER(C.c_uint8) * n)()
+        lens = (C.c_size_t * n)()
+        reps = (Report * n)()
+        br = BatchReport()
+        if on_dev:
+            self._use_torch_stream(fields[0])
+        try:
+            rc = self._L.asz_compress_batch(self._c, n, ptrs, 1 if on_dev else 0, dims, C.c_float(rel_eb), C.byref(p),
+                                            plan.encode(), outs, lens, reps, C.byref(br))
+        finally:
+            if on_dev:
+                self._L.asz_set_stream(self._c, None)
+        self._check(rc)
+        blobs = []
+        for i in range(n):
+            blobs.append(C.string_at(outs[i], lens[i]))
+            self._L.asz_free(outs[i])
+        return blobs, list(reps), br
 
     def set_tsel_mode(self, mode: int):
         """0: certified fast path + exact replay for the rest, one launch per round (default);

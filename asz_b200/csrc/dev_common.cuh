@@ -87,6 +87,50 @@ struct FieldGeom {
     int32_t t_precision;
 };
 
+// ---- Batches: several fields compressed with the same plan, one launch per round for all. ----
+
+struct AmbiguousRecord;
+struct ClassInfo;
+
+// Per-field counters of a batch (device): error bits, fallbacks, ambiguous decisions, and the
+// fast path's hand-off reasons (as asz_report's exact_window, exact_undecided, wide_groups).
+struct BatchCounters {
+    uint32_t err, fb, amb_count, why[3];
+};
+
+// One field of a batch, as the batched kernels see it (device copy).
+struct BatchField {
+    FieldGeom fg;
+    const RoundGeom *rounds;        // layer_num rounds
+    const AxisEntry *ent;           // per-axis target tables of all rounds
+    const ClassInfo *classes;       // 27 per round
+    const float *in;                // original values
+    float *rec, *tval;              // reconstruction, this round's t per block
+    int64_t *tint;                  // t codes, block-major
+    int32_t *qb;                    // QB streams, pivots first
+    const uint64_t *qoff;           // stream offsets (layer_num + 1)
+    int32_t *qb_range;              // [min, max] per stream
+    float *proxies;                 // exact path's proxies, 10 per (block, round)
+    AmbiguousRecord *amb;           // ambiguous decisions for the host replay
+    uint32_t amb_cap;
+    BatchCounters *cnt;
+    float R2;                       // (max - min)^2
+    uint32_t tpl_log2[64];          // threads per target line (log2), per round
+};
+
+#ifdef __CUDACC__
+// Field of global item `gi` given the exclusive prefix `off` (nf + 1 entries) of per-field counts.
+__device__ __forceinline__ uint32_t field_of(const uint64_t *off, uint32_t nf, uint64_t gi) {
+    uint32_t lo = 0, hi = nf;  // off[lo] <= gi < off[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= gi) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+#endif
+
 ASZ_HD uint64_t owner_block(uint64_t i, uint64_t shape) { return i == 0 ? 0 : (i - 1) / shape; }
 
 // Block of coordinate i in a frame starting at h: a block's upper face belongs to it, its lower face

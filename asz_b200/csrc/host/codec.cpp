@@ -24,6 +24,7 @@
 #include <limits>
 #include <map>
 #include <array>
+#include <atomic>
 #include <unordered_map>
 #include <random>
 #include <string>
@@ -154,6 +155,13 @@ struct asz_ctx {
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
         classes, axis, pre, chunks, out, proxies, tlist, spill, iota, plan_qb, plan_e, plan_aux, plan_pay, probe_in, probe_pred,
         rounds_dev, lines_bail, lines_resume;
+    // Batches (asz_compress_batch): per-field slices of these arenas, the captured round sequence
+    // of the last batch, and the launch shapes the autotuner chose per batch shape.
+    DevBuf b_in, b_rec, b_qb, b_tval, b_tint, b_ent, b_cls, b_rounds, b_qoff, b_range, b_range0, b_prox, b_amb, b_cnt,
+        b_fields, b_goff, b_ioff, b_queue, b_hand, b_spill;
+    std::vector<uint64_t> batch_graph_key;
+    cudaGraphExec_t batch_graph = nullptr;
+    std::map<std::vector<uint64_t>, std::array<uint32_t, 3>> batch_tuned;
     // 0: certified fast path + exact path for the rest; 1: exact path for all groups; 2: as 0, with
     // the rounds of all-axis-2 plans fused per column of lines.
     int tsel_mode = 0;
@@ -172,6 +180,7 @@ struct asz_ctx {
     std::vector<float> grad_meta;
     float last_min = 0, last_max = 0;
     PinnedBuf pre_zstd;   // the last compress call's stream before zstd
+    PinnedBuf batch_pre[2];  // batches: two chunks of fields' streams, one encoding while one is compressed
     PinnedBuf raw_in;     // decompress: the stream after zstd
     bool have_last = false;
     // Profiling (asz_profile_*).
@@ -628,13 +637,18 @@ asz_ctx *asz_create(int device) {
 void asz_destroy(asz_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
+    if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
                       &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
                       &c->plan_pay, &c->probe_in, &c->probe_pred, &c->rounds_dev, &c->lines_bail,
-                      &c->lines_resume})
+                      &c->lines_resume, &c->b_in, &c->b_rec, &c->b_qb, &c->b_tval, &c->b_tint, &c->b_ent, &c->b_cls,
+                      &c->b_rounds, &c->b_qoff, &c->b_range, &c->b_range0, &c->b_prox, &c->b_amb, &c->b_cnt, &c->b_fields,
+                      &c->b_goff, &c->b_ioff, &c->b_queue, &c->b_hand, &c->b_spill})
         b->release();
     c->pre_zstd.release();
+    c->batch_pre[0].release();
+    c->batch_pre[1].release();
     c->raw_in.release();
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     if (c->own) cudaStreamDestroy(c->own);
@@ -1760,6 +1774,236 @@ int select_family(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
     return ASZ_OK;
 }
 
+// ---- Entropy stage of one field: the t stream (int64) and L+1 QB streams (int32) Huffman-coded
+// on the device and assembled with their headers into ctx->pre_zstd (compress.tpp:233-291).
+struct EncodeArgs {
+    const Geometry *G;
+    const std::vector<u64> *qb_off, *qb_len;
+    const int32_t *d_qb;       // streams at qb_off
+    const int64_t *d_tint;     // t codes, block-major
+    const int32_t *d_ranges;   // [min, max] per QB stream
+    float mn, mx;
+    bool quintic;
+    const Plan *plan;
+    const asz_params *p;
+    const int64_t *t_given;    // a caller's t table, or nullptr
+    u64 t_len, N;
+};
+
+// Entropy stage of several fields at once: ranges, histograms, code builds (host threads over all
+// streams of all fields), Huffman encoding, and the assembly of each field's pre-zstd stream into
+// one pinned buffer (span[f] = offset, length). Each field's bytes are those of a single-field
+// run; the fields only share the transfers and the synchronisations.
+int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<asz_report *> &Rs,
+                  std::vector<std::pair<u64, u64>> &span, PinnedBuf &pb) {
+    const u64 nf = A.size();
+    cudaStream_t st = ctx->stream;
+    const float t_default = 4.0f / 16;  // insufficient_sample_t (asz_param.hpp:206)
+    std::optional<HostScope> hs_codes(std::in_place, ctx, "host:codes");
+    auto t_huff = clk::now();
+    std::vector<std::vector<StreamOut>> SO(nf);
+    std::vector<std::vector<int32_t>> ranges(nf);
+    for (u64 f = 0; f < nf; f++) {
+        const u64 L = A[f].plan->pred.size();
+        SO[f].resize(L + 2);  // index 0: t stream, 1..L+1: QB streams
+        ranges[f].resize(2 * (L + 1));
+        CK(cudaMemcpyAsync(ranges[f].data(), A[f].d_ranges, ranges[f].size() * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    u64 hist_total = 0;
+    for (u64 f = 0; f < nf; f++) {
+        const EncodeArgs &a = A[f];
+        const u64 L = a.plan->pred.size();
+        std::vector<StreamOut> &so = SO[f];
+        so[0].count = a.G->nblocks * L;
+        const float tv[6] = {t_default, 1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+        for (float t : tv) {
+            int64_t c = host_lround_f(t * (float)a.p->t_precision);
+            lo = std::min(lo, c);
+            hi = std::max(hi, c);
+        }
+        for (u64 i = 0; a.t_given && i < a.t_len; i++) {
+            lo = std::min(lo, a.t_given[i]);
+            hi = std::max(hi, a.t_given[i]);
+        }
+        so[0].lo = lo;
+        so[0].hi = hi;
+        for (u64 s2 = 0; s2 <= L; s2++) {
+            so[s2 + 1].count = (*a.qb_len)[s2];
+            so[s2 + 1].lo = ranges[f][2 * s2];
+            so[s2 + 1].hi = ranges[f][2 * s2 + 1];
+        }
+        for (auto &o : so) {
+            if (!o.count) continue;
+            u64 range = (u64)(o.hi - o.lo) + 1;
+            if (range > (1ull << 27)) return fail(ctx, ASZ_E_UNSUPPORTED, "QB range too wide for the dense histogram");
+            o.hist_off = hist_total;
+            hist_total += range;
+        }
+    }
+    CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
+    CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
+    unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
+    for (u64 f = 0; f < nf; f++) {
+        const EncodeArgs &a = A[f];
+        const u64 L = a.plan->pred.size();
+        std::vector<StreamOut> &so = SO[f];
+        ProfScope ps_hist(ctx, "histogram", (a.G->nblocks * L) * 8 + a.N * 4);
+        if (so[0].count)
+            CK(launch_histogram<int64_t>(a.d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off,
+                                         st));
+        for (u64 s2 = 0; s2 <= L; s2++)
+            if (so[s2 + 1].count)
+                CK(launch_histogram<int32_t>(a.d_qb + (*a.qb_off)[s2], (*a.qb_len)[s2], so[s2 + 1].lo,
+                                             (u64)(so[s2 + 1].hi - so[s2 + 1].lo) + 1, d_hist + so[s2 + 1].hist_off, st));
+    }
+    std::optional<HostScope> hs_h(std::in_place, ctx, "host:codes_hist_d2h");
+    std::vector<u64> hist(hist_total);
+    if (hist_total) CK(cudaMemcpyAsync(hist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    hs_h.reset();
+    std::optional<HostScope> hs_b(std::in_place, ctx, "host:codes_build");
+    // Codes of all streams of all fields, on host threads.
+    std::vector<std::pair<u64, u64>> jobs;
+    for (u64 f = 0; f < nf; f++)
+        for (u64 s2 = 0; s2 < SO[f].size(); s2++)
+            if (SO[f][s2].count) jobs.push_back({f, s2});
+    std::vector<std::string> code_err(jobs.size());
+    std::vector<char> code_ok(jobs.size(), 1);
+    auto build_one = [&](u64 j) {
+        StreamOut &o = SO[jobs[j].first][jobs[j].second];
+        u64 range = (u64)(o.hi - o.lo) + 1;
+        const u64 *h = hist.data() + o.hist_off;
+        // Trim to the symbols present so the code's offset and range match the reference.
+        u64 a0 = 0, b0 = range;
+        while (a0 < b0 && h[a0] == 0) a0++;
+        while (b0 > a0 && h[b0 - 1] == 0) b0--;
+        std::vector<u64> hh(h + a0, h + b0);
+        code_ok[j] = build_code(hh, o.lo + (int64_t)a0, o.lo + (int64_t)b0 - 1, o.count, jobs[j].second == 0, o.code,
+                                code_err[j]);
+        o.lo += (int64_t)a0;
+    };
+    {
+        const u64 nthreads = std::min<u64>(jobs.size(), std::max(1u, std::thread::hardware_concurrency()));
+        std::atomic<u64> next{0};
+        std::vector<std::thread> pool;
+        for (u64 t = 1; t < nthreads; t++)
+            pool.emplace_back([&]() {
+                for (u64 j; (j = next.fetch_add(1)) < jobs.size();) build_one(j);
+            });
+        for (u64 j; (j = next.fetch_add(1)) < jobs.size();) build_one(j);
+        for (auto &t : pool) t.join();
+    }
+    for (u64 j = 0; j < jobs.size(); j++)
+        if (!code_ok[j]) return fail(ctx, ASZ_E_UNSUPPORTED, code_err[j]);
+    u64 code_total = 0, words_total = 0, max_count = 0;
+    std::vector<std::vector<u64>> code_off(nf);
+    for (u64 f = 0; f < nf; f++) {
+        code_off[f].assign(SO[f].size(), 0);
+        for (u64 s2 = 0; s2 < SO[f].size(); s2++) {
+            StreamOut &o = SO[f][s2];
+            if (!o.count) continue;
+            code_off[f][s2] = code_total;
+            code_total += o.code.table.size();
+            o.payload_word_off = words_total;
+            words_total += (o.code.bits + 31) / 32 + 2;
+            max_count = std::max(max_count, o.count);
+        }
+    }
+    hs_b.reset();
+    std::vector<CodeEntry> codes(std::max<u64>(code_total, 1));
+    for (u64 f = 0; f < nf; f++)
+        for (u64 s2 = 0; s2 < SO[f].size(); s2++)
+            if (SO[f][s2].count)
+                std::copy(SO[f][s2].code.table.begin(), SO[f][s2].code.table.end(), codes.begin() + code_off[f][s2]);
+    CK(ctx->codes.reserve(codes.size() * sizeof(CodeEntry)));
+    CK(cudaMemcpyAsync(ctx->codes.p, codes.data(), codes.size() * sizeof(CodeEntry), cudaMemcpyHostToDevice, st));
+    CK(ctx->payload.reserve(std::max<u64>(words_total, 1) * 4));
+    CK(cudaMemsetAsync(ctx->payload.p, 0, std::max<u64>(words_total, 1) * 4, st));
+    CK(ctx->bitoff.reserve(std::max<u64>(max_count, 1) * 8));
+    size_t tmp_bytes = 0;
+    CK(launch_encode<int32_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp_bytes, nullptr, st));
+    size_t tmp64 = 0;
+    CK(launch_encode<int64_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp64, nullptr, st));
+    tmp_bytes = std::max(tmp_bytes, tmp64);
+    CK(ctx->cubtmp.reserve(tmp_bytes));
+    uint32_t *d_pay = ctx->payload.as<uint32_t>();
+    CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
+    hs_codes.reset();
+    for (u64 f = 0; f < nf; f++) {
+        const EncodeArgs &a = A[f];
+        for (u64 s2 = 0; s2 < SO[f].size(); s2++) {
+            StreamOut &o = SO[f][s2];
+            if (!o.count || o.code.maxval == 1) continue;
+            size_t tb = ctx->cubtmp.cap;
+            ProfScope ps(ctx, "huff_encode", o.count * (s2 == 0 ? 8 : 4) + (o.code.bits + 7) / 8);
+            if (s2 == 0)
+                CK(launch_encode<int64_t>(a.d_tint, o.count, o.lo, d_codes + code_off[f][s2], ctx->bitoff.as<u64>(),
+                                          ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
+            else
+                CK(launch_encode<int32_t>(a.d_qb + (*a.qb_off)[s2 - 1], o.count, o.lo, d_codes + code_off[f][s2],
+                                          ctx->bitoff.as<u64>(), ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
+        }
+    }
+    // Stream assembly (compress.tpp:233-291) in pinned memory: the host writes the headers and
+    // code trees while each payload is copied from the device straight into its place.
+    span.assign(nf, {0, 0});
+    u64 all_len = 0;
+    for (u64 f = 0; f < nf; f++) {
+        const u64 L = A[f].plan->pred.size();
+        u64 total_len = 9 + 2 * L;
+        for (auto &o : SO[f]) total_len += 8 + (o.count ? o.code.save_size() + o.code.encode_size() : 0);
+        span[f] = {all_len, total_len};
+        all_len += total_len;
+    }
+    CK(pb.reserve(all_len));
+    pb.len = all_len;
+    auto t_d2h = clk::now();
+    {
+        HostScope hs(ctx, "host:assembly");
+        for (u64 f = 0; f < nf; f++) {
+            const EncodeArgs &a = A[f];
+            const Plan &plan = *a.plan;
+            const u64 L = plan.pred.size();
+            uint8_t *const bs0 = pb.p + span[f].first;
+            uint8_t *w = bs0;
+            std::memcpy(w, &a.mn, 4);
+            std::memcpy(w + 4, &a.mx, 4);
+            w[8] = (uint8_t)(L | 0x40 | (a.quintic ? 0x80 : 0));
+            w += 9;
+            for (u64 l = 0; l < L; l++) {
+                w[0] = (uint8_t)plan.pred[l][5];
+                w[1] = (uint8_t)plan.pred[l][9];
+                w += 2;
+            }
+            for (const StreamOut &o : SO[f]) {
+                for (int i = 0; i < 8; i++) w[i] = (uint8_t)(o.count >> (8 * i));
+                w += 8;
+                if (!o.count) continue;
+                write_tree(o.code, w);
+                w += o.code.save_size();
+                write_len_word(o.code, w);
+                w += 8;
+                if (o.code.maxval != 1) {
+                    u64 nb = (o.code.bits + 7) >> 3;
+                    if (nb) CK(cudaMemcpyAsync(w, d_pay + o.payload_word_off, nb, cudaMemcpyDeviceToHost, st));
+                    w += nb;
+                }
+            }
+            if ((u64)(w - bs0) != span[f].second) return fail(ctx, ASZ_E_DEVICE, "Huffman encoded size mismatch");
+        }
+        CK(cudaStreamSynchronize(st));
+    }
+    const double d2h = secs(t_d2h, clk::now()), huff = secs(t_huff, clk::now());
+    for (asz_report *r : Rs)
+        if (r) {
+            r->d2h_s = d2h;
+            r->huffman_s = huff;
+        }
+    return ASZ_OK;
+}
+
 static int compress_entry(asz_ctx *ctx, const float *in, int in_on_device, const uint64_t dims[3], float rel_eb,
                           const asz_params *pp, const char *plan_text, const int64_t *t_given, uint64_t t_len, uint8_t **out,
                           size_t *out_len, asz_report *rep) {
@@ -1865,174 +2109,15 @@ static int compress_entry(asz_ctx *ctx, const float *in, int in_on_device, const
     }
     Geometry &G = co.G;
     std::vector<u64> &qb_off = co.qb_off, &qb_len = co.qb_len;
-    int32_t *d_qb = ctx->qb.as<int32_t>();
-    int64_t *d_tint = ctx->tint.as<int64_t>();
-    const float t_default = 4.0f / 16;  // insufficient_sample_t (asz_param.hpp:206)
-    std::optional<HostScope> hs_codes(std::in_place, ctx, "host:codes");
-
-    // ---- Huffman stage: t stream (int64) and L+1 QB streams (int32). ----
-    auto t_huff = clk::now();
-    const u64 nstreams = L + 2;  // index 0: t stream, 1..L+1: QB streams
-    std::vector<StreamOut> so(nstreams);
-    std::vector<int32_t> ranges(2 * (L + 1));
-    CK(cudaMemcpyAsync(ranges.data(), dm->qb_range, ranges.size() * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    so[0].count = G.nblocks * L;
     {
-        const float tv[6] = {t_default, 1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
-        int64_t lo = INT64_MAX, hi = INT64_MIN;
-        for (float t : tv) {
-            int64_t c = host_lround_f(t * (float)p.t_precision);
-            lo = std::min(lo, c);
-            hi = std::max(hi, c);
-        }
-        for (u64 i = 0; t_given && i < t_len; i++) {
-            lo = std::min(lo, t_given[i]);
-            hi = std::max(hi, t_given[i]);
-        }
-        so[0].lo = lo;
-        so[0].hi = hi;
+        const std::vector<EncodeArgs> ea{EncodeArgs{&G, &qb_off, &qb_len, ctx->qb.as<int32_t>(), ctx->tint.as<int64_t>(),
+                                                    dm->qb_range, mn, mx, quintic, &plan, &p, t_given, t_len, N}};
+        std::vector<asz_report *> rs{&R};
+        std::vector<std::pair<u64, u64>> span;
+        rc = encode_fields(ctx, ea, rs, span, ctx->pre_zstd);
+        if (rc) return rc;
     }
-    for (u64 s = 0; s <= L; s++) {
-        so[s + 1].count = qb_len[s];
-        so[s + 1].lo = ranges[2 * s];
-        so[s + 1].hi = ranges[2 * s + 1];
-    }
-    u64 hist_total = 0;
-    for (auto &o : so) {
-        if (!o.count) continue;
-        u64 range = (u64)(o.hi - o.lo) + 1;
-        if (range > (1ull << 27)) return fail(ctx, ASZ_E_UNSUPPORTED, "QB range too wide for the dense histogram");
-        o.hist_off = hist_total;
-        hist_total += range;
-    }
-    CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
-    CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
-    unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
-    {
-        ProfScope ps_hist(ctx, "histogram", (G.nblocks * L) * 8 + N * 4);
-        if (so[0].count)
-            CK(launch_histogram<int64_t>(d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off,
-                                         st));
-        for (u64 s = 0; s <= L; s++)
-            if (so[s + 1].count)
-                CK(launch_histogram<int32_t>(d_qb + qb_off[s], qb_len[s], so[s + 1].lo, (u64)(so[s + 1].hi - so[s + 1].lo) + 1,
-                                             d_hist + so[s + 1].hist_off, st));
-    }
-    std::optional<HostScope> hs_h(std::in_place, ctx, "host:codes_hist_d2h");
-    std::vector<u64> hist(hist_total);
-    if (hist_total) CK(cudaMemcpyAsync(hist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    hs_h.reset();
-    std::optional<HostScope> hs_b(std::in_place, ctx, "host:codes_build");
-    // Codes (host) and payload layout.
-    u64 code_total = 0, words_total = 0, max_count = 0;
-    std::vector<u64> code_off(nstreams);
-    // Streams are independent: their codes are built on parallel host threads.
-    std::vector<std::string> code_err(nstreams);
-    std::vector<char> code_ok(nstreams, 1);
-    auto build_one = [&](u64 s) {
-        StreamOut &o = so[s];
-        if (!o.count) return;
-        u64 range = (u64)(o.hi - o.lo) + 1;
-        const u64 *h = hist.data() + o.hist_off;
-        // Trim to the symbols present so the code's offset and range match the reference.
-        u64 a = 0, b = range;
-        while (a < b && h[a] == 0) a++;
-        while (b > a && h[b - 1] == 0) b--;
-        std::vector<u64> hh(h + a, h + b);
-        code_ok[s] = build_code(hh, o.lo + (int64_t)a, o.lo + (int64_t)b - 1, o.count, s == 0, o.code, code_err[s]);
-        o.lo += (int64_t)a;
-    };
-    {
-        std::vector<std::thread> pool;
-        for (u64 s = 1; s < nstreams; s++)
-            if (so[s].count) pool.emplace_back(build_one, s);
-        build_one(0);
-        for (auto &t : pool) t.join();
-    }
-    for (u64 s = 0; s < nstreams; s++)
-        if (!code_ok[s]) return fail(ctx, ASZ_E_UNSUPPORTED, code_err[s]);
-    for (u64 s = 0; s < nstreams; s++) {
-        StreamOut &o = so[s];
-        if (!o.count) continue;
-        code_off[s] = code_total;
-        code_total += o.code.table.size();
-        o.payload_word_off = words_total;
-        words_total += (o.code.bits + 31) / 32 + 2;
-        max_count = std::max(max_count, o.count);
-    }
-    hs_b.reset();
-    std::vector<CodeEntry> codes(std::max<u64>(code_total, 1));
-    for (u64 s = 0; s < nstreams; s++)
-        if (so[s].count) std::copy(so[s].code.table.begin(), so[s].code.table.end(), codes.begin() + code_off[s]);
-    CK(ctx->codes.reserve(codes.size() * sizeof(CodeEntry)));
-    CK(cudaMemcpyAsync(ctx->codes.p, codes.data(), codes.size() * sizeof(CodeEntry), cudaMemcpyHostToDevice, st));
-    CK(ctx->payload.reserve(std::max<u64>(words_total, 1) * 4));
-    CK(cudaMemsetAsync(ctx->payload.p, 0, std::max<u64>(words_total, 1) * 4, st));
-    CK(ctx->bitoff.reserve(std::max<u64>(max_count, 1) * 8));
-    size_t tmp_bytes = 0;
-    CK(launch_encode<int32_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp_bytes, nullptr, st));
-    size_t tmp64 = 0;
-    CK(launch_encode<int64_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp64, nullptr, st));
-    tmp_bytes = std::max(tmp_bytes, tmp64);
-    CK(ctx->cubtmp.reserve(tmp_bytes));
-    uint32_t *d_pay = ctx->payload.as<uint32_t>();
-    CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
-    hs_codes.reset();
-    for (u64 s = 0; s < nstreams; s++) {
-        StreamOut &o = so[s];
-        if (!o.count || o.code.maxval == 1) continue;
-        size_t tb = ctx->cubtmp.cap;
-        ProfScope ps(ctx, "huff_encode", o.count * (s == 0 ? 8 : 4) + (o.code.bits + 7) / 8);
-        if (s == 0)
-            CK(launch_encode<int64_t>(d_tint, o.count, o.lo, d_codes + code_off[s], ctx->bitoff.as<u64>(), ctx->cubtmp.p, tb,
-                                      d_pay + o.payload_word_off, st));
-        else
-            CK(launch_encode<int32_t>(d_qb + qb_off[s - 1], o.count, o.lo, d_codes + code_off[s], ctx->bitoff.as<u64>(),
-                                      ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
-    }
-    // Stream assembly (compress.tpp:233-291) in pinned memory: the host writes the headers and
-    // code trees while each payload is copied from the device straight into its place.
-    u64 total_len = 9 + 2 * L;
-    for (auto &o : so) total_len += 8 + (o.count ? o.code.save_size() + o.code.encode_size() : 0);
     PinnedBuf &pb = ctx->pre_zstd;
-    CK(pb.reserve(total_len));
-    pb.len = total_len;
-    uint8_t *const bs0 = pb.p;
-    uint8_t *w = bs0;
-    std::memcpy(w, &mn, 4);
-    std::memcpy(w + 4, &mx, 4);
-    w[8] = (uint8_t)(L | 0x40 | (quintic ? 0x80 : 0));
-    w += 9;
-    for (u64 l = 0; l < L; l++) {
-        w[0] = (uint8_t)plan.pred[l][5];
-        w[1] = (uint8_t)plan.pred[l][9];
-        w += 2;
-    }
-    auto t_d2h = clk::now();
-    {
-        HostScope hs(ctx, "host:assembly");
-        for (u64 s = 0; s < nstreams; s++) {
-            const StreamOut &o = so[s];
-            for (int i = 0; i < 8; i++) w[i] = (uint8_t)(o.count >> (8 * i));
-            w += 8;
-            if (!o.count) continue;
-            write_tree(o.code, w);
-            w += o.code.save_size();
-            write_len_word(o.code, w);
-            w += 8;
-            if (o.code.maxval != 1) {
-                u64 nb = (o.code.bits + 7) >> 3;
-                if (nb) CK(cudaMemcpyAsync(w, d_pay + o.payload_word_off, nb, cudaMemcpyDeviceToHost, st));
-                w += nb;
-            }
-        }
-        CK(cudaStreamSynchronize(st));
-    }
-    R.d2h_s = secs(t_d2h, clk::now());
-    if ((u64)(w - bs0) != total_len) return fail(ctx, ASZ_E_DEVICE, "Huffman encoded size mismatch");
-    R.huffman_s = secs(t_huff, clk::now());
     R.core_s = secs(t_core, clk::now());
     // zstd level 3 (compress.tpp:294-299).
     auto t_z = clk::now();
@@ -2799,5 +2884,498 @@ extern "C" int64_t asz_check_hashorder(const int64_t *a, const int64_t *b, uint6
 extern "C" int asz_set_tsel_mode(asz_ctx *ctx, int mode) {
     if (!ctx || mode < 0 || mode > 2) return ASZ_E_ARG;
     ctx->tsel_mode = mode;
+    return ASZ_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched compression: many fields of any shapes with one plan and one error bound. Each field's
+// range, default slope and geometry are its own; the rounds run as one sequence for all fields:
+// per round, one launch of each selection kernel (a work queue over every field's (block) groups)
+// and one launch of the round kernel (a work queue over every field's target lines), captured
+// once as a CUDA graph. Each field's result is the single-field result: same kernels per group
+// and per target, only the mapping of work to CTAs differs.
+
+namespace {
+
+struct BatchItem {
+    const float *d_in = nullptr;
+    uint64_t dims[3] = {0, 0, 0};
+    u64 N = 0;
+    float mn = 0, mx = 0, abs_eb = 0, slope = 0, max_invalid = 0;
+    int reason = 0;
+    Geometry G;
+    std::vector<u64> qb_off, qb_len;
+    u64 o_in = 0, o_rec = 0, o_qb = 0, o_tval = 0, o_tint = 0, o_ent = 0, o_prox = 0;
+};
+
+constexpr uint32_t kBatchAmbCap = 1024;
+
+// Launch shapes that change no result: CTAs per SM of the persistent selection and round
+// kernels, and a shift of the threads per target line (fewer threads per line, more lines per CTA).
+using BatchShape = std::array<uint32_t, 3>;
+
+}  // namespace
+
+extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device,
+                                  const uint64_t *dims, float rel_eb, const asz_params *pp, const char *plan_text,
+                                  uint8_t **out, size_t *out_len, asz_report *reps, asz_batch_report *brep) {
+    if (!ctx) return ASZ_E_ARG;
+    auto t_start = clk::now();
+    const uint64_t launches0 = launch_counter();
+    ctx->err.clear();
+    ctx->have_last = false;
+    if (!count || !in || !dims || !plan_text || !out || !out_len) return fail(ctx, ASZ_E_ARG, "null argument");
+    for (uint32_t f = 0; f < count; f++) {
+        out[f] = nullptr;
+        out_len[f] = 0;
+    }
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    int rc = validate(ctx, p, true);
+    if (rc) return rc;
+    if (p.predictor_family == ASZ_FAMILY_AUTO) return fail(ctx, ASZ_E_ARG, "a batch needs a fixed predictor family");
+    Plan plan;
+    std::string perr;
+    if (!parse_plan(plan_text, plan, perr)) return fail(ctx, ASZ_E_ARG, perr);
+    if (plan.pred.size() > 63) return fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    const bool quintic = p.predictor_family == ASZ_FAMILY_QUINTIC;
+    const u64 L = plan.pred.size();
+    const uint32_t nf = count;
+    for (uint32_t f = 0; f < nf; f++) {
+        rc = validate_dims(ctx, dims + 3 * f, rel_eb);
+        if (rc) return fail(ctx, rc, "field " + std::to_string(f) + ": " + ctx->err);
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    CK(ctx->misc.reserve(sizeof(MiscLayout)));
+    asz_batch_report BR{};
+    std::vector<BatchItem> B(nf);
+    // ---- Inputs, ranges, slopes, geometry.
+    u64 in_total = 0;
+    for (uint32_t f = 0; f < nf; f++) {
+        for (int a = 0; a < 3; a++) B[f].dims[a] = dims[3 * f + a];
+        B[f].N = B[f].dims[0] * B[f].dims[1] * B[f].dims[2];
+        B[f].o_in = in_total;
+        if (!in_on_device) in_total += B[f].N;
+        if (!in[f]) return fail(ctx, ASZ_E_ARG, "field " + std::to_string(f) + ": null input");
+    }
+    auto t_h2d = clk::now();
+    if (!in_on_device) {
+        CK(ctx->b_in.reserve(in_total * sizeof(float)));
+        for (uint32_t f = 0; f < nf; f++) {
+            CK(cudaMemcpyAsync(ctx->b_in.as<float>() + B[f].o_in, in[f], B[f].N * sizeof(float), cudaMemcpyHostToDevice, st));
+            B[f].d_in = ctx->b_in.as<float>() + B[f].o_in;
+        }
+        CK(cudaStreamSynchronize(st));
+    } else {
+        for (uint32_t f = 0; f < nf; f++) B[f].d_in = in[f];
+    }
+    BR.h2d_s = secs(t_h2d, clk::now());
+    auto t_prep = clk::now();
+    const std::vector<float> cand = candidate_t(p);
+    u64 nb_total = 0, ent_total = 0, tint_total = 0, qb_total = 0;
+    uint32_t capmax = 1;
+    for (uint32_t f = 0; f < nf; f++) {
+        BatchItem &b = B[f];
+        const std::string tag = "field " + std::to_string(f) + ": ";
+        rc = compute_range(ctx, b.d_in, b.N, b.mn, b.mx);
+        if (rc) return fail(ctx, rc, tag + ctx->err);
+        if (b.mn == b.mx) return fail(ctx, ASZ_E_DATA, tag + "max_val==min_val");
+        b.abs_eb = rel_eb * (b.mx - b.mn);
+        rc = default_slope(ctx, b.d_in, b.dims, p, b.abs_eb, b.mn, b.mx, cand, b.slope, b.max_invalid, b.reason);
+        if (rc) return fail(ctx, rc, tag + ctx->err);
+        build_geometry(b.dims, plan, p, b.abs_eb, b.slope, quintic, b.G);
+        if (!kernel_limits_ok(b.G)) return fail(ctx, ASZ_E_UNSUPPORTED, tag + "field too large for 32-bit line indexing");
+        b.qb_off.assign(L + 1, 0);
+        b.qb_len.assign(L + 1, 0);
+        b.qb_len[0] = b.G.pivots;
+        for (u64 l = 0; l < L; l++) b.qb_len[l + 1] = b.G.rounds[l].qb_total;
+        u64 acc = 0;
+        for (u64 s2 = 0; s2 <= L; s2++) {
+            b.qb_off[s2] = acc;
+            acc += b.qb_len[s2];
+        }
+        if (acc != b.N) return fail(ctx, ASZ_E_DATA, tag + "total_qb_num!=data.size()");
+        for (u64 l = 0; l < L; l++) {
+            for (auto &ci : b.G.classes[l])
+                if (ci.n) ci.log2_off = log2_table(ctx, ci.n);
+            capmax = std::max(capmax, b.G.cap[l]);
+        }
+        b.o_rec = b.o_qb = qb_total;
+        qb_total += b.N;
+        b.o_tval = nb_total;
+        b.o_prox = nb_total * L * 10;
+        nb_total += b.G.nblocks;
+        b.o_tint = tint_total;
+        tint_total += b.G.nblocks * L;
+        b.o_ent = ent_total;
+        ent_total += b.G.ent.size();
+    }
+    rc = upload_log2(ctx);
+    if (rc) return rc;
+    // ---- Arenas and tables.
+    CK(ctx->b_rec.reserve(qb_total * sizeof(float)));
+    CK(ctx->b_qb.reserve(qb_total * sizeof(int32_t)));
+    CK(ctx->b_tval.reserve(std::max<u64>(nb_total, 1) * sizeof(float)));
+    CK(ctx->b_tint.reserve(std::max<u64>(tint_total, 1) * sizeof(int64_t)));
+    CK(ctx->b_ent.reserve(std::max<u64>(ent_total, 1) * sizeof(AxisEntry)));
+    CK(ctx->b_cls.reserve((u64)nf * 27 * L * sizeof(ClassInfo)));
+    CK(ctx->b_rounds.reserve((u64)nf * L * sizeof(RoundGeom)));
+    CK(ctx->b_qoff.reserve((u64)nf * (L + 1) * sizeof(u64)));
+    CK(ctx->b_range.reserve((u64)nf * 2 * (L + 1) * sizeof(int32_t)));
+    CK(ctx->b_range0.reserve((u64)nf * 2 * (L + 1) * sizeof(int32_t)));
+    CK(ctx->b_prox.reserve(std::max<u64>(nb_total * L * 10, 1) * sizeof(float)));
+    CK(ctx->b_amb.reserve((u64)nf * kBatchAmbCap * sizeof(AmbiguousRecord)));
+    CK(ctx->b_cnt.reserve((u64)nf * sizeof(BatchCounters)));
+    CK(ctx->b_fields.reserve((u64)nf * sizeof(BatchField)));
+    CK(ctx->b_goff.reserve((u64)(nf + 1) * sizeof(u64)));
+    CK(ctx->b_ioff.reserve((u64)L * (nf + 1) * sizeof(u64)));
+    CK(ctx->b_queue.reserve((u64)L * 4 * sizeof(uint32_t)));
+    CK(ctx->b_hand.reserve(std::max<u64>(nb_total, 1) * sizeof(unsigned long long)));
+    CK(ctx->b_spill.reserve(std::max<u64>(nb_total, 1) * sizeof(unsigned long long)));
+    uint32_t bcap, tcap;
+    u64 sstride;
+    scratch_dims(capmax, bcap, tcap, sstride);
+    const u64 slots = std::min<u64>(nb_total, 2048);
+    CK(ctx->scratch.reserve(std::max<u64>(slots, 1) * sstride));
+    {
+        std::vector<ClassInfo> cls;
+        std::vector<RoundGeom> rounds;
+        std::vector<u64> qoff;
+        std::vector<int32_t> range0;
+        for (uint32_t f = 0; f < nf; f++) {
+            const BatchItem &b = B[f];
+            CK(cudaMemcpyAsync(ctx->b_ent.as<AxisEntry>() + b.o_ent, b.G.ent.data(), b.G.ent.size() * sizeof(AxisEntry),
+                               cudaMemcpyHostToDevice, st));
+            for (u64 l = 0; l < L; l++) cls.insert(cls.end(), b.G.classes[l].begin(), b.G.classes[l].end());
+            rounds.insert(rounds.end(), b.G.rounds.begin(), b.G.rounds.end());
+            qoff.insert(qoff.end(), b.qb_off.begin(), b.qb_off.end());
+            for (u64 s2 = 0; s2 <= L; s2++) {
+                range0.push_back(INT32_MAX);
+                range0.push_back(INT32_MIN);
+            }
+        }
+        CK(cudaMemcpyAsync(ctx->b_cls.p, cls.data(), cls.size() * sizeof(ClassInfo), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->b_rounds.p, rounds.data(), rounds.size() * sizeof(RoundGeom), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->b_qoff.p, qoff.data(), qoff.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->b_range0.p, range0.data(), range0.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        std::vector<u64> goff(nf + 1, 0);
+        for (uint32_t f = 0; f < nf; f++) goff[f + 1] = goff[f] + B[f].G.nblocks;
+        CK(cudaMemcpyAsync(ctx->b_goff.p, goff.data(), goff.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+    }
+    // Field table and per-round work-item offsets for a launch shape (threads-per-line shift).
+    auto upload_shape = [&](uint32_t tpl_shift) -> int {
+        std::vector<BatchField> F(nf);
+        std::vector<u64> ioff((u64)L * (nf + 1), 0);
+        for (uint32_t f = 0; f < nf; f++) {
+            const BatchItem &b = B[f];
+            BatchField &x = F[f];
+            std::memset(&x, 0, sizeof(x));
+            x.fg = b.G.fg;
+            x.rounds = ctx->b_rounds.as<RoundGeom>() + (u64)f * L;
+            x.ent = ctx->b_ent.as<AxisEntry>() + b.o_ent;
+            x.classes = ctx->b_cls.as<ClassInfo>() + (u64)f * 27 * L;
+            x.in = b.d_in;
+            x.rec = ctx->b_rec.as<float>() + b.o_rec;
+            x.tval = ctx->b_tval.as<float>() + b.o_tval;
+            x.tint = ctx->b_tint.as<int64_t>() + b.o_tint;
+            x.qb = ctx->b_qb.as<int32_t>() + b.o_qb;
+            x.qoff = ctx->b_qoff.as<u64>() + (u64)f * (L + 1);
+            x.qb_range = ctx->b_range.as<int32_t>() + (u64)f * 2 * (L + 1);
+            x.proxies = ctx->b_prox.as<float>() + b.o_prox;
+            x.amb = ctx->b_amb.as<AmbiguousRecord>() + (u64)f * kBatchAmbCap;
+            x.amb_cap = kBatchAmbCap;
+            x.cnt = ctx->b_cnt.as<BatchCounters>() + f;
+            x.R2 = (b.mx - b.mn) * (b.mx - b.mn);
+            for (u64 l = 0; l < L; l++) {
+                const uint32_t lg = round_tpl_log2(b.G.rounds[l].tcount[2]);
+                x.tpl_log2[l] = lg > tpl_shift ? lg - tpl_shift : 0;
+                ioff[l * (nf + 1) + f + 1] = ioff[l * (nf + 1) + f] + round_batch_items(b.G.rounds[l], x.tpl_log2[l]);
+            }
+        }
+        CK(cudaMemcpyAsync(ctx->b_fields.p, F.data(), F.size() * sizeof(BatchField), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->b_ioff.p, ioff.data(), ioff.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
+        return ASZ_OK;
+    };
+    const float t_default = 4.0f / 16;  // insufficient_sample_t (asz_param.hpp:206)
+    const BatchField *dF = ctx->b_fields.as<BatchField>();
+    const u64 *d_goff = ctx->b_goff.as<u64>(), *d_ioff = ctx->b_ioff.as<u64>();
+    uint32_t *d_queue = ctx->b_queue.as<uint32_t>();
+    unsigned long long *d_hand = ctx->b_hand.as<unsigned long long>(), *d_spill = ctx->b_spill.as<unsigned long long>();
+    // The whole sequence: counters and ranges reset, pivots, then per round the batched fast
+    // selection, exact replay, serial spill and prediction.
+    auto enqueue = [&](const BatchShape &sh) -> int {
+        CK(cudaMemcpyAsync(ctx->b_range.p, ctx->b_range0.p, (u64)nf * 2 * (L + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                           st));
+        CK(cudaMemsetAsync(ctx->b_cnt.p, 0, (u64)nf * sizeof(BatchCounters), st));
+        CK(cudaMemsetAsync(ctx->b_queue.p, 0, (u64)L * 4 * sizeof(uint32_t), st));
+        for (uint32_t f = 0; f < nf; f++)
+            CK(launch_pivot_compress(B[f].G.pg, B[f].d_in, ctx->b_rec.as<float>() + B[f].o_rec,
+                                     ctx->b_qb.as<int32_t>() + B[f].o_qb, ctx->b_range.as<int32_t>() + (u64)f * 2 * (L + 1), st));
+        for (u64 l = 0; l < L; l++) {
+            uint32_t *q = d_queue + 4 * l;
+            CK(launch_tsel_fast_batch(dF, d_goff, nf, (uint32_t)l, ctx->log2arena.as<float>(), t_default, q, d_hand, q + 2,
+                                      148 * sh[0], st));
+            CK(launch_tsel_exact_batch(dF, (uint32_t)l, ctx->log2arena.as<float>(), t_default, d_hand, q + 2, d_spill, q + 3,
+                                       exact_cap(), 148, st));
+            CK(launch_tsel_v0_batch(dF, (uint32_t)l, ctx->log2arena.as<float>(), t_default, ctx->scratch.as<uint8_t>(), sstride,
+                                    capmax, bcap, tcap, d_spill, q + 3, slots, st));
+            CK(launch_round_compress_batch(dF, d_ioff + l * (nf + 1), nf, (uint32_t)l, q + 1, 148 * sh[1], st));
+        }
+        return ASZ_OK;
+    };
+    BR.prep_s = secs(t_prep, clk::now());
+    // ---- Launch shapes: measured once per batch shape (the autotuner), then reused.
+    std::vector<uint64_t> shape_key{nf, L, (uint64_t)quintic, p.block_pivot_ratio};
+    for (uint32_t f = 0; f < nf; f++) shape_key.insert(shape_key.end(), B[f].dims, B[f].dims + 3);
+    for (u64 l = 0; l < L; l++) shape_key.push_back((uint64_t)plan.dir[l] * 3 + plan.order[l]);
+    BatchShape best{8, 5, 0};
+    auto tuned = ctx->batch_tuned.find(shape_key);
+    if (tuned != ctx->batch_tuned.end()) {
+        best = tuned->second;
+    } else {
+        auto t_tune = clk::now();
+        cudaEvent_t e0 = prof_event(ctx), e1 = prof_event(ctx);
+        float best_ms = INFINITY;
+        uint32_t last_shift = UINT32_MAX;
+        for (uint32_t shift : {0u, 1u})
+            for (uint32_t fast : {4u, 8u})
+                for (uint32_t round : {3u, 5u}) {
+                    if (shift != last_shift) {
+                        rc = upload_shape(shift);
+                        if (rc) return rc;
+                        last_shift = shift;
+                    }
+                    const BatchShape sh{fast, round, shift};
+                    CK(cudaEventRecord(e0, st));
+                    rc = enqueue(sh);
+                    if (rc) return rc;
+                    CK(cudaEventRecord(e1, st));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = sh;
+                    }
+                }
+        ctx->event_pool.push_back(e0);
+        ctx->event_pool.push_back(e1);
+        ctx->batch_tuned[shape_key] = best;
+        BR.tuned_now = 1;
+        BR.tune_s = secs(t_tune, clk::now());
+    }
+    BR.fast_ctas_per_sm = best[0];
+    BR.round_ctas_per_sm = best[1];
+    BR.tpl_shift = best[2];
+    rc = upload_shape(best[2]);
+    if (rc) return rc;
+    // ---- The round sequence as a CUDA graph (captured once per batch layout).
+    std::vector<uint64_t> graph_key = shape_key;
+    graph_key.insert(graph_key.end(), best.begin(), best.end());
+    for (uint32_t f = 0; f < nf; f++) graph_key.push_back((uint64_t)(uintptr_t)B[f].d_in);
+    for (DevBuf *d : {&ctx->b_rec, &ctx->b_qb, &ctx->b_tval, &ctx->b_tint, &ctx->b_ent, &ctx->b_cls, &ctx->b_rounds,
+                      &ctx->b_qoff, &ctx->b_range, &ctx->b_range0, &ctx->b_prox, &ctx->b_amb, &ctx->b_cnt, &ctx->b_fields,
+                      &ctx->b_goff, &ctx->b_ioff, &ctx->b_queue, &ctx->b_hand, &ctx->b_spill, &ctx->scratch, &ctx->log2arena})
+        graph_key.push_back((uint64_t)(uintptr_t)d->p);
+    graph_key.push_back((uint64_t)(uintptr_t)st);
+    auto t_rounds = clk::now();
+    cudaEvent_t r0 = prof_event(ctx), r1 = prof_event(ctx);
+    if (!ctx->batch_graph || ctx->batch_graph_key != graph_key) {
+        if (ctx->batch_graph) {
+            cudaGraphExecDestroy(ctx->batch_graph);
+            ctx->batch_graph = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        const bool prof = ctx->prof;
+        ctx->prof = false;  // no event records inside the capture
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int erc = enqueue(best);
+        const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        ctx->prof = prof;
+        if (erc) {
+            if (graph) cudaGraphDestroy(graph);
+            return erc;
+        }
+        if (ce != cudaSuccess) return fail(ctx, ASZ_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
+        const cudaError_t ie = cudaGraphInstantiate(&ctx->batch_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            ctx->batch_graph = nullptr;
+            return fail(ctx, ASZ_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        }
+        ctx->batch_graph_key = graph_key;
+    } else {
+        BR.graph_reused = 1;
+    }
+    CK(cudaEventRecord(r0, st));
+    CK(cudaGraphLaunch(ctx->batch_graph, st));
+    CK(cudaEventRecord(r1, st));
+    std::vector<BatchCounters> cnt(nf);
+    CK(cudaMemcpyAsync(cnt.data(), ctx->b_cnt.p, nf * sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, r0, r1));
+        BR.rounds_ms = ms;
+        ctx->event_pool.push_back(r0);
+        ctx->event_pool.push_back(r1);
+    }
+    BR.rounds_s = secs(t_rounds, clk::now());
+    for (uint32_t f = 0; f < nf; f++)
+        if (cnt[f].err)
+            return fail(ctx, ASZ_E_DEVICE, "field " + std::to_string(f) + ": round kernels reported an internal error " +
+                                               std::to_string(cnt[f].err));
+    // ---- Host replay of the ambiguous coefficient decisions (glibc log10f, compress.tpp:127-142).
+    // A field whose replay confirms every provisional choice keeps its batch result; a field whose
+    // replay changes one takes the single-field path, which reruns its rounds with the choices.
+    std::vector<char> single(nf, 0);
+    for (uint32_t f = 0; f < nf; f++) {
+        if (!cnt[f].amb_count) continue;
+        if (cnt[f].amb_count > kBatchAmbCap) {
+            single[f] = 1;
+            continue;
+        }
+        std::vector<AmbiguousRecord> recs(cnt[f].amb_count);
+        CK(cudaMemcpyAsync(recs.data(), ctx->b_amb.as<AmbiguousRecord>() + (u64)f * kBatchAmbCap,
+                           recs.size() * sizeof(AmbiguousRecord), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (const AmbiguousRecord &r : recs) {
+            const float t = replay_decision(r, B[f].G.rounds[r.round].slope);
+            if ((int32_t)host_lround_f(t * (float)p.t_precision) != r.provisional) single[f] = 1;
+        }
+    }
+    // ---- Entropy stage in chunks of fields (one set of transfers and syncs per chunk); zstd on
+    // host threads from the chunk's pinned buffer while the next chunk is encoded.
+    auto t_enc = clk::now();
+    std::vector<asz_report> R(nf);
+    for (auto &r : R) std::memset(&r, 0, sizeof(r));
+    std::vector<std::string> zerr(nf);
+    std::vector<double> zsec(nf, 0.0);
+    std::vector<std::thread> zth[2];
+    auto join_buf = [&](int k) {
+        for (auto &t : zth[k]) t.join();
+        zth[k].clear();
+    };
+    int frc = ASZ_OK;
+    const uint32_t kChunk = 8;
+    std::vector<uint32_t> order;
+    for (uint32_t f = 0; f < nf; f++)
+        if (!single[f]) order.push_back(f);
+    for (size_t c0 = 0, k = 0; c0 < order.size() && !frc; c0 += kChunk, k ^= 1) {
+        join_buf((int)k);  // the zstd threads of two chunks ago are done with this buffer
+        std::vector<EncodeArgs> ea;
+        std::vector<asz_report *> rs;
+        const size_t c1 = std::min(order.size(), c0 + kChunk);
+        for (size_t i = c0; i < c1; i++) {
+            const uint32_t f = order[i];
+            const BatchItem &b = B[f];
+            ea.push_back(EncodeArgs{&b.G, &b.qb_off, &b.qb_len, ctx->b_qb.as<int32_t>() + b.o_qb,
+                                    ctx->b_tint.as<int64_t>() + b.o_tint, ctx->b_range.as<int32_t>() + (u64)f * 2 * (L + 1),
+                                    b.mn, b.mx, quintic, &plan, &p, nullptr, 0, b.N});
+            rs.push_back(&R[f]);
+        }
+        std::vector<std::pair<u64, u64>> span;
+        PinnedBuf &pb = ctx->batch_pre[k];
+        const int erc = encode_fields(ctx, ea, rs, span, pb);
+        if (erc) {
+            frc = erc;
+            break;
+        }
+        for (size_t i = c0; i < c1; i++) {
+            const uint32_t f = order[i];
+            const uint8_t *src = pb.p + span[i - c0].first;
+            const size_t len = span[i - c0].second;
+            R[f].pre_zstd_len = len;
+            zth[k].emplace_back([&, f, src, len]() {
+                auto tz = clk::now();
+                size_t bound = ZSTD_compressBound(len);
+                uint8_t *z = (uint8_t *)std::malloc(bound ? bound : 1);
+                if (!z) {
+                    zerr[f] = "out of host memory";
+                    return;
+                }
+                size_t zl = ZSTD_compress(z, bound, src, len, 3);
+                if (ZSTD_isError(zl)) {
+                    std::free(z);
+                    zerr[f] = std::string("ZSTD_compress: ") + ZSTD_getErrorName(zl);
+                    return;
+                }
+                out[f] = z;
+                out_len[f] = zl;
+                zsec[f] = secs(tz, clk::now());
+            });
+        }
+    }
+    join_buf(0);
+    join_buf(1);
+    for (uint32_t f = 0; f < nf && !frc; f++) {
+        BatchItem &b = B[f];
+        asz_report &r = R[f];
+        if (single[f]) {
+            BR.fields_fallback++;
+            uint8_t *o1 = nullptr;
+            size_t l1 = 0;
+            frc = compress_entry(ctx, b.d_in, 1, b.dims, rel_eb, &p, plan_text, nullptr, 0, &o1, &l1, &r);
+            out[f] = o1;
+            out_len[f] = l1;
+            continue;
+        }
+        r.min_val = b.mn;
+        r.max_val = b.mx;
+        r.abs_eb = b.abs_eb;
+        r.default_slope = b.slope;
+        r.slope_max_invalid_ratio = b.max_invalid;
+        r.slope_fallback_reason = b.reason;
+        r.layer_num = L;
+        r.quintic = quintic ? 1 : 0;
+        r.t_fallback_count = cnt[f].fb;
+        r.ambiguous_decisions = cnt[f].amb_count;
+        r.exact_window = cnt[f].why[0];
+        r.exact_undecided = cnt[f].why[1];
+        r.wide_groups = cnt[f].why[2];
+        for (int a = 0; a < 3; a++) {
+            r.pivot_stride[a] = (uint32_t)b.G.fg.pivot_stride[a];
+            r.block_shape[a] = (uint32_t)b.G.fg.block_shape[a];
+            r.block_num[a] = (uint32_t)b.G.fg.block_num[a];
+        }
+        std::snprintf(r.plan, sizeof(r.plan), "%s", plan_text);
+    }
+    BR.encode_s = secs(t_enc, clk::now());
+    if (frc) {
+        for (uint32_t f = 0; f < nf; f++) {
+            std::free(out[f]);
+            out[f] = nullptr;
+            out_len[f] = 0;
+        }
+        return frc;
+    }
+    for (uint32_t f = 0; f < nf; f++)
+        if (!zerr[f].empty()) {
+            for (uint32_t g = 0; g < nf; g++) {
+                std::free(out[g]);
+                out[g] = nullptr;
+                out_len[g] = 0;
+            }
+            return fail(ctx, ASZ_E_DATA, "field " + std::to_string(f) + ": " + zerr[f]);
+        }
+    for (uint32_t f = 0; f < nf; f++) {
+        BR.zstd_s += zsec[f];
+        if (!R[f].asz_len) {
+            R[f].asz_len = out_len[f];
+            R[f].zstd_s = zsec[f];
+            R[f].cr = (float)B[f].N * sizeof(float) / (float)out_len[f];
+            R[f].br = 8 * sizeof(float) / R[f].cr;
+        }
+        BR.input_bytes += B[f].N * sizeof(float);
+        BR.output_bytes += out_len[f];
+    }
+    BR.kernel_launches = launch_counter() - launches0;
+    BR.total_s = secs(t_start, clk::now());
+    if (reps)
+        for (uint32_t f = 0; f < nf; f++) reps[f] = R[f];
+    if (brep) *brep = BR;
     return ASZ_OK;
 }

@@ -134,48 +134,47 @@ __device__ __forceinline__ LineMap line_map(uint32_t tpl_log2) {
 // axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
 // kProbe: every axis divides, as the diagnostics instantiation that the predictor-family probe runs
 // does (one out-of-line clone for all axes), and pred_out receives each target's prediction.
+// Targets of line `line` (k0, k1) handled by the sub-th of the line's 2^tpl_log2 threads.
 template <bool kProbe>
-__global__ void __launch_bounds__(256, 5)
-    round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
-                          const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
-                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out) {
-    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd), r0 = __dmul_rn(rinv, 0.5);
+__device__ __forceinline__ void compress_line(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *__restrict__ ent,
+                                              uint32_t tpl_log2, uint32_t sub, uint32_t line, const float *__restrict__ tval,
+                                              const float *__restrict__ in, float *__restrict__ rec, int32_t *__restrict__ qb,
+                                              uint32_t *err_word, float *__restrict__ pred_out, double ebd, double eb2,
+                                              double rinv, double r0, int32_t &lo, int32_t &hi) {
     const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
     const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
-    const uint32_t lines = (uint32_t)rg.tcount[0] * T1;
     const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
     const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
-    const LineMap m = line_map(tpl_log2);
     const int dir = rg.dir;
-    int32_t lo = INT32_MAX, hi = INT32_MIN;
-    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += gridDim.x * m.lines_per_cta) {
-        const uint32_t k0 = line / T1, k1 = line - k0 * T1;
-        const AxisEntry e0 = load_entry(e0t + k0), e1 = load_entry(e1t + k1);
-        const uint64_t line_pos = (uint64_t)e0.ii * n1n2 + (uint64_t)e1.ii * n2;
-        const uint32_t line_blk = e0.bb * nb1 + e1.bb;
-        const LineQB lq = line_qb(rg, e0, e1);
-        for (uint32_t k2 = m.sub; k2 < T2; k2 += 1u << tpl_log2) {
-            const AxisEntry e2 = load_entry(e2t + k2);
-            const uint64_t pos = line_pos + e2.ii;
-            const uint64_t qi = target_qb(rg, lq, e0, e1, e2);
-            if (qi >= rg.qb_total) {
-                atomicOr(err_word, 4u);
-                continue;
-            }
-            const uint32_t sc = dir == 0 ? e0.stencil : dir == 1 ? e1.stencil : e2.stencil;
-            const float t = sc == kStencilCubic ? tval[(uint64_t)line_blk * nb2 + e2.bb] : 0.0f;
-            const float pred = predict_case(rec, pos, rg.dist, sc, t);
-            const double pd = (double)pred;
-            const double diff = __dsub_rn(pd, (double)in[pos]);
-            const double q = dir == 0 && !kProbe ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
-            if (kProbe) pred_out[pos] = pred;
-            const int32_t v = (int32_t)lround_d(q);
-            qb[qi] = v;
-            rec[pos] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
-            lo = min(lo, v);
-            hi = max(hi, v);
+    const uint32_t k0 = line / T1, k1 = line - k0 * T1;
+    const AxisEntry e0 = load_entry(e0t + k0), e1 = load_entry(e1t + k1);
+    const uint64_t line_pos = (uint64_t)e0.ii * n1n2 + (uint64_t)e1.ii * n2;
+    const uint32_t line_blk = e0.bb * nb1 + e1.bb;
+    const LineQB lq = line_qb(rg, e0, e1);
+    for (uint32_t k2 = sub; k2 < T2; k2 += 1u << tpl_log2) {
+        const AxisEntry e2 = load_entry(e2t + k2);
+        const uint64_t pos = line_pos + e2.ii;
+        const uint64_t qi = target_qb(rg, lq, e0, e1, e2);
+        if (qi >= rg.qb_total) {
+            atomicOr(err_word, 4u);
+            continue;
         }
+        const uint32_t sc = dir == 0 ? e0.stencil : dir == 1 ? e1.stencil : e2.stencil;
+        const float t = sc == kStencilCubic ? tval[(uint64_t)line_blk * nb2 + e2.bb] : 0.0f;
+        const float pred = predict_case(rec, pos, rg.dist, sc, t);
+        const double pd = (double)pred;
+        const double diff = __dsub_rn(pd, (double)in[pos]);
+        const double q = dir == 0 && !kProbe ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+        if (kProbe) pred_out[pos] = pred;
+        const int32_t v = (int32_t)lround_d(q);
+        qb[qi] = v;
+        rec[pos] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
+        lo = min(lo, v);
+        hi = max(hi, v);
     }
+}
+
+__device__ __forceinline__ void reduce_range(int32_t lo, int32_t hi, int32_t *qb_range) {
     for (int o = 16; o > 0; o >>= 1) {
         lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
         hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
@@ -183,6 +182,60 @@ __global__ void __launch_bounds__(256, 5)
     if ((threadIdx.x & 31) == 0 && lo <= hi) {
         atomicMin(&qb_range[0], lo);
         atomicMax(&qb_range[1], hi);
+    }
+}
+
+// Compress round: quantise the residual and write the reconstruction in place.
+// compress.tpp:35-37 as emitted: axis 0 multiplies by the hoisted 0.5*(1/eb) (inlined loop),
+// axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
+// kProbe: every axis divides, as the diagnostics instantiation that the predictor-family probe runs
+// does (one out-of-line clone for all axes), and pred_out receives each target's prediction.
+template <bool kProbe>
+__global__ void __launch_bounds__(256, 5)
+    round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
+                          const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
+                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out) {
+    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd), r0 = __dmul_rn(rinv, 0.5);
+    const uint32_t lines = (uint32_t)rg.tcount[0] * (uint32_t)rg.tcount[1];
+    const LineMap m = line_map(tpl_log2);
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += gridDim.x * m.lines_per_cta)
+        compress_line<kProbe>(fg, rg, ent, tpl_log2, m.sub, line, tval, in, rec, qb, err_word, pred_out, ebd, eb2, rinv, r0, lo,
+                              hi);
+    reduce_range(lo, hi, qb_range);
+}
+
+// Batched form: one work queue over the (field, item) pairs of a round, an item being
+// kBatchChunks CTA-sized chunks of one field's target lines (256 >> tpl_log2 lines each).
+constexpr uint32_t kBatchChunks = 8;
+
+__global__ void __launch_bounds__(256, 5)
+    round_compress_batch_kernel(const BatchField *__restrict__ F, const uint64_t *__restrict__ ioff, uint32_t nf, uint32_t l,
+                                uint32_t *queue) {
+    __shared__ uint64_t item;
+    const uint64_t total = ioff[nf];
+    for (;;) {
+        if (threadIdx.x == 0) item = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint64_t it = item;
+        __syncthreads();
+        if (it >= total) break;
+        const uint32_t f = field_of(ioff, nf, it);
+        const BatchField &B = F[f];
+        const RoundGeom &rg = B.rounds[l];
+        const uint32_t tpl = B.tpl_log2[l];
+        const LineMap m = line_map(tpl);
+        const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd), r0 = __dmul_rn(rinv, 0.5);
+        const uint32_t lines = (uint32_t)rg.tcount[0] * (uint32_t)rg.tcount[1];
+        const uint64_t c0 = (it - ioff[f]) * kBatchChunks;
+        int32_t lo = INT32_MAX, hi = INT32_MIN;
+        for (uint32_t c = 0; c < kBatchChunks; c++) {
+            const uint64_t line = (c0 + c) * m.lines_per_cta + m.row;
+            if (line < lines)
+                compress_line<false>(B.fg, rg, B.ent, tpl, m.sub, (uint32_t)line, B.tval, B.in, B.rec, B.qb + B.qoff[l + 1],
+                                     &B.cnt->err, nullptr, ebd, eb2, rinv, r0, lo, hi);
+        }
+        reduce_range(lo, hi, B.qb_range + 2 * (l + 1));
     }
 }
 
@@ -306,6 +359,21 @@ cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, cons
     else
         round_compress_kernel<false><<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
                                                                          nullptr);
+    count_launch();
+    return cudaGetLastError();
+}
+
+uint32_t round_tpl_log2(uint64_t t2) { return tpl_log2_for(t2); }
+
+uint64_t round_batch_items(const RoundGeom &rg, uint32_t tpl_log2) {
+    const uint64_t lines = rg.tcount[0] * rg.tcount[1], per_cta = 256u >> tpl_log2;
+    const uint64_t chunks = (lines + per_cta - 1) / per_cta;
+    return rg.targets ? (chunks + kBatchChunks - 1) / kBatchChunks : 0;
+}
+
+cudaError_t launch_round_compress_batch(const BatchField *F, const uint64_t *ioff, uint32_t nf, uint32_t l, uint32_t *queue,
+                                        uint32_t grid, cudaStream_t st) {
+    round_compress_batch_kernel<<<grid ? grid : 148 * 5, 256, 0, st>>>(F, ioff, nf, l, queue);
     count_launch();
     return cudaGetLastError();
 }

@@ -234,24 +234,15 @@ __device__ __forceinline__ int class_of(uint64_t b, uint64_t nb) { return b == 0
 
 // One thread per block for round `l`. Writes the chosen t (float) per block, its code into
 // t_int[block * layer_num + l], and appends ambiguous decisions.
-__global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
-                               const float *__restrict__ rec, const float *__restrict__ orig,
-                               const float *__restrict__ log2arena, float R2, float t_default,
-                               uint8_t *scratch, uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap,
-                               float *__restrict__ tval, int64_t *__restrict__ t_int, uint32_t *__restrict__ fb_count,
-                               AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
-                               const uint32_t *__restrict__ overrides, uint32_t n_overrides,
-                               float *__restrict__ proxies, const uint32_t *__restrict__ list,
-                               const uint32_t *__restrict__ list_count, uint32_t *__restrict__ err_word) {
+// Serial selection of group g of one field and round by one thread, with its scratch slot.
+__device__ void v0_one(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *__restrict__ classes,
+                       const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
+                       float R2, float t_default, uint8_t *slot, uint32_t cap, uint32_t bcap, uint32_t tcap,
+                       float *__restrict__ tval, int64_t *__restrict__ t_int, uint32_t *fb_count, AmbiguousRecord *amb,
+                       uint32_t amb_cap, uint32_t *amb_count, const uint32_t *__restrict__ overrides, uint32_t n_overrides,
+                       float *__restrict__ proxies, uint32_t *err_word, uint64_t g) {
     const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-    // With a list, each thread settles the listed groups tid, tid+nthreads, ... in its own scratch
-    // slot; without one, thread g settles group g.
-    const uint64_t items = list ? *list_count : nblocks;
-    for (uint64_t it = tid; it < items; it += nthreads) {
-    const uint64_t g = list ? list[it] : it;
-    if (g >= nblocks) continue;
+    if (g >= nblocks) return;
     const uint64_t b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1],
                    b0 = g / (fg.block_num[1] * fg.block_num[2]);
     const uint64_t bb[3] = {b0, b1, b2};
@@ -286,12 +277,12 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
         box.neg_2_stat_eb = rg.neg_2_stat_eb;
         box.stat_eb = rg.stat_eb;
         box.n = ci.n;
-        Scratch s = carve(scratch + tid * scratch_stride, cap, bcap, tcap);
+        Scratch s = carve(slot, cap, bcap, tcap);
         FieldRef fr{rec, orig, fg.n[1] * fg.n[2], fg.n[2]};
         uint32_t m = ci.n == 0 ? 0 : build_abmap(box, fr, s);
         if (m == UINT32_MAX) {
             atomicOr(err_word, 1u);
-            continue;
+            return;
         }
         if (m == 0) {
             fb = true;
@@ -352,6 +343,43 @@ __global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const Cla
     if (fb) atomicAdd(fb_count, 1u);
     tval[g] = best_t;
     t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(best_t, (float)fg.t_precision));
+}
+
+__global__ void tsel_v0_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
+                               const float *__restrict__ rec, const float *__restrict__ orig,
+                               const float *__restrict__ log2arena, float R2, float t_default,
+                               uint8_t *scratch, uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap,
+                               float *__restrict__ tval, int64_t *__restrict__ t_int, uint32_t *__restrict__ fb_count,
+                               AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count,
+                               const uint32_t *__restrict__ overrides, uint32_t n_overrides,
+                               float *__restrict__ proxies, const uint32_t *__restrict__ list,
+                               const uint32_t *__restrict__ list_count, uint32_t *__restrict__ err_word) {
+    const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    // With a list, each thread settles the listed groups tid, tid+nthreads, ... in its own scratch
+    // slot; without one, thread g settles group g.
+    const uint64_t items = list ? *list_count : nblocks;
+    for (uint64_t it = tid; it < items; it += nthreads)
+        v0_one(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, scratch + tid * scratch_stride, cap, bcap, tcap, tval,
+               t_int, fb_count, amb, amb_cap, amb_count, overrides, n_overrides, proxies, err_word, list ? list[it] : it);
+}
+
+// Batched form over (field << 32 | group) entries of all fields of a batch.
+__global__ void tsel_v0_batch_kernel(const BatchField *__restrict__ F, uint32_t l, const float *__restrict__ log2arena,
+                                     float t_default, uint8_t *scratch, uint64_t scratch_stride, uint32_t cap, uint32_t bcap,
+                                     uint32_t tcap, const unsigned long long *__restrict__ list,
+                                     const uint32_t *__restrict__ list_count) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t items = *list_count;
+    for (uint64_t it = tid; it < items; it += nthreads) {
+        const unsigned long long e = list[it];
+        const BatchField &B = F[e >> 32];
+        const uint64_t nb = B.fg.block_num[0] * B.fg.block_num[1] * B.fg.block_num[2];
+        v0_one(B.fg, B.rounds[l], l, B.classes + 27 * l, B.rec, B.in, log2arena, B.R2, t_default, scratch + tid * scratch_stride,
+               cap, bcap, tcap, B.tval, B.tint, &B.cnt->fb, B.amb, B.amb_cap, &B.cnt->amb_count, nullptr, 0,
+               B.proxies ? B.proxies + nb * l * 10 : nullptr, &B.cnt->err, e & 0xffffffffull);
     }
 }
 
@@ -394,6 +422,15 @@ cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
                                                                   scratch, scratch_stride, cap, bcap, tcap, tval, t_int,
                                                                   fb_count, amb, amb_cap, amb_count, overrides, n_overrides,
                                                                   proxies, list, list_count, err);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tsel_v0_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default, uint8_t *scratch,
+                                 uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap,
+                                 const unsigned long long *list, const uint32_t *list_count, uint64_t slots, cudaStream_t st) {
+    tsel_v0_batch_kernel<<<(unsigned)((slots + 63) / 64), 64, 0, st>>>(F, l, log2arena, t_default, scratch, scratch_stride, cap,
+                                                                        bcap, tcap, list, list_count);
     count_launch();
     return cudaGetLastError();
 }

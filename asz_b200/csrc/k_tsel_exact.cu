@@ -408,6 +408,113 @@ __device__ Band psnr_band(float x) {
 
 // Exact t selection for the listed groups of round l; groups that do not fit the arena go to
 // `spill` for the serial kernel.
+// Exact replay of group g of one field and round (compress.tpp:91-144 in the maps' order). The
+// caller's spill(g) receives a group too large for shared memory (thread 0).
+template <class Spill>
+__device__ void exact_one(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *__restrict__ classes,
+                          const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
+                          float R2, float t_default, float *__restrict__ tval, int64_t *__restrict__ t_int, uint32_t *fb_count,
+                          AmbiguousRecord *amb, uint32_t amb_cap, uint32_t *amb_count, const uint32_t *__restrict__ overrides,
+                          uint32_t n_overrides, float *__restrict__ proxies, uint64_t g, uint8_t *smem, uint32_t cap,
+                          float *h1v, float *xv, uint32_t &m_sh, const Spill &spill) {
+    const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
+    const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+    if (g >= nblocks) return;
+    const uint64_t b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1],
+                   b0 = g / (fg.block_num[1] * fg.block_num[2]);
+    const uint64_t bb[3] = {b0, b1, b2};
+    const int cls = (class_of(b0, fg.block_num[0]) * 3 + class_of(b1, fg.block_num[1])) * 3 + class_of(b2, fg.block_num[2]);
+    const ClassInfo ci = classes[cls];
+    const int d = rg.dir;
+    ExactGroup eg;
+    for (int a = 0; a < 3; a++) {
+        uint64_t lo = fg.origin[a] + bb[a] * fg.block_shape[a];
+        uint64_t hi = min(fg.origin[a] + (bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
+        if (a != d && lo != 0) lo += rg.stride[a];
+        if (a == d) {
+            lo += 3 * rg.stride[a] / 2;
+            hi -= 3 * rg.stride[a] / 2;
+        }
+        eg.box.lo[a] = lo;
+        eg.box.hi[a] = hi;
+        eg.box.step[a] = rg.stride[a] * ci.ss;
+    }
+    eg.box.dist = rg.dist;
+    eg.box.neg_2_stat_eb = rg.neg_2_stat_eb;
+    eg.box.stat_eb = rg.stat_eb;
+    eg.n = ci.n;
+    ProxyEval ev[5];
+    for (int c = 0; c < 5; c++) ev[c] = ProxyEval{cand[c], rg.eb};
+    if (threadIdx.x == 0) m_sh = 0;
+    __syncthreads();
+    bool ok = exact_eval(eg, rec, orig, fg.n[1] * fg.n[2], fg.n[2], ev, 5, R2, log2arena + ci.log2_off, smem, cap, h1v,
+                         xv, &m_sh);
+    __syncthreads();
+    if (!ok) {
+        if (threadIdx.x == 0) spill(g);
+        __syncthreads();
+        return;
+    }
+    if (threadIdx.x == 0) {
+        float best_t = t_default;
+        bool fb = m_sh == 0;
+        bool forced = false;
+        for (uint32_t i = 0; i < n_overrides; i++)
+            if (overrides[3 * i] == (uint32_t)g && overrides[3 * i + 1] == l) {
+                forced = true;
+                best_t = __uint_as_float(overrides[3 * i + 2]);
+            }
+        if (!fb && !forced) {
+            if (proxies)
+                for (int c = 0; c < 5; c++) {
+                    proxies[g * 10 + c] = h1v[c];
+                    proxies[g * 10 + 5 + c] = xv[c];
+                }
+            int best = 1;
+            bool ambiguous = false;
+            for (int c = 0; c < 5; c++) {
+                if (cand[c] == cand[best]) continue;
+                float d_h1 = __fsub_rn(h1v[best], h1v[c]);
+                bool accept;
+                if (__float_as_uint(xv[c]) == __float_as_uint(xv[best]) && isfinite(xv[c]) && xv[c] > 0.0f) {
+                    accept = __fmaf_rn(d_h1, rg.slope, 0.0f) > 0.0f;
+                } else {
+                    Band pc = psnr_band(xv[c]), pb = psnr_band(xv[best]);
+                    float s_mid = __fmaf_rn(d_h1, rg.slope, __fsub_rn(pc.mid, pb.mid));
+                    float s_lo = __fmaf_rn(d_h1, rg.slope, __fsub_rn(pc.lo, pb.hi));
+                    float s_hi = __fmaf_rn(d_h1, rg.slope, __fsub_rn(pc.hi, pb.lo));
+                    if (!((s_lo > 0.0f) || !(s_hi > 0.0f))) ambiguous = true;
+                    accept = s_mid > 0.0f;
+                }
+                if (accept) best = c;
+            }
+            best_t = cand[best];
+            if (ambiguous) {
+                uint32_t k = atomicAdd(amb_count, 1u);
+                if (k < amb_cap) {
+                    AmbiguousRecord &r = amb[k];
+                    r.block = (uint32_t)g;
+                    r.round = l;
+                    r.provisional = (int32_t)lround_f(__fmul_rn(best_t, (float)fg.t_precision));
+                    for (int c = 0; c < 5; c++) {
+                        r.h1[c] = h1v[c];
+                        r.x[c] = xv[c];
+                    }
+                }
+            }
+        }
+        if (fb) atomicAdd(fb_count, 1u);
+        tval[g] = best_t;
+        t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(best_t, (float)fg.t_precision));
+    }
+    __syncthreads();
+}
+
+struct ListSpill {
+    uint32_t *list, *count;
+    __device__ void operator()(uint64_t g) const { list[atomicAdd(count, 1u)] = (uint32_t)g; }
+};
+
 __global__ void __launch_bounds__(kThreads)
     tsel_exact_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
                       const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
@@ -417,106 +524,44 @@ __global__ void __launch_bounds__(kThreads)
                       const uint32_t *__restrict__ list, const uint32_t *__restrict__ list_count, uint32_t *spill,
                       uint32_t *spill_count, uint32_t smem_bytes, uint32_t cap) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     const uint32_t items = *list_count;
-    const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+    __shared__ float h1v[kMaxEvals], xv[kMaxEvals];
+    __shared__ uint32_t m_sh;
+    const ListSpill sp{spill, spill_count};
+    for (uint32_t it = blockIdx.x; it < items; it += gridDim.x)
+        exact_one(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int, fb_count, amb, amb_cap, amb_count,
+                  overrides, n_overrides, proxies, list[it], smem, cap, h1v, xv, m_sh, sp);
+}
+
+// Batched form: the (field << 32 | group) entries that the batched fast path handed off, for all
+// fields of a batch at once; spills go to one list of entries of the same form.
+struct PairSpill {
+    unsigned long long *list;
+    uint32_t *count;
+    uint32_t f;
+    __device__ void operator()(uint64_t g) const { list[atomicAdd(count, 1u)] = ((unsigned long long)f << 32) | g; }
+};
+
+__global__ void __launch_bounds__(kThreads)
+    tsel_exact_batch_kernel(const BatchField *__restrict__ F, uint32_t l, const float *__restrict__ log2arena,
+                            float t_default, const unsigned long long *__restrict__ list, const uint32_t *__restrict__ list_count,
+                            unsigned long long *spill, uint32_t *spill_count, uint32_t cap) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint32_t items = *list_count;
     __shared__ float h1v[kMaxEvals], xv[kMaxEvals];
     __shared__ uint32_t m_sh;
     for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
-        const uint64_t g = list[it];
-        if (g >= nblocks) continue;
-        const uint64_t b2 = g % fg.block_num[2], b1 = (g / fg.block_num[2]) % fg.block_num[1],
-                       b0 = g / (fg.block_num[1] * fg.block_num[2]);
-        const uint64_t bb[3] = {b0, b1, b2};
-        const int cls = (class_of(b0, fg.block_num[0]) * 3 + class_of(b1, fg.block_num[1])) * 3 + class_of(b2, fg.block_num[2]);
-        const ClassInfo ci = classes[cls];
-        const int d = rg.dir;
-        ExactGroup eg;
-        for (int a = 0; a < 3; a++) {
-            uint64_t lo = fg.origin[a] + bb[a] * fg.block_shape[a];
-            uint64_t hi = min(fg.origin[a] + (bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
-            if (a != d && lo != 0) lo += rg.stride[a];
-            if (a == d) {
-                lo += 3 * rg.stride[a] / 2;
-                hi -= 3 * rg.stride[a] / 2;
-            }
-            eg.box.lo[a] = lo;
-            eg.box.hi[a] = hi;
-            eg.box.step[a] = rg.stride[a] * ci.ss;
-        }
-        eg.box.dist = rg.dist;
-        eg.box.neg_2_stat_eb = rg.neg_2_stat_eb;
-        eg.box.stat_eb = rg.stat_eb;
-        eg.n = ci.n;
-        ProxyEval ev[5];
-        for (int c = 0; c < 5; c++) ev[c] = ProxyEval{cand[c], rg.eb};
-        if (threadIdx.x == 0) m_sh = 0;
-        __syncthreads();
-        bool ok = exact_eval(eg, rec, orig, fg.n[1] * fg.n[2], fg.n[2], ev, 5, R2, log2arena + ci.log2_off, smem, cap, h1v,
-                             xv, &m_sh);
-        __syncthreads();
-        if (!ok) {
-            if (threadIdx.x == 0) spill[atomicAdd(spill_count, 1u)] = (uint32_t)g;
-            __syncthreads();
-            continue;
-        }
-        if (threadIdx.x == 0) {
-            float best_t = t_default;
-            bool fb = m_sh == 0;
-            bool forced = false;
-            for (uint32_t i = 0; i < n_overrides; i++)
-                if (overrides[3 * i] == (uint32_t)g && overrides[3 * i + 1] == l) {
-                    forced = true;
-                    best_t = __uint_as_float(overrides[3 * i + 2]);
-                }
-            if (!fb && !forced) {
-                if (proxies)
-                    for (int c = 0; c < 5; c++) {
-                        proxies[g * 10 + c] = h1v[c];
-                        proxies[g * 10 + 5 + c] = xv[c];
-                    }
-                int best = 1;
-                bool ambiguous = false;
-                for (int c = 0; c < 5; c++) {
-                    if (cand[c] == cand[best]) continue;
-                    float d_h1 = __fsub_rn(h1v[best], h1v[c]);
-                    bool accept;
-                    if (__float_as_uint(xv[c]) == __float_as_uint(xv[best]) && isfinite(xv[c]) && xv[c] > 0.0f) {
-                        accept = __fmaf_rn(d_h1, rg.slope, 0.0f) > 0.0f;
-                    } else {
-                        Band pc = psnr_band(xv[c]), pb = psnr_band(xv[best]);
-                        float s_mid = __fmaf_rn(d_h1, rg.slope, __fsub_rn(pc.mid, pb.mid));
-                        float s_lo = __fmaf_rn(d_h1, rg.slope, __fsub_rn(pc.lo, pb.hi));
-                        float s_hi = __fmaf_rn(d_h1, rg.slope, __fsub_rn(pc.hi, pb.lo));
-                        if (!((s_lo > 0.0f) || !(s_hi > 0.0f))) ambiguous = true;
-                        accept = s_mid > 0.0f;
-                    }
-                    if (accept) best = c;
-                }
-                best_t = cand[best];
-                if (ambiguous) {
-                    uint32_t k = atomicAdd(amb_count, 1u);
-                    if (k < amb_cap) {
-                        AmbiguousRecord &r = amb[k];
-                        r.block = (uint32_t)g;
-                        r.round = l;
-                        r.provisional = (int32_t)lround_f(__fmul_rn(best_t, (float)fg.t_precision));
-                        for (int c = 0; c < 5; c++) {
-                            r.h1[c] = h1v[c];
-                            r.x[c] = xv[c];
-                        }
-                    }
-                }
-            }
-            if (fb) atomicAdd(fb_count, 1u);
-            tval[g] = best_t;
-            t_int[g * fg.layer_num + l] = lround_f(__fmul_rn(best_t, (float)fg.t_precision));
-        }
-        __syncthreads();
+        const unsigned long long e = list[it];
+        const uint32_t f = (uint32_t)(e >> 32);
+        const BatchField &B = F[f];
+        const uint64_t nb = B.fg.block_num[0] * B.fg.block_num[1] * B.fg.block_num[2];
+        const PairSpill sp{spill, spill_count, f};
+        exact_one(B.fg, B.rounds[l], l, B.classes + 27 * l, B.rec, B.in, log2arena, B.R2, t_default, B.tval, B.tint, &B.cnt->fb,
+                  B.amb, B.amb_cap, &B.cnt->amb_count, nullptr, 0, B.proxies ? B.proxies + nb * l * 10 : nullptr,
+                  e & 0xffffffffull, smem, cap, h1v, xv, m_sh, sp);
     }
 }
 
-// Default-slope proxies: the three axis maps, each evaluated for every (t, eb). One CTA per map.
 __global__ void __launch_bounds__(kThreads)
     slope_exact_kernel(const SampleBox *__restrict__ boxes, const ProxyEval *__restrict__ evals, uint32_t n_evals,
                        const float *__restrict__ orig, uint64_t n1n2, uint64_t n2, const float *__restrict__ log2arena,
@@ -556,6 +601,17 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
     tsel_exact_kernel<<<grid, kThreads, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int,
                                                      fb_count, amb, amb_cap, amb_count, overrides, n_overrides, proxies, list,
                                                      list_count, spill, spill_count, smem, cap);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tsel_exact_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default,
+                                    const unsigned long long *list, const uint32_t *list_count, unsigned long long *spill,
+                                    uint32_t *spill_count, uint32_t cap, unsigned grid, cudaStream_t st) {
+    uint32_t smem = exact_smem_bytes(cap);
+    cudaError_t e = cudaFuncSetAttribute(tsel_exact_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    tsel_exact_batch_kernel<<<grid, kThreads, smem, st>>>(F, l, log2arena, t_default, list, list_count, spill, spill_count, cap);
     count_launch();
     return cudaGetLastError();
 }

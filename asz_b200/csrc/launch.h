@@ -63,6 +63,24 @@ struct PlanCand {
 cudaError_t launch_range(const float *x, uint64_t n, int32_t *out, unsigned long long *nonfinite, cudaStream_t st);
 cudaError_t launch_zero_first_last(const float *x, uint64_t n, unsigned long long *first, unsigned long long *last,
                                    cudaStream_t st);
+// Batches (host/batch.cpp): one launch per round for every field of a batch. The fast selection and
+// the round kernel take work items from a queue (a device counter, zero before the launch); items
+// map to fields through an exclusive prefix of per-field item counts (nf + 1 entries). Groups the
+// fast path hands off, and groups the exact path spills, are (field << 32 | group) entries.
+cudaError_t launch_tsel_fast_batch(const BatchField *F, const uint64_t *goff, uint32_t nf, uint32_t l, const float *log2arena,
+                                   float t_default, uint32_t *queue, unsigned long long *handoff_list, uint32_t *handoff_count,
+                                   uint32_t grid, cudaStream_t st);
+cudaError_t launch_tsel_exact_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default,
+                                    const unsigned long long *list, const uint32_t *list_count, unsigned long long *spill,
+                                    uint32_t *spill_count, uint32_t cap, unsigned grid, cudaStream_t st);
+cudaError_t launch_tsel_v0_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default, uint8_t *scratch,
+                                 uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap,
+                                 const unsigned long long *list, const uint32_t *list_count, uint64_t slots, cudaStream_t st);
+uint32_t round_tpl_log2(uint64_t t2);
+uint64_t round_batch_items(const RoundGeom &rg, uint32_t tpl_log2);
+cudaError_t launch_round_compress_batch(const BatchField *F, const uint64_t *ioff, uint32_t nf, uint32_t l, uint32_t *queue,
+                                        uint32_t grid, cudaStream_t st);
+
 // Open-loop AB samples of every (block, round) group for the gradient tuner (k_grad.cu).
 cudaError_t launch_grad_gather(const FieldGeom &fg, const RoundGeom *rounds, const ClassInfo *classes, const float *x,
                                const uint32_t *off, uint64_t groups, float *A, float *B, uint32_t *err, cudaStream_t st);

@@ -190,6 +190,32 @@ int asz_grad_tune(const float *A, const float *B, const uint32_t *offsets, const
                   float t_min, float t_max, int32_t t_precision, uint32_t steps, float step0, uint32_t step_cap,
                   uint32_t team, int64_t *t_codes, float *t_relaxed, uint32_t *stats, void *cuda_stream);
 
+/* ---- Batches: many fields, one plan, one error bound (no counterpart in the reference, which
+ * compresses one field per process). Each field gets the bytes asz_compress gives it: its own
+ * range, default slope and geometry; the rounds of all fields run together, per round one
+ * launch of each selection kernel and of the prediction kernel, each over a work queue of every
+ * field's (block) groups or target lines, captured once per batch layout as a CUDA graph. The
+ * persistent grids' CTAs per SM and the threads per target line come from an autotuner that times
+ * the candidates on the first batch of a shape and reuses the choice. A field with a coefficient
+ * decision that needs the host's log10f replay takes the single-field path (fields_fallback).
+ * zstd runs on host threads as each field's stream is ready. */
+typedef struct asz_batch_report {
+    double total_s, h2d_s, prep_s, tune_s, rounds_s, encode_s, zstd_s; /* zstd_s: summed over threads */
+    double rounds_ms;            /* device time of the captured round sequence */
+    uint64_t input_bytes, output_bytes, kernel_launches;
+    uint32_t tuned_now;          /* the autotuner ran in this call */
+    uint32_t graph_reused;       /* the captured sequence of a previous call was replayed */
+    uint32_t fields_fallback;    /* fields that took the single-field path */
+    uint32_t fast_ctas_per_sm, round_ctas_per_sm, tpl_shift;  /* launch shapes in use */
+} asz_batch_report;
+
+/* in: count field pointers (host, or device when in_on_device); dims: 3 per field; plan required;
+ * the family must be fixed. out[f] / out_len[f] receive each field's .asz (asz_free each);
+ * reps (count entries) and brep are optional. */
+int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device, const uint64_t *dims,
+                       float rel_eb, const asz_params *p, const char *plan, uint8_t **out, size_t *out_len,
+                       asz_report *reps, asz_batch_report *brep);
+
 /* Decompress .asz bytes into `out` (prod(dims) floats; host pointer, or device pointer when
  * out_on_device is nonzero). */
 int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const uint64_t dims[3], float rel_eb,
