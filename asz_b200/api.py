@@ -116,6 +116,9 @@ def lib():
     L.asz_compress_batch.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_float,
                                      C.POINTER(Params), C.c_char_p, C.c_void_p, C.POINTER(C.c_size_t),
                                      C.POINTER(Report), C.POINTER(BatchReport)]
+    L.asz_compress_batch_with_t.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.POINTER(C.c_uint64),
+                                            C.c_float, C.POINTER(Params), C.c_char_p, C.c_void_p, C.POINTER(C.c_uint64),
+                                            C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(Report), C.POINTER(BatchReport)]
     L.asz_decompress.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint64), C.c_float,
                                  C.POINTER(Params), C.c_void_p, C.c_int, C.POINTER(Report)]
     L.asz_free.argtypes = [C.c_void_p]
@@ -291,9 +294,11 @@ class Context:
             self._L.asz_free(out)
         return blob, rep
 
-    def compress_batch(self, fields, rel_eb: float, plan: str, family: str = "cubic", params: Params | None = None):
+    def compress_batch(self, fields, rel_eb: float, plan: str, family: str = "cubic", params: Params | None = None,
+                       t_tables=None):
         """Compress several fields (all NumPy arrays, or all contiguous float32 CUDA tensors on one
-        stream) with one plan; returns (list of asz bytes, list of Report, BatchReport)."""
+        stream) with one plan; returns (list of asz bytes, list of Report, BatchReport). t_tables:
+        optional per-field block-major t codes (NumPy or torch int64) replacing the selection."""
         p = params if params is not None else default_params()
         p.predictor_family = _family_code(family)
         n = len(fields)
@@ -320,8 +325,18 @@ class Context:
         if on_dev:
             self._use_torch_stream(fields[0])
         try:
-            rc = self._L.asz_compress_batch(self._c, n, ptrs, 1 if on_dev else 0, dims, C.c_float(rel_eb), C.byref(p),
-                                            plan.encode(), outs, lens, reps, C.byref(br))
+            if t_tables is None:
+                rc = self._L.asz_compress_batch(self._c, n, ptrs, 1 if on_dev else 0, dims, C.c_float(rel_eb), C.byref(p),
+                                                plan.encode(), outs, lens, reps, C.byref(br))
+            else:
+                tabs = [np.ascontiguousarray(t.detach().cpu().numpy() if hasattr(t, "detach") else t, dtype=np.int64)
+                        for t in t_tables]
+                keep.extend(tabs)
+                tptr = (C.c_void_p * n)(*[t.ctypes.data for t in tabs])
+                tlen = (C.c_uint64 * n)(*[t.size for t in tabs])
+                rc = self._L.asz_compress_batch_with_t(self._c, n, ptrs, 1 if on_dev else 0, dims, C.c_float(rel_eb),
+                                                       C.byref(p), plan.encode(), tptr, tlen, outs, lens, reps,
+                                                       C.byref(br))
         finally:
             if on_dev:
                 self._L.asz_set_stream(self._c, None)

@@ -87,6 +87,16 @@ struct FieldGeom {
     int32_t t_precision;
 };
 
+// The pivot lattice (compress.tpp:162-175) and its quantisation step.
+struct PivotGeom {
+    uint64_t cnt[3];      // pivots per axis
+    uint64_t stride[3];
+    uint64_t origin[3];   // first pivot (the frame origin)
+    uint64_t n1n2, n2;
+    double rp;            // 0.5 / (double)pivot_eb
+    double peb2;          // 2 * (double)pivot_eb
+};
+
 // ---- Batches: several fields compressed with the same plan, one launch per round for all. ----
 
 struct AmbiguousRecord;
@@ -101,6 +111,7 @@ struct BatchCounters {
 // One field of a batch, as the batched kernels see it (device copy).
 struct BatchField {
     FieldGeom fg;
+    PivotGeom pg;
     const RoundGeom *rounds;        // layer_num rounds
     const AxisEntry *ent;           // per-axis target tables of all rounds
     const ClassInfo *classes;       // 27 per round

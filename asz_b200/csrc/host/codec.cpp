@@ -158,7 +158,7 @@ struct asz_ctx {
     // Batches (asz_compress_batch): per-field slices of these arenas, the captured round sequence
     // of the last batch, and the launch shapes the autotuner chose per batch shape.
     DevBuf b_in, b_rec, b_qb, b_tval, b_tint, b_ent, b_cls, b_rounds, b_qoff, b_range, b_range0, b_prox, b_amb, b_cnt,
-        b_fields, b_goff, b_ioff, b_queue, b_hand, b_spill;
+        b_fields, b_goff, b_poff, b_ioff, b_queue, b_hand, b_spill;
     std::vector<uint64_t> batch_graph_key;
     cudaGraphExec_t batch_graph = nullptr;
     std::map<std::vector<uint64_t>, std::array<uint32_t, 3>> batch_tuned;
@@ -644,7 +644,7 @@ void asz_destroy(asz_ctx *c) {
                       &c->plan_pay, &c->probe_in, &c->probe_pred, &c->rounds_dev, &c->lines_bail,
                       &c->lines_resume, &c->b_in, &c->b_rec, &c->b_qb, &c->b_tval, &c->b_tint, &c->b_ent, &c->b_cls,
                       &c->b_rounds, &c->b_qoff, &c->b_range, &c->b_range0, &c->b_prox, &c->b_amb, &c->b_cnt, &c->b_fields,
-                      &c->b_goff, &c->b_ioff, &c->b_queue, &c->b_hand, &c->b_spill})
+                      &c->b_goff, &c->b_poff, &c->b_ioff, &c->b_queue, &c->b_hand, &c->b_spill})
         b->release();
     c->pre_zstd.release();
     c->batch_pre[0].release();
@@ -2916,9 +2916,10 @@ using BatchShape = std::array<uint32_t, 3>;
 
 }  // namespace
 
-extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device,
-                                  const uint64_t *dims, float rel_eb, const asz_params *pp, const char *plan_text,
-                                  uint8_t **out, size_t *out_len, asz_report *reps, asz_batch_report *brep) {
+static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device, const uint64_t *dims,
+                               float rel_eb, const asz_params *pp, const char *plan_text, const int64_t *const *t_tables,
+                               const uint64_t *t_lens, uint8_t **out, size_t *out_len, asz_report *reps,
+                               asz_batch_report *brep) {
     if (!ctx) return ASZ_E_ARG;
     auto t_start = clk::now();
     const uint64_t launches0 = launch_counter();
@@ -2997,6 +2998,8 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
             acc += b.qb_len[s2];
         }
         if (acc != b.N) return fail(ctx, ASZ_E_DATA, tag + "total_qb_num!=data.size()");
+        if (t_tables && t_lens[f] != b.G.nblocks * L)
+            return fail(ctx, ASZ_E_ARG, tag + "t table length does not match the plan's blocks and rounds");
         for (u64 l = 0; l < L; l++) {
             for (auto &ci : b.G.classes[l])
                 if (ci.n) ci.log2_off = log2_table(ctx, ci.n);
@@ -3030,6 +3033,7 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
     CK(ctx->b_cnt.reserve((u64)nf * sizeof(BatchCounters)));
     CK(ctx->b_fields.reserve((u64)nf * sizeof(BatchField)));
     CK(ctx->b_goff.reserve((u64)(nf + 1) * sizeof(u64)));
+    CK(ctx->b_poff.reserve((u64)(nf + 1) * sizeof(u64)));
     CK(ctx->b_ioff.reserve((u64)L * (nf + 1) * sizeof(u64)));
     CK(ctx->b_queue.reserve((u64)L * 4 * sizeof(uint32_t)));
     CK(ctx->b_hand.reserve(std::max<u64>(nb_total, 1) * sizeof(unsigned long long)));
@@ -3039,6 +3043,7 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
     scratch_dims(capmax, bcap, tcap, sstride);
     const u64 slots = std::min<u64>(nb_total, 2048);
     CK(ctx->scratch.reserve(std::max<u64>(slots, 1) * sstride));
+    u64 pivots_total = 0;
     {
         std::vector<ClassInfo> cls;
         std::vector<RoundGeom> rounds;
@@ -3060,10 +3065,20 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
         CK(cudaMemcpyAsync(ctx->b_rounds.p, rounds.data(), rounds.size() * sizeof(RoundGeom), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->b_qoff.p, qoff.data(), qoff.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->b_range0.p, range0.data(), range0.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-        std::vector<u64> goff(nf + 1, 0);
-        for (uint32_t f = 0; f < nf; f++) goff[f + 1] = goff[f] + B[f].G.nblocks;
+        std::vector<u64> goff(nf + 1, 0), poff(nf + 1, 0);
+        for (uint32_t f = 0; f < nf; f++) {
+            goff[f + 1] = goff[f] + B[f].G.nblocks;
+            poff[f + 1] = poff[f] + B[f].G.pivots;
+        }
+        pivots_total = poff[nf];
         CK(cudaMemcpyAsync(ctx->b_goff.p, goff.data(), goff.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->b_poff.p, poff.data(), poff.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
     }
+    if (t_tables)
+        for (uint32_t f = 0; f < nf; f++)
+            CK(cudaMemcpyAsync(ctx->b_tint.as<int64_t>() + B[f].o_tint, t_tables[f], t_lens[f] * sizeof(int64_t),
+                               cudaMemcpyHostToDevice, st));
     // Field table and per-round work-item offsets for a launch shape (threads-per-line shift).
     auto upload_shape = [&](uint32_t tpl_shift) -> int {
         std::vector<BatchField> F(nf);
@@ -3073,6 +3088,7 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
             BatchField &x = F[f];
             std::memset(&x, 0, sizeof(x));
             x.fg = b.G.fg;
+            x.pg = b.G.pg;
             x.rounds = ctx->b_rounds.as<RoundGeom>() + (u64)f * L;
             x.ent = ctx->b_ent.as<AxisEntry>() + b.o_ent;
             x.classes = ctx->b_cls.as<ClassInfo>() + (u64)f * 27 * L;
@@ -3111,11 +3127,15 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
                            st));
         CK(cudaMemsetAsync(ctx->b_cnt.p, 0, (u64)nf * sizeof(BatchCounters), st));
         CK(cudaMemsetAsync(ctx->b_queue.p, 0, (u64)L * 4 * sizeof(uint32_t), st));
-        for (uint32_t f = 0; f < nf; f++)
-            CK(launch_pivot_compress(B[f].G.pg, B[f].d_in, ctx->b_rec.as<float>() + B[f].o_rec,
-                                     ctx->b_qb.as<int32_t>() + B[f].o_qb, ctx->b_range.as<int32_t>() + (u64)f * 2 * (L + 1), st));
+        CK(launch_pivot_compress_batch(dF, ctx->b_poff.as<u64>(), nf, pivots_total, st));
         for (u64 l = 0; l < L; l++) {
             uint32_t *q = d_queue + 4 * l;
+            if (t_tables) {
+                // The caller's t codes replace the coefficient selection.
+                CK(launch_tval_from_codes_batch(dF, d_goff, nf, nb_total, (uint32_t)l, st));
+                CK(launch_round_compress_batch(dF, d_ioff + l * (nf + 1), nf, (uint32_t)l, q + 1, 148 * sh[1], st));
+                continue;
+            }
             CK(launch_tsel_fast_batch(dF, d_goff, nf, (uint32_t)l, ctx->log2arena.as<float>(), t_default, q, d_hand, q + 2,
                                       148 * sh[0], st));
             CK(launch_tsel_exact_batch(dF, (uint32_t)l, ctx->log2arena.as<float>(), t_default, d_hand, q + 2, d_spill, q + 3,
@@ -3128,7 +3148,7 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
     };
     BR.prep_s = secs(t_prep, clk::now());
     // ---- Launch shapes: measured once per batch shape (the autotuner), then reused.
-    std::vector<uint64_t> shape_key{nf, L, (uint64_t)quintic, p.block_pivot_ratio};
+    std::vector<uint64_t> shape_key{nf, L, (uint64_t)quintic, p.block_pivot_ratio, (uint64_t)(t_tables != nullptr)};
     for (uint32_t f = 0; f < nf; f++) shape_key.insert(shape_key.end(), B[f].dims, B[f].dims + 3);
     for (u64 l = 0; l < L; l++) shape_key.push_back((uint64_t)plan.dir[l] * 3 + plan.order[l]);
     BatchShape best{8, 5, 0};
@@ -3178,7 +3198,8 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
     for (uint32_t f = 0; f < nf; f++) graph_key.push_back((uint64_t)(uintptr_t)B[f].d_in);
     for (DevBuf *d : {&ctx->b_rec, &ctx->b_qb, &ctx->b_tval, &ctx->b_tint, &ctx->b_ent, &ctx->b_cls, &ctx->b_rounds,
                       &ctx->b_qoff, &ctx->b_range, &ctx->b_range0, &ctx->b_prox, &ctx->b_amb, &ctx->b_cnt, &ctx->b_fields,
-                      &ctx->b_goff, &ctx->b_ioff, &ctx->b_queue, &ctx->b_hand, &ctx->b_spill, &ctx->scratch, &ctx->log2arena})
+                      &ctx->b_goff, &ctx->b_poff, &ctx->b_ioff, &ctx->b_queue, &ctx->b_hand, &ctx->b_spill, &ctx->scratch,
+                      &ctx->log2arena})
         graph_key.push_back((uint64_t)(uintptr_t)d->p);
     graph_key.push_back((uint64_t)(uintptr_t)st);
     auto t_rounds = clk::now();
@@ -3274,7 +3295,8 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
             const BatchItem &b = B[f];
             ea.push_back(EncodeArgs{&b.G, &b.qb_off, &b.qb_len, ctx->b_qb.as<int32_t>() + b.o_qb,
                                     ctx->b_tint.as<int64_t>() + b.o_tint, ctx->b_range.as<int32_t>() + (u64)f * 2 * (L + 1),
-                                    b.mn, b.mx, quintic, &plan, &p, nullptr, 0, b.N});
+                                    b.mn, b.mx, quintic, &plan, &p, t_tables ? t_tables[f] : nullptr,
+                                    t_tables ? t_lens[f] : 0, b.N});
             rs.push_back(&R[f]);
         }
         std::vector<std::pair<u64, u64>> span;
@@ -3318,7 +3340,8 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
             BR.fields_fallback++;
             uint8_t *o1 = nullptr;
             size_t l1 = 0;
-            frc = compress_entry(ctx, b.d_in, 1, b.dims, rel_eb, &p, plan_text, nullptr, 0, &o1, &l1, &r);
+            frc = compress_entry(ctx, b.d_in, 1, b.dims, rel_eb, &p, plan_text, t_tables ? t_tables[f] : nullptr,
+                                 t_tables ? t_lens[f] : 0, &o1, &l1, &r);
             out[f] = o1;
             out_len[f] = l1;
             continue;
@@ -3378,4 +3401,34 @@ extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *con
         for (uint32_t f = 0; f < nf; f++) reps[f] = R[f];
     if (brep) *brep = BR;
     return ASZ_OK;
+}
+
+extern "C" int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device,
+                                  const uint64_t *dims, float rel_eb, const asz_params *pp, const char *plan_text,
+                                  uint8_t **out, size_t *out_len, asz_report *reps, asz_batch_report *brep) {
+    return compress_batch_impl(ctx, count, in, in_on_device, dims, rel_eb, pp, plan_text, nullptr, nullptr, out, out_len, reps,
+                               brep);
+}
+
+extern "C" int asz_compress_batch_with_t(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device,
+                                         const uint64_t *dims, float rel_eb, const asz_params *pp, const char *plan_text,
+                                         const int64_t *const *t_tables, const uint64_t *t_lens, uint8_t **out,
+                                         size_t *out_len, asz_report *reps, asz_batch_report *brep) {
+    if (!ctx) return ASZ_E_ARG;
+    ctx->err.clear();
+    if (!t_tables || !t_lens) return fail(ctx, ASZ_E_ARG, "null t tables");
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    const int64_t lo = (int64_t)std::llround((double)p.t_min * p.t_precision);
+    const int64_t hi = (int64_t)std::llround((double)p.t_max * p.t_precision);
+    for (uint32_t f = 0; f < count; f++) {
+        if (!t_tables[f]) return fail(ctx, ASZ_E_ARG, "field " + std::to_string(f) + ": null t table");
+        for (uint64_t i = 0; i < t_lens[f]; i++)
+            if (t_tables[f][i] < lo || t_tables[f][i] > hi)
+                return fail(ctx, ASZ_E_ARG, "field " + std::to_string(f) + ": t code outside [t_min, t_max] at index " +
+                                                std::to_string(i));
+    }
+    return compress_batch_impl(ctx, count, in, in_on_device, dims, rel_eb, &p, plan_text, t_tables, t_lens, out, out_len, reps,
+                               brep);
 }

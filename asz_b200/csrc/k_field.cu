@@ -104,6 +104,44 @@ __global__ void pivot_compress_kernel(PivotGeom pg, const float *__restrict__ in
     }
 }
 
+// Batched form: the pivots of every field of a batch, one item per pivot; a field's parameters
+// come from its record, so a captured launch serves any data of the same shapes.
+__global__ void pivot_compress_batch_kernel(const BatchField *__restrict__ F, const uint64_t *__restrict__ poff, uint32_t nf) {
+    const uint64_t total = poff[nf];
+    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < total; gi += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t f = field_of(poff, nf, gi);
+        const BatchField &B = F[f];
+        const PivotGeom &pg = B.pg;
+        const uint64_t k = gi - poff[f];
+        const uint64_t k2 = k % pg.cnt[2], k1 = (k / pg.cnt[2]) % pg.cnt[1], k0 = k / (pg.cnt[1] * pg.cnt[2]);
+        const uint64_t pos = (pg.origin[0] + k0 * pg.stride[0]) * pg.n1n2 + (pg.origin[1] + k1 * pg.stride[1]) * pg.n2 +
+                             pg.origin[2] + k2 * pg.stride[2];
+        const int32_t q = (int32_t)lround_d(__dmul_rn((double)B.in[pos], pg.rp));
+        B.qb[k] = q;
+        B.rec[pos] = __double2float_rn(__dmul_rn((double)q, pg.peb2));
+        // Range of stream 0: one atomic pair per warp when the warp's items share a field.
+        const uint32_t act = __activemask();
+        const uint32_t f0 = __shfl_sync(act, f, __ffs(act) - 1);
+        if (__all_sync(act, f == f0)) {
+            int32_t lo = q, hi = q;
+            for (int o = 16; o > 0; o >>= 1) {
+                const int32_t l2 = __shfl_xor_sync(act, lo, o), h2 = __shfl_xor_sync(act, hi, o);
+                if ((act >> ((threadIdx.x ^ o) & 31)) & 1) {
+                    lo = min(lo, l2);
+                    hi = max(hi, h2);
+                }
+            }
+            if ((threadIdx.x & 31) == (uint32_t)(__ffs(act) - 1)) {
+                atomicMin(&B.qb_range[0], lo);
+                atomicMax(&B.qb_range[1], hi);
+            }
+        } else {
+            atomicMin(&B.qb_range[0], q);
+            atomicMax(&B.qb_range[1], q);
+        }
+    }
+}
+
 __global__ void pivot_decompress_kernel(PivotGeom pg, const int32_t *__restrict__ qb, float *__restrict__ rec) {
     const uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
@@ -313,6 +351,26 @@ __global__ void tval_from_codes_kernel(const int64_t *__restrict__ t_int, uint64
         tval[g] = __fdiv_rn(__ll2float_rn(t_int[g * L + l]), tp);
 }
 
+// Batched form: every field's blocks of a batch (fields found by their block-offset prefix).
+__global__ void tval_from_codes_batch_kernel(const BatchField *__restrict__ F, const uint64_t *__restrict__ goff, uint32_t nf,
+                                             uint32_t l) {
+    const uint64_t total = goff[nf];
+    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < total; gi += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t f = field_of(goff, nf, gi);
+        const BatchField &B = F[f];
+        const uint64_t g = gi - goff[f];
+        B.tval[g] = __fdiv_rn(__ll2float_rn(B.tint[g * B.fg.layer_num + l]), (float)B.fg.t_precision);
+    }
+}
+
+cudaError_t launch_tval_from_codes_batch(const BatchField *F, const uint64_t *goff, uint32_t nf, uint64_t total_blocks,
+                                         uint32_t l, cudaStream_t st) {
+    if (total_blocks == 0) return cudaSuccess;
+    tval_from_codes_batch_kernel<<<grid_for(total_blocks, 256, 148 * 8), 256, 0, st>>>(F, goff, nf, l);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_tval_from_codes(const int64_t *t_int, uint64_t nblocks, uint32_t L, uint32_t l, float tp, float *tval,
                                    cudaStream_t st) {
     if (nblocks == 0) return cudaSuccess;
@@ -325,6 +383,14 @@ cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *r
                                   cudaStream_t st) {
     uint64_t total = pg.cnt[0] * pg.cnt[1] * pg.cnt[2];
     pivot_compress_kernel<<<grid_for(total, 256, 148 * 16), 256, 0, st>>>(pg, in, rec, qb, qb_range);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pivot_compress_batch(const BatchField *F, const uint64_t *poff, uint32_t nf, uint64_t total_pivots,
+                                        cudaStream_t st) {
+    if (total_pivots == 0) return cudaSuccess;
+    pivot_compress_batch_kernel<<<grid_for(total_pivots, 256, 148 * 16), 256, 0, st>>>(F, poff, nf);
     count_launch();
     return cudaGetLastError();
 }

@@ -15,14 +15,6 @@ namespace asz {
 uint64_t &launch_counter();
 inline void count_launch() { ++launch_counter(); }
 
-struct PivotGeom {
-    uint64_t cnt[3];      // pivots per axis
-    uint64_t stride[3];
-    uint64_t origin[3];   // first pivot (the frame origin)
-    uint64_t n1n2, n2;
-    double rp;            // 0.5 / (double)pivot_eb
-    double peb2;          // 2 * (double)pivot_eb
-};
 
 struct CodeEntry {
     uint32_t code;
@@ -76,6 +68,10 @@ cudaError_t launch_tsel_exact_batch(const BatchField *F, uint32_t l, const float
 cudaError_t launch_tsel_v0_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default, uint8_t *scratch,
                                  uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap,
                                  const unsigned long long *list, const uint32_t *list_count, uint64_t slots, cudaStream_t st);
+cudaError_t launch_pivot_compress_batch(const BatchField *F, const uint64_t *poff, uint32_t nf, uint64_t total_pivots,
+                                        cudaStream_t st);
+cudaError_t launch_tval_from_codes_batch(const BatchField *F, const uint64_t *goff, uint32_t nf, uint64_t total_blocks,
+                                         uint32_t l, cudaStream_t st);
 uint32_t round_tpl_log2(uint64_t t2);
 uint64_t round_batch_items(const RoundGeom &rg, uint32_t tpl_log2);
 cudaError_t launch_round_compress_batch(const BatchField *F, const uint64_t *ioff, uint32_t nf, uint32_t l, uint32_t *queue,

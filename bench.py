@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--shape", default="512,512,512", help="field shape (smaller shapes are for profiler captures)")
     ap.add_argument("--no-tune", action="store_true", help="skip the plan-search / family-selection measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48-field batch measurement")
+    ap.add_argument("--no-series", action="store_true", help="skip the 16-step time-series measurement")
     args = ap.parse_args()
     shape = tuple(int(v) for v in args.shape.split(","))
     if args.impl == "reference":
@@ -392,6 +393,7 @@ def main():
         del c1
     grad_tune = None if args.no_tune else grad_tune_section(ctx, L, dev, rank, barrier)
     batch = None if args.no_batch else batch_section(ctx, dev, rank)
+    series = None if args.no_series else series_section(ctx, dev, rank)
     L.asz_set_stream(ctx._c, None)
     # Max over ranks.
     times = torch.tensor([core_ms, dec_ms, e2e_ms, e2e_dec_ms], device=dev)
@@ -452,7 +454,7 @@ def main():
         "roofline": roofline, "roofline_path": roofline_path, "profile": prof, "host_phases_ms": host_phases,
         "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
         "cpu_baseline": cpu, "clocks": clocks.summary(),
-        "gpu_launches": int(launches), "tune": tune, "grad_tune": grad_tune, "batch": batch,
+        "gpu_launches": int(launches), "tune": tune, "grad_tune": grad_tune, "batch": batch, "series": series,
     }
     print(json.dumps(out))
     if pg:
@@ -478,6 +480,85 @@ def grf_torch(seed, shape, alpha, device):
     f -= f.mean()
     f /= f.std()
     return f.contiguous()
+
+
+C5_SHAPE = (1024, 1024, 512)
+
+
+def c5_steps_torch(seed, shape, count, device, velocity=(1.5, 0.7, 0.3)):
+    """Config 5's time steps on the device: step 0 is a k^-5/3 field plus a tanh front of width 4
+    (amplitude 10x the std) and a zero slab over 10% of axis 0; step n is step 0 advected by n times
+    the velocity (periodic trilinear resampling) plus white noise at 1e-3 of the range."""
+    import torch
+    base = grf_torch(seed, shape, 5.0 / 3.0, device)
+    gen = np.random.default_rng(seed)
+    nrm = gen.standard_normal(3)
+    nrm /= np.linalg.norm(nrm)
+    c = [gen.uniform(0.25 * s, 0.75 * s) for s in shape]
+    ax = [torch.arange(s, device=device, dtype=torch.float32) for s in shape]
+    d = (ax[0][:, None, None] - c[0]) * nrm[0] + (ax[1][None, :, None] - c[1]) * nrm[1] + (ax[2][None, None, :] - c[2]) * nrm[2]
+    base += 10.0 * base.std() * torch.tanh(d / 4.0)
+    del d
+    z0 = int(gen.integers(0, shape[0] - shape[0] // 10))
+    base[z0:z0 + shape[0] // 10] = 0.0
+    g = torch.Generator(device=device).manual_seed(seed + 1)
+    for n in range(count):
+        if n == 0:
+            yield base.clone()
+            continue
+        out = base
+        for axis, v in enumerate(velocity):
+            s = v * n
+            i = int(np.floor(s))
+            w = s - i
+            out = (1 - w) * torch.roll(out, i, dims=axis) + w * torch.roll(out, i + 1, dims=axis)
+        out += torch.randn(shape, generator=g, device=device) * (1e-3 * float(out.max() - out.min()))
+        yield out.contiguous()
+
+
+def series_section(ctx, dev, rank, steps=16, batch=4, rel_eb=1e-4):
+    """Config 5: 16 steps of a 1024x1024x512 field (2 GiB each), REL 1e-4. Step 0: plan search and
+    coefficient scan; steps 1-15: step 0's plan, gradient-tuned coefficients, 4 steps per batched
+    call. Against full tuning of steps 1 and 15 on their own (plan search + scan)."""
+    import time
+
+    import torch
+
+    from asz_b200 import api, series
+    p = api.default_params(block_pivot_ratio=BPR)
+    nbytes = 4 * C5_SHAPE[0] * C5_SHAPE[1] * C5_SHAPE[2]
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    out = []
+    for s in series.compress_series(ctx, c5_steps_torch(500 + rank, C5_SHAPE, steps, dev), rel_eb, p, "cubic", batch):
+        out.append({"index": s.index, "len": len(s.blob), "tune_ms": s.tune_ms, "call_s": s.info.get("call_s"),
+                    "batch_total_s": s.info.get("batch_total_s"), "abs_eb": s.report.abs_eb})
+    torch.cuda.synchronize(dev)
+    total_s = time.perf_counter() - t0
+    plan = None
+    full = {}
+    for k, x in enumerate(c5_steps_torch(500 + rank, C5_SHAPE, steps, dev)):
+        if k not in (1, steps - 1):
+            continue
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        blob, r = ctx.compress(x, rel_eb, None, "cubic", p)
+        full[k] = {"len": len(blob), "call_s": time.perf_counter() - t1, "plan_s": r.plan_s, "plan": r.plan.decode()}
+        plan = plan or r.plan.decode()
+        del x
+    later = [o for o in out if o["index"] > 0]
+    batches_s = sum({o["batch_total_s"] for o in later})
+    return {"steps": steps, "shape": "x".join(map(str, C5_SHAPE)), "bytes_per_step": nbytes, "rel_eb": rel_eb,
+            "batch": batch, "total_s": total_s, "series_gbs": steps * nbytes / total_s / 1e9,
+            "step0_full_tuning_s": out[0]["call_s"],
+            "later_tune_ms_mean": sum(o["tune_ms"] for o in later) / len(later),
+            "later_batched_calls_s": batches_s, "later_gbs": len(later) * nbytes / batches_s / 1e9,
+            "cr": [nbytes / o["len"] for o in out],
+            "full_tuning": {str(k): {**v, "cr": nbytes / v["len"],
+                                     "cr_reuse_over_full": out[k]["len"] and v["len"] / out[k]["len"]}
+                            for k, v in full.items()},
+            "timing": "host wall clock; total_s covers generating the steps on the device, step 0's full tuning "
+                      "and the later steps' tuning and batched calls (zstd included)"}
 
 
 def batch_section(ctx, dev, rank, count=48, lo=96, hi=512, steps=3):

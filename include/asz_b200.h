@@ -216,6 +216,14 @@ int asz_compress_batch(asz_ctx *ctx, uint32_t count, const float *const *in, int
                        float rel_eb, const asz_params *p, const char *plan, uint8_t **out, size_t *out_len,
                        asz_report *reps, asz_batch_report *brep);
 
+/* As asz_compress_batch, with each field's t codes given (t_tables[f], t_lens[f] entries,
+ * block-major as for asz_compress_with_t) instead of selected: the time-series form, where the plan
+ * of the first step is reused and each later step's coefficients come from the gradient tuner. */
+int asz_compress_batch_with_t(asz_ctx *ctx, uint32_t count, const float *const *in, int in_on_device,
+                              const uint64_t *dims, float rel_eb, const asz_params *p, const char *plan,
+                              const int64_t *const *t_tables, const uint64_t *t_lens, uint8_t **out, size_t *out_len,
+                              asz_report *reps, asz_batch_report *brep);
+
 /* Decompress .asz bytes into `out` (prod(dims) floats; host pointer, or device pointer when
  * out_on_device is nonzero). */
 int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const uint64_t dims[3], float rel_eb,

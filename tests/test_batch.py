@@ -37,6 +37,14 @@ def test_batch_equals_single_field(gpu_ctx, plan, family):
             assert blob == single
     o = O.compress(fs[0], 1e-3, plan, family == "quintic", O.default_params(block_pivot_ratio=3))
     assert blobs[0] == o.asz
+    # New data of the same shapes replays the captured sequence: the values it reads (error
+    # bounds, slopes, classes) come from the fields' records, not from the capture.
+    fs2 = [f * 3.0 + 1.0 for f in fs]
+    blobs2, _, br2 = gpu_ctx.compress_batch(fs2, 1e-3, plan, family, p)
+    assert br2.graph_reused == 1
+    for f, blob in zip(fs2, blobs2):
+        single, _ = gpu_ctx.compress(f, 1e-3, plan, family, p)
+        assert blob == single
 
 
 def test_batch_device_inputs_and_errors(gpu_ctx):
