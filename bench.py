@@ -673,9 +673,14 @@ def grad_tune_section(ctx, L, dev, rank, barrier):
     del x
     return out
 
-# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernel
-# family, from the committed ncu captures; None until captured.
-TRAFFIC_PER_LAUNCH = {}
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel families, from
+# an ncu capture of a 256x512x512 C2 field (plan cubic2_012 x9, REL 1e-3): the mean per launch,
+# doubled for the 512^3 field (the traffic grows with the number of values).
+TRAFFIC_PER_LAUNCH = {
+    "tsel_fast": 2 * (291.48e6 + 8.45e6),
+    "round_compress": 2 * (359.66e6 + 127.39e6),
+    "round_decompress": 2 * (167.80e6 + 57.93e6),
+}
 
 
 class PROFILE_ENTRY(_C.Structure):
