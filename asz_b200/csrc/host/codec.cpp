@@ -154,7 +154,7 @@ struct asz_ctx {
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
         classes, axis, pre, chunks, out, proxies, tlist, spill, iota, plan_qb, plan_e, plan_aux, plan_pay, probe_in, probe_pred,
-        rounds_dev, lines_bail, lines_resume;
+        rounds_dev, lines_bail, lines_resume, enc;
     // Batches (asz_compress_batch): per-field slices of these arenas, the captured round sequence
     // of the last batch, and the launch shapes the autotuner chose per batch shape.
     DevBuf b_in, b_rec, b_qb, b_tval, b_tint, b_ent, b_cls, b_rounds, b_qoff, b_range, b_range0, b_prox, b_amb, b_cnt,
@@ -642,7 +642,7 @@ void asz_destroy(asz_ctx *c) {
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
                       &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
                       &c->plan_pay, &c->probe_in, &c->probe_pred, &c->rounds_dev, &c->lines_bail,
-                      &c->lines_resume, &c->b_in, &c->b_rec, &c->b_qb, &c->b_tval, &c->b_tint, &c->b_ent, &c->b_cls,
+                      &c->lines_resume, &c->enc, &c->b_in, &c->b_rec, &c->b_qb, &c->b_tval, &c->b_tint, &c->b_ent, &c->b_cls,
                       &c->b_rounds, &c->b_qoff, &c->b_range, &c->b_range0, &c->b_prox, &c->b_amb, &c->b_cnt, &c->b_fields,
                       &c->b_goff, &c->b_poff, &c->b_ioff, &c->b_queue, &c->b_hand, &c->b_spill})
         b->release();
@@ -1921,29 +1921,63 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
     CK(cudaMemcpyAsync(ctx->codes.p, codes.data(), codes.size() * sizeof(CodeEntry), cudaMemcpyHostToDevice, st));
     CK(ctx->payload.reserve(std::max<u64>(words_total, 1) * 4));
     CK(cudaMemsetAsync(ctx->payload.p, 0, std::max<u64>(words_total, 1) * 4, st));
-    CK(ctx->bitoff.reserve(std::max<u64>(max_count, 1) * 8));
-    size_t tmp_bytes = 0;
-    CK(launch_encode<int32_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp_bytes, nullptr, st));
-    size_t tmp64 = 0;
-    CK(launch_encode<int64_t>(nullptr, max_count, 0, nullptr, ctx->bitoff.as<u64>(), nullptr, tmp64, nullptr, st));
-    tmp_bytes = std::max(tmp_bytes, tmp64);
-    CK(ctx->cubtmp.reserve(tmp_bytes));
     uint32_t *d_pay = ctx->payload.as<uint32_t>();
     CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
     hs_codes.reset();
-    for (u64 f = 0; f < nf; f++) {
-        const EncodeArgs &a = A[f];
-        for (u64 s2 = 0; s2 < SO[f].size(); s2++) {
-            StreamOut &o = SO[f][s2];
-            if (!o.count || o.code.maxval == 1) continue;
+    {
+        // Every stream of every field in two sets of launches, one per symbol type (the t streams
+        // are int64, the QB streams int32).
+        std::vector<EncStream> es[2];
+        std::vector<u64> toff[2] = {{0}, {0}};
+        u64 enc_bytes = 0;
+        for (u64 f = 0; f < nf; f++) {
+            const EncodeArgs &a = A[f];
+            for (u64 s2 = 0; s2 < SO[f].size(); s2++) {
+                StreamOut &o = SO[f][s2];
+                if (!o.count || o.code.maxval == 1) continue;
+                const int k = s2 == 0 ? 1 : 0;
+                const void *sym = s2 == 0 ? (const void *)a.d_tint : (const void *)(a.d_qb + (*a.qb_off)[s2 - 1]);
+                es[k].push_back(EncStream{sym, o.count, o.lo, d_codes + code_off[f][s2], d_pay + o.payload_word_off});
+                const u64 tile = k ? enc_tile<int64_t>() : enc_tile<int32_t>();
+                toff[k].push_back(toff[k].back() + (o.count + tile - 1) / tile);
+                enc_bytes += o.count * (s2 == 0 ? 8 : 4) + (o.code.bits + 7) / 8;
+            }
+        }
+        // Layout in ctx->enc: per type the stream records, the tile prefix, tile_bits, tile_scan.
+        u64 off[2][4], bytes = 0;
+        auto place = [&](u64 n) {
+            const u64 o = bytes;
+            bytes += (n + 15) / 16 * 16;
+            return o;
+        };
+        size_t tmp_bytes = 0;
+        for (int k = 0; k < 2; k++) {
+            const u64 nt = toff[k].back();
+            off[k][0] = place(es[k].size() * sizeof(EncStream));
+            off[k][1] = place(toff[k].size() * sizeof(u64));
+            off[k][2] = place((nt + 1) * sizeof(u64));
+            off[k][3] = place((nt + 1) * sizeof(u64));
+            size_t tb = 0;
+            if (k == 0) CK(launch_encode_tiles<int32_t>(nullptr, 0, nullptr, nt, nullptr, nullptr, nullptr, tb, st));
+            else CK(launch_encode_tiles<int64_t>(nullptr, 0, nullptr, nt, nullptr, nullptr, nullptr, tb, st));
+            tmp_bytes = std::max(tmp_bytes, tb);
+        }
+        CK(ctx->enc.reserve(std::max<u64>(bytes, 16)));
+        CK(ctx->cubtmp.reserve(std::max<size_t>(tmp_bytes, 16)));
+        uint8_t *eb = ctx->enc.as<uint8_t>();
+        ProfScope ps(ctx, "huff_encode", enc_bytes);
+        for (int k = 0; k < 2; k++) {
+            const u64 nt = toff[k].back();
+            if (!nt) continue;
+            CK(cudaMemcpyAsync(eb + off[k][0], es[k].data(), es[k].size() * sizeof(EncStream), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(eb + off[k][1], toff[k].data(), toff[k].size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(eb + off[k][2] + nt * sizeof(u64), 0, sizeof(u64), st));  // the scan's total
             size_t tb = ctx->cubtmp.cap;
-            ProfScope ps(ctx, "huff_encode", o.count * (s2 == 0 ? 8 : 4) + (o.code.bits + 7) / 8);
-            if (s2 == 0)
-                CK(launch_encode<int64_t>(a.d_tint, o.count, o.lo, d_codes + code_off[f][s2], ctx->bitoff.as<u64>(),
-                                          ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
-            else
-                CK(launch_encode<int32_t>(a.d_qb + (*a.qb_off)[s2 - 1], o.count, o.lo, d_codes + code_off[f][s2],
-                                          ctx->bitoff.as<u64>(), ctx->cubtmp.p, tb, d_pay + o.payload_word_off, st));
+            const EncStream *E = (const EncStream *)(eb + off[k][0]);
+            const u64 *T = (const u64 *)(eb + off[k][1]);
+            u64 *tbits = (u64 *)(eb + off[k][2]), *tscan = (u64 *)(eb + off[k][3]);
+            if (k == 0) CK(launch_encode_tiles<int32_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
+            else CK(launch_encode_tiles<int64_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
         }
     }
     // Stream assembly (compress.tpp:233-291) in pinned memory: the host writes the headers and

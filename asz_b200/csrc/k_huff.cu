@@ -65,6 +65,106 @@ __global__ void encode_kernel(const T *__restrict__ s, uint64_t n, int64_t offse
 }
 
 // ---------------------------------------------------------------------------------------------
+// Tiled encoding of several streams in one set of launches: per tile of kEncTile symbols its bit
+// count (tile_bits_kernel), an exclusive scan over all tiles, and a packing pass
+// (encode_tile_kernel) that builds each tile's bits in shared memory and writes them as whole
+// words, with atomicOr only on its first and last word, which it may share with the neighbouring
+// tiles. A stream's tiles are consecutive; a tile's bit offset in its stream is the scan at the tile
+// minus the scan at the stream's first tile.
+
+__device__ __forceinline__ uint32_t stream_of(const uint64_t *toff, uint32_t ns, uint64_t t) {
+    uint32_t lo = 0, hi = ns;  // toff[lo] <= t < toff[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (toff[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kEncThreads)
+    tile_bits_kernel(const EncStream *__restrict__ S, uint32_t ns, const uint64_t *__restrict__ toff, uint64_t ntiles,
+                     uint64_t *__restrict__ tile_bits) {
+    __shared__ uint32_t red[kEncThreads / 32];
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const EncStream &E = S[stream_of(toff, ns, t)];
+        const T *sym = reinterpret_cast<const T *>(E.s);
+        const uint64_t i0 = (t - toff[stream_of(toff, ns, t)]) * enc_tile<T>();
+        const uint64_t i1 = min(i0 + enc_tile<T>(), E.n);
+        uint32_t bits = 0;
+        for (uint64_t i = i0 + threadIdx.x; i < i1; i += kEncThreads)
+            bits += E.tab[(uint64_t)((int64_t)sym[i] - E.offset)].len;
+        for (int o = 16; o; o >>= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bits;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint64_t sum = 0;
+            for (int w = 0; w < kEncThreads / 32; w++) sum += red[w];
+            tile_bits[t] = sum;
+        }
+        __syncthreads();
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kEncThreads)
+    encode_tile_kernel(const EncStream *__restrict__ S, uint32_t ns, const uint64_t *__restrict__ toff, uint64_t ntiles,
+                       const uint64_t *__restrict__ tile_scan) {
+    constexpr uint32_t kTile = enc_tile<T>(), kPer = kTile / kEncThreads;
+    __shared__ T sym_sh[kTile];
+    __shared__ uint32_t buf[kTile + 2];  // codes are at most 32 bits, plus the leading shift
+    __shared__ uint32_t wsum[kEncThreads / 32];
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t si = stream_of(toff, ns, t);
+        const EncStream &E = S[si];
+        const T *sym = reinterpret_cast<const T *>(E.s);
+        const uint64_t i0 = (t - toff[si]) * kTile;
+        const uint32_t cnt = (uint32_t)min((uint64_t)kTile, E.n - i0);
+        const uint64_t bit0 = tile_scan[t] - tile_scan[toff[si]];
+        const uint32_t shift = (uint32_t)(bit0 & 31);
+        for (uint32_t i = threadIdx.x; i < cnt; i += kEncThreads) sym_sh[i] = sym[i0 + i];
+        for (uint32_t i = threadIdx.x; i < kTile + 2; i += kEncThreads) buf[i] = 0u;
+        __syncthreads();
+        // This thread's symbols: kPer consecutive ones, so its bits are one consecutive run.
+        const uint32_t j0 = threadIdx.x * kPer;
+        uint32_t mine = 0;
+        for (uint32_t j = j0; j < j0 + kPer && j < cnt; j++) mine += E.tab[(uint64_t)((int64_t)sym_sh[j] - E.offset)].len;
+        // Exclusive scan of the threads' bit counts (warp shuffles, then the warps' sums).
+        uint32_t incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((threadIdx.x & 31) >= (uint32_t)o) incl += v;
+        }
+        if ((threadIdx.x & 31) == 31) wsum[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        uint32_t before = 0;
+        for (uint32_t w = 0; w < (threadIdx.x >> 5); w++) before += wsum[w];
+        uint32_t pos = shift + before + incl - mine;
+        for (uint32_t j = j0; j < j0 + kPer && j < cnt; j++) {
+            const CodeEntry e = E.tab[(uint64_t)((int64_t)sym_sh[j] - E.offset)];
+            const uint64_t v = (uint64_t)e.code << (pos & 31);
+            if ((uint32_t)v) atomicOr(&buf[pos >> 5], (uint32_t)v);
+            if ((pos & 31) + e.len > 32 && (uint32_t)(v >> 32)) atomicOr(&buf[(pos >> 5) + 1], (uint32_t)(v >> 32));
+            pos += e.len;
+        }
+        __syncthreads();
+        uint32_t total = 0;
+        for (uint32_t w = 0; w < kEncThreads / 32; w++) total += wsum[w];
+        const uint32_t nw = (shift + total + 31) >> 5;
+        uint32_t *out = E.out + (bit0 >> 5);
+        for (uint32_t i = threadIdx.x; i < nw; i += kEncThreads) {
+            if (i == 0 || i == nw - 1) {
+                if (buf[i]) atomicOr(&out[i], buf[i]);
+            } else {
+                out[i] = buf[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Decoding. The host builds a lookup table of 2^lut_bits entries indexed by the next lut_bits
 // payload bits (LSB-first): len>0 gives a complete code of that length and its symbol index;
 // len==0 means the code is longer, and `node` is the tree node reached after lut_bits bits.
@@ -322,6 +422,26 @@ cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntr
     count_launch();
     return cudaGetLastError();
 }
+
+template <class T>
+cudaError_t launch_encode_tiles(const EncStream *streams, uint32_t ns, const uint64_t *toff, uint64_t ntiles, uint64_t *tile_bits,
+                                uint64_t *tile_scan, void *tmp, size_t &tmp_bytes, cudaStream_t st) {
+    if (tmp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, tile_bits, tile_scan, (int64_t)ntiles + 1, st);
+    if (ntiles == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, 148 * 8);
+    tile_bits_kernel<T><<<grid, kEncThreads, 0, st>>>(streams, ns, toff, ntiles, tile_bits);
+    count_launch();
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, tile_bits, tile_scan, (int64_t)ntiles + 1, st);
+    if (e != cudaSuccess) return e;
+    encode_tile_kernel<T><<<grid, kEncThreads, 0, st>>>(streams, ns, toff, ntiles, tile_scan);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_encode_tiles<int32_t>(const EncStream *, uint32_t, const uint64_t *, uint64_t, uint64_t *, uint64_t *,
+                                                  void *, size_t &, cudaStream_t);
+template cudaError_t launch_encode_tiles<int64_t>(const EncStream *, uint32_t, const uint64_t *, uint64_t, uint64_t *, uint64_t *,
+                                                  void *, size_t &, cudaStream_t);
 
 cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st) {
     if (tmp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, in, out, (int64_t)n, st);
