@@ -447,7 +447,7 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
                     rep[a] = 1;
                 }
             }
-            ClassInfo ci{1, 0, 0, 1};
+            ClassInfo ci{1, 0, 0, 1, {0, 0, 0}, 0, 0};
             if (!exists) {
                 G.classes[l][cls] = ci;
                 continue;
@@ -472,8 +472,13 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
             u64 n = 1;
             for (int a = 0; a < 3; a++) {
                 u64 step = stride[a] * ss;
-                n *= hi[a] > lo[a] ? (hi[a] - lo[a] + step - 1) / step : 0;
+                const u64 c = hi[a] > lo[a] ? (hi[a] - lo[a] + step - 1) / step : 0;
+                ci.cnt[a] = (uint32_t)c;
+                n *= c;
             }
+            auto magic = [](u64 dv) { return dv > 1 && dv <= 0xffffffffull ? (uint32_t)(0xffffffffull / dv + 1) : 0u; };
+            ci.m2 = magic(ci.cnt[2]);
+            ci.m12 = magic((u64)ci.cnt[1] * ci.cnt[2]);
             ci.ss = (uint32_t)ss;
             ci.n = (uint32_t)n;
             ci.fallback = n == 0 ? 1 : 0;

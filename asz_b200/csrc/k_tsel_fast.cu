@@ -62,23 +62,18 @@ __device__ void fast_one(GroupShared &sh, const FieldGeom &fg, const RoundGeom &
         }
         return;
     }
+    // The per-axis sample counts and their division constants come with the class.
     FastSampleGeo sg;
-    uint32_t cnt[3];
     for (int a = 0; a < 3; a++) {
         uint64_t lo = fg.origin[a] + bb[a] * fg.block_shape[a];
-        uint64_t hi = min(fg.origin[a] + (bb[a] + 1) * fg.block_shape[a] + 1, fg.n[a]);
         if (a != d && lo != 0) lo += rg.stride[a];
-        if (a == d) {
-            lo += 3 * rg.stride[a] / 2;
-            hi -= 3 * rg.stride[a] / 2;
-        }
+        if (a == d) lo += 3 * rg.stride[a] / 2;
         sg.lo[a] = lo;
         sg.step[a] = rg.stride[a] * ci.ss;
-        cnt[a] = (uint32_t)((hi - lo + sg.step[a] - 1) / sg.step[a]);
     }
-    sg.cnt2 = cnt[2];
-    sg.c2 = small_div(cnt[2]);
-    sg.c12 = small_div(cnt[1] * cnt[2]);
+    sg.cnt2 = ci.cnt[2];
+    sg.c2 = SmallDiv{ci.cnt[2], ci.m2};
+    sg.c12 = SmallDiv{ci.cnt[1] * ci.cnt[2], ci.m12};
     const GlobalSrc src{sg, rec, orig, fg.n[1], fg.n[2], rg.dist, rg.neg_2_stat_eb};
     float t = 0.0f;
     const uint32_t code = fast_group(sh, src, n, rg, log2arena + ci.log2_off, R2, why, t);

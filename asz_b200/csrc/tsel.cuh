@@ -40,6 +40,8 @@ struct ClassInfo {
     uint32_t n;          // samples
     uint32_t log2_off;   // log2 table offset for n
     uint32_t fallback;   // 1: the block is too short along the axis (compress.tpp:96)
+    uint32_t cnt[3];     // samples per axis (the same for every block of the class)
+    uint32_t m2, m12;    // floor((2^32 - 1) / d) + 1 for d = cnt[2] and cnt[1] * cnt[2] (0 when d <= 1)
 };
 
 // A per-block t decision that needs the host's glibc log10f to settle.

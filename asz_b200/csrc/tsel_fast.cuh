@@ -211,11 +211,13 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
     // Window placement from the first kThreads samples (one per thread): their bin range per
     // candidate, centred in the window. A group whose samples overflow the window is redone
     // with the exact ranges of all samples.
-    float af0 = 0.0f, bf0 = 0.0f;
-    bool nz0 = false;
+    // Each thread's first two samples are loaded together and kept for the main pass.
+    float af0 = 0.0f, bf0 = 0.0f, af1 = 0.0f, bf1 = 0.0f;
+    bool nz0 = false, nz1 = false;
     float afmin = INFINITY, afmax = -INFINITY, bfmin = INFINITY, bfmax = -INFINITY;
     if (tid < n) {
         src.keys(tid, af0, bf0, nz0);
+        if (tid + kThreads < n) src.keys(tid + kThreads, af1, bf1, nz1);
         afmin = afmax = af0;
         bfmin = bfmax = bf0;
     }
@@ -277,6 +279,10 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
                 af = af0;
                 bf = bf0;
                 nz = nz0;
+            } else if (s == tid + kThreads) {
+                af = af1;
+                bf = bf1;
+                nz = nz1;
             } else {
                 src.keys(s, af, bf, nz);
             }

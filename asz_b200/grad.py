@@ -61,6 +61,7 @@ class Problem:
     offsets: "torch.Tensor"  # int32 [groups + 1] (uint32 values)
     meta: "torch.Tensor"     # float32 [groups, 4]: layer eb, stat eb, 0.5 / stat eb, layer slope
     info: GradProblem
+    bufs: tuple = ()         # the allocations behind A and B (never empty, so never a null pointer)
 
     @property
     def groups(self) -> int:
@@ -69,6 +70,12 @@ class Problem:
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr())
+
+
+def _ab(prob):
+    """Device pointers of the samples (their allocations, valid even when there are none)."""
+    a, b = prob.bufs if prob.bufs else (prob.A, prob.B)
+    return _ptr(a), _ptr(b)
 
 
 def _stream(t):
@@ -103,7 +110,7 @@ def prepare(ctx: api.Context, x, rel_eb: float, plan: str, params: api.Params | 
         ctx._check(L.asz_grad_gather(ctx._c, _ptr(A), _ptr(B), _ptr(off), _ptr(meta)))
     finally:
         L.asz_set_stream(ctx._c, None)
-    return Problem(A[:S], B[:S], off, meta[:G], info)
+    return Problem(A[:S], B[:S], off, meta[:G], info, (A, B))
 
 
 class RelaxedProxy:
@@ -128,7 +135,7 @@ def _make_function():
             L = _bind(api.lib())
             t = t.contiguous()
             J = torch.empty_like(t)
-            rc = L.asz_grad_forward(_ptr(prob.A), _ptr(prob.B), _ptr(prob.offsets), _ptr(prob.meta),
+            rc = L.asz_grad_forward(*_ab(prob), _ptr(prob.offsets), _ptr(prob.meta),
                                     C.c_float(prob.info.R2), _ptr(t), prob.groups, _ptr(J), _stream(t))
             if rc:
                 raise api.AszError(rc, "asz_grad_forward failed")
@@ -143,7 +150,7 @@ def _make_function():
             L = _bind(api.lib())
             gJ = gJ.contiguous()
             gt = torch.empty_like(t)
-            rc = L.asz_grad_backward(_ptr(prob.A), _ptr(prob.B), _ptr(prob.offsets), _ptr(prob.meta),
+            rc = L.asz_grad_backward(*_ab(prob), _ptr(prob.offsets), _ptr(prob.meta),
                                      C.c_float(prob.info.R2), _ptr(t), _ptr(gJ), prob.groups, _ptr(gt), _stream(t))
             if rc:
                 raise api.AszError(rc, "asz_grad_backward failed")
@@ -202,7 +209,7 @@ def tune(prob: Problem, steps: int = STEPS, step0: float = STEP0, with_relaxed: 
     stream = torch.cuda.current_stream(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    rc = L.asz_grad_tune(_ptr(prob.A), _ptr(prob.B), _ptr(prob.offsets), _ptr(prob.meta), C.c_float(prob.info.R2), G,
+    rc = L.asz_grad_tune(*_ab(prob), _ptr(prob.offsets), _ptr(prob.meta), C.c_float(prob.info.R2), G,
                          C.c_float(prob.info.t_min), C.c_float(prob.info.t_max), prob.info.t_precision, steps,
                          C.c_float(step0), step_cap, team, _ptr(codes), _ptr(relaxed) if relaxed is not None else None, _ptr(stats),
                          _stream(codes))

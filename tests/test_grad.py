@@ -165,3 +165,37 @@ def test_tuned_stream_matches_oracle(gpu_ctx, rel_eb):
     print(f"rel_eb {rel_eb}: CR tuned {len(f.tobytes()) / len(blob):.4f} plain {len(f.tobytes()) / len(plain):.4f}; "
           f"{info}")
     assert len(blob) <= 1.02 * len(plain)
+
+
+@pytest.mark.gpu
+def test_given_t_errors(gpu_ctx):
+    """Given t tables: a wrong length and a code outside [t_min, t_max] are rejected with a message;
+    the tuner's launch rejects a team size it cannot run."""
+    import ctypes as C
+
+    import asz_b200.api as api
+    from asz_b200 import grad
+    f = _c4_small(shape=(40, 40, 48))
+    plan = ",".join(["cubic0_012", "cubic1_012", "cubic2_012"] * 2)
+    p = api.default_params(block_pivot_ratio=3)
+    _, rep = gpu_ctx.compress(f, 1e-3, plan, "cubic", p)
+    n = gpu_ctx.debug_t().size
+    with pytest.raises(api.AszError, match="t table length"):
+        gpu_ctx.compress_with_t(f, 1e-3, plan, "cubic", p, np.full(n + 1, 8, np.int64))
+    with pytest.raises(api.AszError, match="outside"):
+        gpu_ctx.compress_with_t(f, 1e-3, plan, "cubic", p, np.full(n, 13, np.int64))
+    with pytest.raises(api.AszError, match="t table length"):
+        gpu_ctx.compress_batch([f, f], 1e-3, plan, "cubic", p, t_tables=[np.full(n, 8, np.int64), np.full(3, 8, np.int64)])
+    prob = grad.prepare(gpu_ctx, f, 1e-3, plan, p)
+    assert prob.info.samples > 0
+    with pytest.raises(api.AszError):
+        grad.tune(prob, team=1024)
+    codes, info = grad.tune(prob, team=64)
+    blob, _ = gpu_ctx.compress_with_t(f, 1e-3, plan, "cubic", p, codes)
+    o = O.compress(f, 1e-3, plan, False, O.default_params(block_pivot_ratio=3), t_int=codes.cpu().numpy())
+    assert blob == o.asz
+    # A plan whose every group falls back has no samples at all: every code stays the default.
+    empty = grad.prepare(gpu_ctx, f[:8, :8, :8].copy(), 1e-3, "cubic0_012", api.default_params(block_pivot_ratio=2))
+    assert empty.info.samples == 0
+    codes0, _ = grad.tune(empty)
+    assert (codes0 == 8).all()
