@@ -212,6 +212,74 @@ __device__ __forceinline__ void compress_line(const FieldGeom &fg, const RoundGe
     }
 }
 
+// Two lines at once (lineB == UINT32_MAX: none). Both lines share the k2 sequence; each step loads
+// both targets' inputs before it computes and stores either, so the loads overlap.
+template <bool kProbe>
+__device__ __forceinline__ void compress_lines2(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *__restrict__ ent,
+                                                uint32_t tpl_log2, uint32_t sub, uint32_t lineA, uint32_t lineB,
+                                                const float *__restrict__ tval, const float *__restrict__ in,
+                                                float *__restrict__ rec, int32_t *__restrict__ qb, uint32_t *err_word,
+                                                float *__restrict__ pred_out, double ebd, double eb2, double rinv, double r0,
+                                                int32_t &lo, int32_t &hi) {
+    const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
+    const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
+    const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
+    const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
+    const int dir = rg.dir;
+    const bool hasB = lineB != UINT32_MAX;
+    const uint32_t a0 = lineA / T1, b0 = hasB ? lineB / T1 : a0;
+    const AxisEntry e0A = load_entry(e0t + a0), e1A = load_entry(e1t + (lineA - a0 * T1));
+    const AxisEntry e0B = load_entry(e0t + b0), e1B = load_entry(e1t + (hasB ? lineB - b0 * T1 : lineA - a0 * T1));
+    const uint64_t posA0 = (uint64_t)e0A.ii * n1n2 + (uint64_t)e1A.ii * n2, posB0 = (uint64_t)e0B.ii * n1n2 + (uint64_t)e1B.ii * n2;
+    const uint32_t blkA = e0A.bb * nb1 + e1A.bb, blkB = e0B.bb * nb1 + e1B.bb;
+    const LineQB lqA = line_qb(rg, e0A, e1A), lqB = line_qb(rg, e0B, e1B);
+    for (uint32_t k2 = sub; k2 < T2; k2 += 1u << tpl_log2) {
+        const AxisEntry e2 = load_entry(e2t + k2);
+        const uint64_t posA = posA0 + e2.ii, posB = posB0 + e2.ii;
+        const uint64_t qiA = target_qb(rg, lqA, e0A, e1A, e2), qiB = target_qb(rg, lqB, e0B, e1B, e2);
+        const uint32_t scA = dir == 0 ? e0A.stencil : dir == 1 ? e1A.stencil : e2.stencil;
+        const uint32_t scB = dir == 0 ? e0B.stencil : dir == 1 ? e1B.stencil : e2.stencil;
+        const bool okA = qiA < rg.qb_total, okB = hasB && qiB < rg.qb_total;
+        if (!okA || (hasB && !okB)) atomicOr(err_word, 4u);
+        StencilIn vA{}, vB{};
+        float xA = 0.0f, xB = 0.0f, tA = 0.0f, tB = 0.0f;
+        if (okA) {
+            vA = load_stencil(rec, posA, rg.dist, scA);
+            xA = __ldg(in + posA);
+            if (scA == kStencilCubic) tA = __ldg(tval + (uint64_t)blkA * nb2 + e2.bb);
+        }
+        if (okB) {
+            vB = load_stencil(rec, posB, rg.dist, scB);
+            xB = __ldg(in + posB);
+            if (scB == kStencilCubic) tB = __ldg(tval + (uint64_t)blkB * nb2 + e2.bb);
+        }
+        if (okA) {
+            const float pred = predict_loaded(vA, scA, tA);
+            const double pd = (double)pred;
+            const double diff = __dsub_rn(pd, (double)xA);
+            const double q = dir == 0 && !kProbe ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+            if (kProbe) pred_out[posA] = pred;
+            const int32_t v = (int32_t)lround_d(q);
+            qb[qiA] = v;
+            rec[posA] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
+            lo = min(lo, v);
+            hi = max(hi, v);
+        }
+        if (okB) {
+            const float pred = predict_loaded(vB, scB, tB);
+            const double pd = (double)pred;
+            const double diff = __dsub_rn(pd, (double)xB);
+            const double q = dir == 0 && !kProbe ? __dmul_rn(diff, r0) : quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+            if (kProbe) pred_out[posB] = pred;
+            const int32_t v = (int32_t)lround_d(q);
+            qb[qiB] = v;
+            rec[posB] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
+            lo = min(lo, v);
+            hi = max(hi, v);
+        }
+    }
+}
+
 __device__ __forceinline__ void reduce_range(int32_t lo, int32_t hi, int32_t *qb_range) {
     for (int o = 16; o > 0; o >>= 1) {
         lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -229,7 +297,7 @@ __device__ __forceinline__ void reduce_range(int32_t lo, int32_t hi, int32_t *qb
 // kProbe: every axis divides, as the diagnostics instantiation that the predictor-family probe runs
 // does (one out-of-line clone for all axes), and pred_out receives each target's prediction.
 template <bool kProbe>
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(256, 4)
     round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
                           const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
                           int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out) {
@@ -237,9 +305,12 @@ __global__ void __launch_bounds__(256, 5)
     const uint32_t lines = (uint32_t)rg.tcount[0] * (uint32_t)rg.tcount[1];
     const LineMap m = line_map(tpl_log2);
     int32_t lo = INT32_MAX, hi = INT32_MIN;
-    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += gridDim.x * m.lines_per_cta)
-        compress_line<kProbe>(fg, rg, ent, tpl_log2, m.sub, line, tval, in, rec, qb, err_word, pred_out, ebd, eb2, rinv, r0, lo,
-                              hi);
+    const uint32_t step = gridDim.x * m.lines_per_cta;
+    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += 2 * step) {
+        const uint32_t lineB = line + step < lines ? line + step : UINT32_MAX;
+        compress_lines2<kProbe>(fg, rg, ent, tpl_log2, m.sub, line, lineB, tval, in, rec, qb, err_word, pred_out, ebd, eb2, rinv,
+                                r0, lo, hi);
+    }
     reduce_range(lo, hi, qb_range);
 }
 
@@ -411,7 +482,7 @@ static uint32_t tpl_log2_for(uint64_t t2) {
 static unsigned round_grid(const RoundGeom &rg, uint32_t tpl_log2) {
     const uint64_t lines = rg.tcount[0] * rg.tcount[1];
     const uint64_t per_cta = 256u >> tpl_log2;
-    return grid_for(lines, (unsigned)per_cta, 148 * 32);
+    return grid_for(lines, (unsigned)(2 * per_cta), 148 * 32);
 }
 
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,

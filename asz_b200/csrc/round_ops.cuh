@@ -49,6 +49,83 @@ __device__ __forceinline__ float predict_case(const float *__restrict__ c, uint6
     }
 }
 
+// A target's stencil inputs, loaded ahead of its prediction: the neighbours that its stencil case
+// uses (others are not read) through the read-only path. Within a round, no target reads a
+// position that the round writes, so these loads may run ahead of the round's stores.
+struct StencilIn {
+    float m1, p1, m3, p3, m5, p5;
+};
+
+__device__ __forceinline__ StencilIn load_stencil(const float *__restrict__ c, uint64_t pos, uint64_t dist, uint32_t sc) {
+    StencilIn v{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    switch (sc) {
+    case kStencilQuintic:
+        v.m5 = __ldg(c + pos - 5 * dist);
+        v.p5 = __ldg(c + pos + 5 * dist);
+        [[fallthrough]];
+    case kStencilCubic:
+        v.m3 = __ldg(c + pos - 3 * dist);
+        v.p3 = __ldg(c + pos + 3 * dist);
+        v.m1 = __ldg(c + pos - dist);
+        v.p1 = __ldg(c + pos + dist);
+        break;
+    case kStencilLeft1:
+        v.m1 = __ldg(c + pos - dist);
+        break;
+    case kStencilLeft2:
+        v.m1 = __ldg(c + pos - dist);
+        v.p1 = __ldg(c + pos + dist);
+        break;
+    case kStencilLeft3:
+        v.m1 = __ldg(c + pos - dist);
+        v.p1 = __ldg(c + pos + dist);
+        v.p3 = __ldg(c + pos + 3 * dist);
+        break;
+    case kStencilRight1:
+        v.m1 = __ldg(c + pos - dist);
+        v.m3 = __ldg(c + pos - 3 * dist);
+        break;
+    default:  // kStencilRight2
+        v.m1 = __ldg(c + pos - dist);
+        v.p1 = __ldg(c + pos + dist);
+        v.m3 = __ldg(c + pos - 3 * dist);
+        break;
+    }
+    return v;
+}
+
+// predict_case on loaded inputs: the same operations in the same order.
+__device__ __forceinline__ float predict_loaded(const StencilIn &v, uint32_t sc, float t) {
+    switch (sc) {
+    case kStencilQuintic: {
+        float s1 = __fadd_rn(v.m1, v.p1);
+        float s3 = __fadd_rn(v.m3, v.p3);
+        float s5 = __fadd_rn(v.m5, v.p5);
+        double acc = __dmul_rn((double)s3, kQuinticB);
+        acc = __fma_rn((double)s1, kQuinticI, acc);
+        acc = __fma_rn((double)s5, kQuinticA, acc);
+        return __double2float_rn(acc);
+    }
+    case kStencilLeft1:
+        return v.m1;
+    case kStencilLeft2:
+        return __fmul_rn(__fadd_rn(v.m1, v.p1), 0.5f);
+    case kStencilLeft3:
+        return __fmul_rn(__fsub_rn(__fmaf_rn(v.m1, 3.0f, __fmul_rn(v.p1, 6.0f)), v.p3), 0.125f);
+    case kStencilRight1:
+        return __fmul_rn(__fmaf_rn(v.m1, 3.0f, -v.m3), 0.5f);
+    case kStencilRight2:
+        return __fmul_rn(__fmaf_rn(v.p1, 3.0f, __fmaf_rn(v.m1, 6.0f, -v.m3)), 0.125f);
+    default: {
+        float s3 = __fadd_rn(v.m3, v.p3);
+        float s1 = __fadd_rn(v.m1, v.p1);
+        double td = (double)t;
+        float p1 = __double2float_rn(__dmul_rn((double)s3, __dsub_rn(0.25, td)));
+        return __double2float_rn(__fma_rn(__dadd_rn(0.25, td), (double)s1, (double)p1));
+    }
+    }
+}
+
 __device__ __forceinline__ AxisEntry load_entry(const AxisEntry *e) {
     const uint4 *p = reinterpret_cast<const uint4 *>(e);
     uint4 a = __ldg(p), b = __ldg(p + 1);
