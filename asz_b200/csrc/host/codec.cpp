@@ -35,10 +35,14 @@
 #include "../launch.h"
 #include "../listsim.cuh"
 #include "../../../include/asz_b200.h"
+#include "buffers.h"
 #include "huffman_host.h"
+#include "internal.h"
 #include "zstd_api.h"
 
 using namespace asz;
+using asz::host::DevBuf;
+using asz::host::PinnedBuf;
 
 namespace {
 
@@ -46,53 +50,6 @@ using u64 = uint64_t;
 using clk = std::chrono::steady_clock;
 
 double secs(clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); }
-
-// Grow-only device buffer.
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    cudaError_t reserve(size_t bytes) {
-        if (bytes <= cap) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = std::max<size_t>(bytes, 256);
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) cap = want;
-        return e;
-    }
-    template <class T>
-    T *as() const {
-        return (T *)p;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
-// Grow-only pinned host buffer: the stream before zstd is staged here, so the device<->host copies
-// of the Huffman payloads run at DMA speed straight into (or out of) their final positions.
-struct PinnedBuf {
-    uint8_t *p = nullptr;
-    size_t cap = 0, len = 0;
-    cudaError_t reserve(size_t bytes) {
-        if (bytes <= cap) return cudaSuccess;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = std::max<size_t>(bytes + bytes / 8, 4096);
-        cudaError_t e = cudaHostAlloc((void **)&p, want, cudaHostAllocDefault);
-        if (e == cudaSuccess) cap = want;
-        return e;
-    }
-    void release() {
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = len = 0;
-    }
-};
 
 // llround of a float as the reference's -Ofast build computes it (see dev_common.cuh).
 int64_t host_lround_f(float x) {
@@ -198,6 +155,8 @@ struct asz_ctx {
     };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> event_pool;
+    // Prediction sweep (host/sweep.cpp): its buffers, owned there.
+    void *sweep = nullptr;
 };
 
 namespace {
@@ -656,6 +615,7 @@ void asz_destroy(asz_ctx *c) {
     c->batch_pre[1].release();
     c->raw_in.release();
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    asz::host::sweep_release(c->sweep);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
 }
@@ -700,7 +660,9 @@ struct MiscLayout {  // small device words, one allocation
     ProxyEval evals[64];
 };
 
-int compute_range(asz_ctx *ctx, const float *d_in, u64 N, float &mn, float &mx) {
+// first_max: a zero maximum takes the sign of the first largest element (std::max_element)
+// instead of the last one (std::minmax_element).
+int compute_range(asz_ctx *ctx, const float *d_in, u64 N, float &mn, float &mx, bool first_max = false) {
     MiscLayout init{};
     init.range[0] = INT32_MAX;
     init.range[1] = INT32_MIN;
@@ -732,7 +694,7 @@ int compute_range(asz_ctx *ctx, const float *d_in, u64 N, float &mn, float &mx) 
         CK(cudaMemcpyAsync(fl, &dm->zfirst, 16, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         if (mn == 0.0f) CK(cudaMemcpy(&mn, d_in + fl[0], 4, cudaMemcpyDeviceToHost));
-        if (mx == 0.0f) CK(cudaMemcpy(&mx, d_in + fl[1], 4, cudaMemcpyDeviceToHost));
+        if (mx == 0.0f) CK(cudaMemcpy(&mx, d_in + fl[first_max ? 0 : 1], 4, cudaMemcpyDeviceToHost));
     }
     return ASZ_OK;
 }
@@ -3471,3 +3433,28 @@ extern "C" int asz_compress_batch_with_t(asz_ctx *ctx, uint32_t count, const flo
     return compress_batch_impl(ctx, count, in, in_on_device, dims, rel_eb, &p, plan_text, t_tables, t_lens, out, out_len, reps,
                                brep);
 }
+
+// ---------------------------------------------------------------------------------------------
+// Internal interface for the other C-ABI translation units (host/internal.h).
+
+namespace asz::host {
+
+cudaStream_t ctx_stream(asz_ctx *c) { return c->stream; }
+
+int ctx_fail(asz_ctx *c, int code, const std::string &m) { return fail(c, code, m); }
+
+int ctx_range(asz_ctx *ctx, const float *d_in, uint64_t n, bool first_max, float &mn, float &mx) {
+    CK(ctx->misc.reserve(sizeof(MiscLayout)));
+    return compute_range(ctx, d_in, n, mn, mx, first_max);
+}
+
+int ctx_upload(asz_ctx *ctx, const float *in, uint64_t n, const float **d_in) {
+    CK(ctx->in.reserve(n * sizeof(float)));
+    CK(cudaMemcpyAsync(ctx->in.p, in, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    *d_in = ctx->in.as<float>();
+    return ASZ_OK;
+}
+
+void *&ctx_sweep_state(asz_ctx *c) { return c->sweep; }
+
+}  // namespace asz::host

@@ -187,4 +187,55 @@ cudaError_t launch_decode_write(const uint8_t *base, uint64_t chunk_bits, const 
 template <class T>
 cudaError_t launch_fill(T *out, uint64_t n, T v, cudaStream_t st);
 
+// Prediction sweep (k_sweep.cu; c_codes/s2_many_prediction.cpp:126-397). Targets are visited as
+// lines: loop levels 0 and 1 (axes axis[0], axis[1]) select a line, level 2 (axis[2], the QB
+// order) runs along it. Legacy targets: start + index * step per level, per_line = count[2].
+// Common targets (common = 1): every level covers [5, n - 5) and only points with an odd
+// coordinate sum count, so a line whose outer coordinates have an even sum holds inner_odd
+// targets (the odd inner coordinates) and the others inner_even; per_line is the larger.
+struct SweepGeom {
+    uint64_t n[3];
+    uint64_t dist[2];          // linear neighbour distances (dist[1]: second 2D4R axis)
+    uint64_t start[3], step[3], count[3];
+    uint64_t inner_odd, inner_even;
+    uint64_t lines, per_line, targets;
+    uint32_t axis[3];
+    uint32_t kind;             // 0: 1D4R, 1: 2D4R, 2: 1D6R
+    uint32_t common;
+};
+// Target `it` of the (line, position) space: false when the position is past its line's count
+// (common targets); else its coordinates i[] and its index j in the QB stream. Lines before line
+// (a, b) of the common targets, split by the parity of a + b, give j.
+ASZ_HD bool sweep_target(const SweepGeom &g, uint64_t it, uint64_t i[3], uint64_t &j) {
+    const uint64_t line = it / g.per_line, k = it - line * g.per_line;
+    const uint64_t a = line / g.count[1], b = line - a * g.count[1];
+    i[g.axis[0]] = g.start[0] + a * g.step[0];
+    i[g.axis[1]] = g.start[1] + b * g.step[1];
+    if (!g.common) {
+        i[g.axis[2]] = g.start[2] + k * g.step[2];
+        j = it;
+        return true;
+    }
+    // (a + 5) + (b + 5) has the parity of a + b; the inner coordinate makes the sum odd.
+    const bool odd_line = (a + b) & 1;
+    if (k >= (odd_line ? g.inner_even : g.inner_odd)) return false;
+    i[g.axis[2]] = (odd_line ? 6 : 5) + 2 * k;
+    const uint64_t L1 = g.count[1];
+    const uint64_t q0 = (a + 1) / 2 * ((L1 + 1) / 2) + a / 2 * (L1 / 2) + ((a & 1) ? b / 2 : (b + 1) / 2);
+    const uint64_t q1 = a * L1 + b - q0;
+    j = q0 * g.inner_odd + q1 * g.inner_even + k;
+    return true;
+}
+// One coefficient set: 1D4R lo = 0.25 - t, hi = 0.25 + t; 2D4R hi weighs the first axis, lo the
+// second; 1D6R c0 = a, c1 = b, w = 0.5 - (a + b).
+struct SweepCoef {
+    double c0, c1, w, lo, hi;
+};
+cudaError_t launch_sweep_predict(const float *d, const SweepGeom &g, const SweepCoef *coef, uint32_t ncoef, double abs_eb,
+                                 double neg_2_eb, int64_t *qb, uint64_t qb_stride, double *part, long long *mm,
+                                 cudaStream_t st);
+uint32_t sweep_predict_grid(const SweepGeom &g);
+cudaError_t launch_sweep_sums(const double *part, uint32_t nparts, uint32_t ncoef, double *sums, cudaStream_t st);
+cudaError_t launch_sweep_first(const int64_t *s, uint64_t n, int64_t offset, unsigned long long *first, cudaStream_t st);
+
 }  // namespace asz

@@ -271,6 +271,41 @@ int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset);
 int asz_error_stats_noalloc(const float *x, const float *y, uint64_t n, double value_range, void *cuda_stream,
                             double *max_err, double *psnr, char *err, size_t err_len);
 
+/* ---------------------------------------------------------------------------------------------
+ * Prediction sweep: the GPU form of the reference's study tool s2_many_prediction
+ * (c_codes/s2_many_prediction.cpp:164-464, whose command line bin/s2_many_prediction keeps). One
+ * call runs one predictor ("1d4r<axis>_xx<order>", "2d4r<axes>_xx<order>" with axes 01, 02 or 12,
+ * "1d6r<axis>_xx<order>") over each relative error bound and each coefficient of the predictor's
+ * grid: t = i/32, i = 0..12 (1d4r); t = i/24, i = -6..6 (2d4r); the six-reference grid "legacy",
+ * "augmented" or "transition" (1d6r, six_reference_grid :89-124). Targets are "legacy",
+ * "shared1d" (1d4r margin 5) or "common" (for_each_common_target :126-149). Each row carries the
+ * tool's figures: BR and CR from the zstd-3 size of the Huffman-coded QB stream, H1, prediction
+ * RMSE and MAE, PSNR, and the sample count. QB streams, H1, the Huffman and zstd sizes (so BR
+ * and CR) are the reference's exactly; RMSE, MAE and PSNR come from sums taken in a different
+ * order and agree to rounding (relative 1e-12 in the tests). */
+typedef struct asz_sweep_row {
+    double rel_eb, c0, c1;        /* c0 = t (1d4r, 2d4r) or a (1d6r); c1 = b (1d6r) */
+    uint64_t samples, huffman_bytes, zstd_bytes;
+    double mse_sum, rmse_sum, mae_sum;   /* sums over the targets, before the divisions */
+    double br, cr, h1, h1_cr, rmse, mae, psnr;
+    double encode_seconds;        /* this row's share of its batch's histogram, Huffman and zstd time */
+} asz_sweep_row;
+
+/* The coefficient grid of a predictor: fills c0/c1 up to cap, the count in *count. */
+int asz_sweep_coefs(const char *predictor, const char *six_grid, double *c0, double *c1, uint64_t cap, uint64_t *count);
+/* Host-side run of the kernel's target mapping (no GPU involved): the targets' (i0, i1, i2) in QB
+ * stream order into coords[0, 3 x count) when coords is non-NULL (cap >= count). Returns
+ * ASZ_E_DEVICE if the mapping misses or repeats a stream position. */
+int asz_sweep_targets(const uint64_t dims[3], const char *predictor, const char *targets, uint64_t *coords, uint64_t cap,
+                      uint64_t *count);
+/* Rows for every rel_eb (outer) and coefficient (inner), the reference's order, into rows[0,
+ * cap); *n_rows = n_eb x grid size (ASZ_E_ARG when cap is smaller). min_max (may be NULL)
+ * receives the field's float minimum and maximum (std::min_element / std::max_element). The
+ * field must have every dimension >= 12, finite values and max > min. */
+int asz_sweep(asz_ctx *ctx, const float *data, int on_device, const uint64_t dims[3], const char *predictor,
+              const char *targets, const char *six_grid, const double *rel_eb, uint64_t n_eb, asz_sweep_row *rows,
+              uint64_t cap, uint64_t *n_rows, float *min_max);
+
 /* Host-side self-check of the target geometry the round kernels use, for a field of the given
  * dims, plan and block ratio (no GPU involved): every stencil and sampling read is in bounds
  * and hits a value written in an earlier round, every point is written once, and the QB index

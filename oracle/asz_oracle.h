@@ -113,6 +113,30 @@ uint64_t aszo_i64map_order(const int64_t *k, uint64_t n, uint64_t *order);
 void aszo_h1_psnr(const int64_t *a, const int64_t *b, uint64_t n, float t, float abs_eb, float stat_eb,
                   float min_val, float max_val, float *h1, float *psnr, float *x, float *mse);
 
+/* Prediction sweep (c_codes/s2_many_prediction.cpp), one row = one predictor, rel_eb and
+ * coefficient set. Sums are before the divisions by the sample count. */
+typedef struct aszo_sweep_row {
+    double c0, c1;                 /* t (1d4r, 2d4r) or a, b (1d6r) */
+    uint64_t samples, huffman_bytes, zstd_bytes;
+    double mse_sum, rmse_sum, mae_sum;
+    double br, cr, h1, h1_cr, rmse, mae, psnr;
+} aszo_sweep_row;
+
+/* Coefficients of a predictor ("1d4r0_xx2", "2d4r01_xx1", "1d6r2_xx0"): t = i/32 (1d4r), i/24
+ * (2d4r), or the six-reference grid "legacy" | "augmented" | "transition" (1d6r). Returns the
+ * count (arrays filled up to cap) or -1. */
+int aszo_sweep_coefs(const char *predictor, const char *six_grid, double *c0, double *c1, uint64_t cap);
+/* The targets in stream order as (i0, i1, i2) triples (up to cap); returns the count. targets:
+ * "legacy" | "shared1d" | "common". */
+uint64_t aszo_sweep_targets(const uint64_t dims[3], const char *predictor, const char *targets, uint64_t *coords,
+                            uint64_t cap);
+/* One row: QB stream (qb_out may be NULL), H1, Huffman + zstd sizes and the figures. */
+int aszo_sweep_run(const float *data, const uint64_t dims[3], const char *predictor, const char *targets, double rel_eb,
+                   float min_val, float max_val, double c0, double c1, int64_t *qb_out, uint64_t qb_cap,
+                   aszo_sweep_row *row, char *err);
+/* Fills br, cr, h1_cr, rmse, mae and psnr from the sizes and sums; range = max - min. */
+void aszo_sweep_finish(aszo_sweep_row *row, double range);
+
 #ifdef __cplusplus
 }
 #endif

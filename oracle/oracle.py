@@ -56,6 +56,13 @@ class _Result(C.Structure):
     ]
 
 
+class SweepRow(C.Structure):
+    _fields_ = [("c0", C.c_double), ("c1", C.c_double), ("samples", C.c_uint64), ("huffman_bytes", C.c_uint64),
+                ("zstd_bytes", C.c_uint64), ("mse_sum", C.c_double), ("rmse_sum", C.c_double), ("mae_sum", C.c_double),
+                ("br", C.c_double), ("cr", C.c_double), ("h1", C.c_double), ("h1_cr", C.c_double), ("rmse", C.c_double),
+                ("mae", C.c_double), ("psnr", C.c_double)]
+
+
 def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
@@ -90,6 +97,13 @@ def liboracle():
         lib.aszo_i64map_order.restype = C.c_uint64
         lib.aszo_h1_psnr.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_float, C.c_float, C.c_float,
                                      C.c_float, C.c_float] + [C.POINTER(C.c_float)] * 4
+        lib.aszo_sweep_coefs.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint64]
+        lib.aszo_sweep_targets.argtypes = [C.POINTER(C.c_uint64), C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64]
+        lib.aszo_sweep_targets.restype = C.c_uint64
+        lib.aszo_sweep_run.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_char_p, C.c_char_p, C.c_double,
+                                       C.c_float, C.c_float, C.c_double, C.c_double, C.c_void_p, C.c_uint64,
+                                       C.POINTER(SweepRow), C.c_char_p]
+        lib.aszo_sweep_finish.argtypes = [C.POINTER(SweepRow), C.c_double]
         _LIB = lib
     return _LIB
 
@@ -220,6 +234,40 @@ def i64map_order(keys: np.ndarray) -> np.ndarray:
     out = np.empty(keys.size, np.uint64)
     k = liboracle().aszo_i64map_order(keys.ctypes.data, keys.size, out.ctypes.data)
     return out[:k].astype(np.int64)
+
+
+def sweep_coefs(predictor: str, six_grid: str = "legacy"):
+    """Coefficient list of a sweep predictor: [(c0, c1), ...]."""
+    a, b = np.empty(128), np.empty(128)
+    n = liboracle().aszo_sweep_coefs(predictor.encode(), six_grid.encode(), a.ctypes.data, b.ctypes.data, 128)
+    if n < 0:
+        raise ValueError(predictor)
+    return list(zip(a[:n].tolist(), b[:n].tolist()))
+
+
+def sweep_targets(shape, predictor: str, targets: str = "legacy") -> np.ndarray:
+    """(S, 3) uint64 target coordinates in stream order."""
+    lib = liboracle()
+    n = lib.aszo_sweep_targets(_dims(shape), predictor.encode(), targets.encode(), None, 0)
+    out = np.empty((n, 3), np.uint64)
+    lib.aszo_sweep_targets(_dims(shape), predictor.encode(), targets.encode(), out.ctypes.data, n)
+    return out
+
+
+def sweep_run(data: np.ndarray, predictor: str, rel_eb: float, c0: float, c1: float = 0.0, targets: str = "legacy",
+              with_qb: bool = False):
+    """One sweep row on the CPU: SweepRow (and the int64 QB stream when with_qb)."""
+    lib = liboracle()
+    d = np.ascontiguousarray(data, np.float32)
+    mn, mx = float(d.min()), float(d.max())
+    cap = int(d.size) if with_qb else 0
+    qb = np.empty(cap, np.int64)
+    row, err = SweepRow(), C.create_string_buffer(256)
+    rc = lib.aszo_sweep_run(d.ctypes.data, _dims(d.shape), predictor.encode(), targets.encode(), rel_eb, mn, mx, c0, c1,
+                            qb.ctypes.data if with_qb else None, cap, C.byref(row), err)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return (row, qb[: row.samples]) if with_qb else row
 
 
 # ---------------------------------------------------------------------------------------------
