@@ -211,6 +211,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the plan-search / family-selection measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48-field batch measurement")
     ap.add_argument("--no-series", action="store_true", help="skip the 16-step time-series measurement")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the prediction-sweep (s2_many_prediction) measurement")
     args = ap.parse_args()
     shape = tuple(int(v) for v in args.shape.split(","))
     if args.impl == "reference":
@@ -394,6 +395,7 @@ def main():
     grad_tune = None if args.no_tune else grad_tune_section(ctx, L, dev, rank, barrier)
     batch = None if args.no_batch else batch_section(ctx, dev, rank)
     series = None if args.no_series else series_section(ctx, dev, rank)
+    sweep = None if args.no_sweep else sweep_section(ctx, dev, rank, with_reference=not args.no_cpu_baseline)
     L.asz_set_stream(ctx._c, None)
     # Max over ranks.
     times = torch.tensor([core_ms, dec_ms, e2e_ms, e2e_dec_ms], device=dev)
@@ -455,6 +457,7 @@ def main():
         "decompress_profile": prof_dec, "decompress_host_phases_ms": host_phases_dec,
         "cpu_baseline": cpu, "clocks": clocks.summary(),
         "gpu_launches": int(launches), "tune": tune, "grad_tune": grad_tune, "batch": batch, "series": series,
+        "sweep": sweep,
     }
     print(json.dumps(out))
     if pg:
@@ -613,6 +616,68 @@ def batch_section(ctx, dev, rank, count=48, lo=96, hi=512, steps=3):
                       "batch_python_wall_s adds the Python wrapper's copies of the 48 outputs; single_calls_s: host "
                       "wall clock around 48 asz_compress calls; rounds_device_ms: CUDA events around the captured "
                       "round sequence"}
+def sweep_section(ctx, dev, rank, rel_eb=1e-3, with_reference=True, ref_planes=50):
+    """The prediction sweep of s2_many_prediction on the C1 shape (100x500x500 k^-11/3 GRF + blobs
+    + noise): all 27 predictors with the legacy grids and targets at one error bound (594 rows),
+    the field resident on the device. Beside it, the reference tool (oracle/_ref, built from its
+    sources) on the first `ref_planes` planes for the 1d4r2 stencil (39 rows), with our rows on the
+    same slab compared line by line with its printed figures."""
+    import torch
+
+    from asz_b200 import fields
+    from asz_b200 import sweep as sw
+    x = fields.c1_field(seed=11 + rank, shape=C1_SHAPE)
+    xd = torch.from_numpy(x).to(dev)
+    preds = sw.predictors("all")
+    sw.run(ctx, xd, preds[0], [rel_eb])
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    nrows = targets = 0
+    enc = 0.0
+    for p in preds:
+        rows, _ = sw.run(ctx, xd, p, [rel_eb])
+        nrows += len(rows)
+        targets += sum(r.samples for r in rows)
+        enc += sum(r.encode_seconds for r in rows)
+    gpu_s = time.perf_counter() - t0
+    out = {"field": "x".join(map(str, C1_SHAPE)) + " k^-11/3 GRF + 20 blobs + 1e-4 noise", "rel_eb": rel_eb,
+           "predictors": len(preds), "rows": nrows, "targets": targets, "wall_s": gpu_s, "rows_per_s": nrows / gpu_s,
+           "targets_per_s": targets / gpu_s, "encode_share": enc / gpu_s,
+           "timing": "host wall clock around one asz_sweep call per predictor (field on the device): prediction, "
+                     "histograms, Huffman encoding on the GPU, H1, framing and libzstd level 3 on the host threads; "
+                     "encode_share: the part spent from the histograms to the last zstd"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    exe = O.ref_binary("s2_many_prediction")
+    if with_reference and rank == 0 and exe is not None:
+        slab = np.ascontiguousarray(x[:ref_planes])
+        with tempfile.TemporaryDirectory() as wd:
+            inp = os.path.join(wd, "slab.f32")
+            slab.tofile(inp)
+            t0 = time.perf_counter()
+            r = subprocess.run([exe, inp, *map(str, slab.shape), os.path.join(wd, "ref"), "1d4r2", repr(rel_eb)],
+                               capture_output=True, text=True)
+            ref_s = time.perf_counter() - t0
+        if r.returncode == 0:
+            ref_lines = [ln for ln in r.stdout.splitlines() if not ln.startswith(("predictor=", "total_seconds="))]
+            ours, ours_rows, t0 = [], 0, time.perf_counter()
+            for p in sw.predictors("1d4r2"):
+                rows, mm = sw.run(ctx, slab, p, [rel_eb])
+                ours_rows += len(rows)
+                for g in rows:
+                    ours += [f"rel_eb={g.rel_eb:f}, t={g.c0:f}", f"BR={g.br:f}, CR={g.cr:f}", f"H1={g.h1:f}, H1_cr={g.h1_cr:f}",
+                             f"RMSE={g.rmse:f}, MAE={g.mae:f}", f"PSNR={g.psnr:f}", ""]
+            ours_s = time.perf_counter() - t0
+            ref_rows = sum(1 for ln in ref_lines if ln.startswith("BR="))
+            out["reference"] = {"sample": f"reference s2_many_prediction, stencil 1d4r2 (3 orders x 13 t) at {rel_eb:g} "
+                                          f"on a {'x'.join(map(str, slab.shape))} slab, one core, wall time",
+                                "kind": "reference", "cores": 1, "rows": ref_rows, "wall_s": ref_s,
+                                "rows_per_s": ref_rows / ref_s, "ours_rows_per_s_same_slab": ours_rows / ours_s,
+                                "speedup_same_slab": (ref_s / ref_rows) / (ours_s / ours_rows),
+                                "printed_lines_identical": ours == ref_lines[3:]}
+    return out
+
+
 SELECTION_FAMILIES = ("tsel_fast", "tsel_exact", "tsel_serial")
 
 
