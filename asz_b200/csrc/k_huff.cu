@@ -108,11 +108,13 @@ __global__ void __launch_bounds__(kEncThreads)
 }
 
 template <class T>
-__global__ void __launch_bounds__(kEncThreads)
+__global__ void __launch_bounds__(kEncThreads, 4)
     encode_tile_kernel(const EncStream *__restrict__ S, uint32_t ns, const uint64_t *__restrict__ toff, uint64_t ntiles,
                        const uint64_t *__restrict__ tile_scan) {
     constexpr uint32_t kTile = enc_tile<T>(), kPer = kTile / kEncThreads;
-    __shared__ T sym_sh[kTile];
+    // Symbol i sits at i + i / kPer: each thread reads its own kPer consecutive symbols, and the
+    // one-slot gap between runs spreads a warp's reads over all banks.
+    __shared__ T sym_sh[kTile + kEncThreads];
     __shared__ uint32_t buf[kTile + 2];  // codes are at most 32 bits, plus the leading shift
     __shared__ uint32_t wsum[kEncThreads / 32];
     for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -123,13 +125,21 @@ __global__ void __launch_bounds__(kEncThreads)
         const uint32_t cnt = (uint32_t)min((uint64_t)kTile, E.n - i0);
         const uint64_t bit0 = tile_scan[t] - tile_scan[toff[si]];
         const uint32_t shift = (uint32_t)(bit0 & 31);
-        for (uint32_t i = threadIdx.x; i < cnt; i += kEncThreads) sym_sh[i] = sym[i0 + i];
+        for (uint32_t i = threadIdx.x; i < cnt; i += kEncThreads) sym_sh[i + i / kPer] = sym[i0 + i];
         for (uint32_t i = threadIdx.x; i < kTile + 2; i += kEncThreads) buf[i] = 0u;
         __syncthreads();
         // This thread's symbols: kPer consecutive ones, so its bits are one consecutive run.
         const uint32_t j0 = threadIdx.x * kPer;
+        uint32_t code[kPer], len[kPer];
         uint32_t mine = 0;
-        for (uint32_t j = j0; j < j0 + kPer && j < cnt; j++) mine += E.tab[(uint64_t)((int64_t)sym_sh[j] - E.offset)].len;
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; k++) {
+            CodeEntry e{0u, 0u};
+            if (j0 + k < cnt) e = E.tab[(uint64_t)((int64_t)sym_sh[j0 + k + threadIdx.x] - E.offset)];
+            code[k] = e.code;
+            len[k] = e.len;
+            mine += e.len;
+        }
         // Exclusive scan of the threads' bit counts (warp shuffles, then the warps' sums).
         uint32_t incl = mine;
         for (int o = 1; o < 32; o <<= 1) {
@@ -140,13 +150,27 @@ __global__ void __launch_bounds__(kEncThreads)
         __syncthreads();
         uint32_t before = 0;
         for (uint32_t w = 0; w < (threadIdx.x >> 5); w++) before += wsum[w];
-        uint32_t pos = shift + before + incl - mine;
-        for (uint32_t j = j0; j < j0 + kPer && j < cnt; j++) {
-            const CodeEntry e = E.tab[(uint64_t)((int64_t)sym_sh[j] - E.offset)];
-            const uint64_t v = (uint64_t)e.code << (pos & 31);
-            if ((uint32_t)v) atomicOr(&buf[pos >> 5], (uint32_t)v);
-            if ((pos & 31) + e.len > 32 && (uint32_t)(v >> 32)) atomicOr(&buf[(pos >> 5) + 1], (uint32_t)(v >> 32));
-            pos += e.len;
+        // Pack the run in a register: the run's first and last words may be shared with the
+        // neighbouring runs and are or-ed in; the words between belong to this thread alone.
+        const uint32_t pos = shift + before + incl - mine;
+        if (mine) {
+            uint32_t w = pos >> 5, nacc = pos & 31;
+            uint64_t acc = 0;
+            bool first = true;
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; k++) {
+                acc |= (uint64_t)code[k] << nacc;
+                nacc += len[k];
+                if (nacc >= 32) {
+                    if (first) atomicOr(&buf[w], (uint32_t)acc);
+                    else buf[w] = (uint32_t)acc;
+                    first = false;
+                    w++;
+                    acc >>= 32;
+                    nacc -= 32;
+                }
+            }
+            if (nacc) atomicOr(&buf[w], (uint32_t)acc);
         }
         __syncthreads();
         uint32_t total = 0;
