@@ -89,6 +89,7 @@ bool sweep_geometry(const Predictor &p, const u64 n[3], const std::string &targe
     for (int a = 0; a < 3; a++)
         if (a != p.order) g.axis[k++] = (uint32_t)a;
     g.axis[2] = (uint32_t)p.order;
+    g.line_per_thread = p.order != 2;
     if (targets == "common") {
         g.common = 1;
         for (int l = 0; l < 3; l++) {
@@ -388,9 +389,8 @@ extern "C" int asz_sweep(asz_ctx *ctx, const float *data, int on_device, const u
             CK(cudaMemsetAsync(W.first.p, 0xff, htot * 8, st));
             for (u64 k = 0; k < kc; k++) {
                 const int64_t *s = d_qb + k * S;
-                CK(launch_histogram<int64_t>(s, S, h_mm[2 * k], hoff[k + 1] - hoff[k],
-                                             W.hist.as<unsigned long long>() + hoff[k], st));
-                CK(launch_sweep_first(s, S, h_mm[2 * k], W.first.as<unsigned long long>() + hoff[k], st));
+                CK(launch_sweep_stats(s, S, h_mm[2 * k], hoff[k + 1] - hoff[k], W.hist.as<unsigned long long>() + hoff[k],
+                                      W.first.as<unsigned long long>() + hoff[k], st));
             }
             u64 *h_hist = (u64 *)W.counts.p, *h_first = h_hist + htot;
             CK(cudaMemcpyAsync(h_hist, W.hist.p, htot * 8, cudaMemcpyDeviceToHost, st));

@@ -202,6 +202,7 @@ struct SweepGeom {
     uint32_t axis[3];
     uint32_t kind;             // 0: 1D4R, 1: 2D4R, 2: 1D6R
     uint32_t common;
+    uint32_t line_per_thread;  // the QB-order axis is not the contiguous one: a thread walks a line
 };
 // Target `it` of the (line, position) space: false when the position is past its line's count
 // (common targets); else its coordinates i[] and its index j in the QB stream. Lines before line
@@ -236,6 +237,7 @@ cudaError_t launch_sweep_predict(const float *d, const SweepGeom &g, const Sweep
                                  cudaStream_t st);
 uint32_t sweep_predict_grid(const SweepGeom &g);
 cudaError_t launch_sweep_sums(const double *part, uint32_t nparts, uint32_t ncoef, double *sums, cudaStream_t st);
-cudaError_t launch_sweep_first(const int64_t *s, uint64_t n, int64_t offset, unsigned long long *first, cudaStream_t st);
+cudaError_t launch_sweep_stats(const int64_t *s, uint64_t n, int64_t offset, uint64_t range, unsigned long long *hist,
+                               unsigned long long *first, cudaStream_t st);
 
 }  // namespace asz
