@@ -741,10 +741,12 @@ def grad_tune_section(ctx, L, dev, rank, barrier):
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel families, from
 # an ncu capture of a 256x512x512 C2 field (plan cubic2_012 x9, REL 1e-3): the mean per launch,
 # doubled for the 512^3 field (the traffic grows with the number of values).
+# huff_encode is one scope of two launches (tile bit counts, then packing) per compression.
 TRAFFIC_PER_LAUNCH = {
-    "tsel_fast": 2 * (291.48e6 + 8.45e6),
-    "round_compress": 2 * (359.66e6 + 127.39e6),
-    "round_decompress": 2 * (167.80e6 + 57.93e6),
+    "tsel_fast": 2 * (291.49e6 + 8.27e6),
+    "round_compress": 2 * (349.70e6 + 120.10e6),
+    "round_decompress": 2 * (212.82e6 + 91.04e6),
+    "huff_encode": 2 * (268.67e6 + 0.14e6 + 270.14e6 + 38.99e6),
 }
 
 
