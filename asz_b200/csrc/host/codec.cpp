@@ -3152,7 +3152,7 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
     std::vector<uint64_t> shape_key{nf, L, (uint64_t)quintic, p.block_pivot_ratio, (uint64_t)(t_tables != nullptr)};
     for (uint32_t f = 0; f < nf; f++) shape_key.insert(shape_key.end(), B[f].dims, B[f].dims + 3);
     for (u64 l = 0; l < L; l++) shape_key.push_back((uint64_t)plan.dir[l] * 3 + plan.order[l]);
-    BatchShape best{8, 5, 0};
+    BatchShape best{16, 5, 0};
     auto tuned = ctx->batch_tuned.find(shape_key);
     if (tuned != ctx->batch_tuned.end()) {
         best = tuned->second;
@@ -3162,7 +3162,7 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
         float best_ms = INFINITY;
         uint32_t last_shift = UINT32_MAX;
         for (uint32_t shift : {0u, 1u})
-            for (uint32_t fast : {4u, 8u})
+            for (uint32_t fast : {8u, 16u})
                 for (uint32_t round : {3u, 5u}) {
                     if (shift != last_shift) {
                         rc = upload_shape(shift);

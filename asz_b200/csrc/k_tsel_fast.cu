@@ -95,7 +95,7 @@ struct ListHandOff {
 // One CTA per (block, round) group at a time (persistent grid). list_out receives the groups this
 // path could not settle; why[0] counts those whose bins span too many windows, why[1] those with an
 // undecidable comparison; why[2] counts the groups settled here by window-by-window counting.
-__global__ void __launch_bounds__(kThreads, 8)
+__global__ void __launch_bounds__(kThreads, 16)
     tsel_fast_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
                      const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
                      float R2, float t_default, float *__restrict__ tval, int64_t *__restrict__ t_int,
@@ -124,7 +124,7 @@ struct PairHandOff {
     __device__ void operator()(uint64_t g) const { list[atomicAdd(count, 1u)] = ((unsigned long long)f << 32) | g; }
 };
 
-__global__ void __launch_bounds__(kThreads, 8)
+__global__ void __launch_bounds__(kThreads, 16)
     tsel_fast_batch_kernel(const BatchField *__restrict__ F, const uint64_t *__restrict__ goff, uint32_t nf, uint32_t l,
                            const float *__restrict__ log2arena, float t_default, uint32_t *queue,
                            unsigned long long *handoff_list, uint32_t *handoff_count) {

@@ -119,7 +119,7 @@ __device__ __forceinline__ uint64_t fast_sample_pos(const FastSampleGeo &sg, uin
     return (i0 * n1 + i1) * n2 + i2;
 }
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 64;
 constexpr int kWarps = kThreads / 32;
 
 // Shared state of one group (one CTA).
