@@ -393,9 +393,9 @@ def main():
                 "auto": auto, "fixed_cyclic": fixed, "timing": "host wall clock around one C-ABI call each"}
         del c1
     grad_tune = None if args.no_tune else grad_tune_section(ctx, L, dev, rank, barrier)
+    sweep = None if args.no_sweep else sweep_section(ctx, dev, rank, with_reference=not args.no_cpu_baseline)
     batch = None if args.no_batch else batch_section(ctx, dev, rank)
     series = None if args.no_series else series_section(ctx, dev, rank)
-    sweep = None if args.no_sweep else sweep_section(ctx, dev, rank, with_reference=not args.no_cpu_baseline)
     L.asz_set_stream(ctx._c, None)
     # Max over ranks.
     times = torch.tensor([core_ms, dec_ms, e2e_ms, e2e_dec_ms], device=dev)
