@@ -1960,6 +1960,9 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
     }
     CK(pb.reserve(all_len));
     pb.len = all_len;
+    // The encoding launches finish before the copy timer starts, so that d2h_s holds the copies
+    // (and the host's header writing between them) and none of the kernels' time.
+    CK(cudaStreamSynchronize(st));
     auto t_d2h = clk::now();
     {
         HostScope hs(ctx, "host:assembly");
