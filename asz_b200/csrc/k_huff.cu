@@ -399,17 +399,45 @@ __global__ void __launch_bounds__(256)
         uint64_t o = off[k] - off[d.chunk0];
         BitReader br;
         br.init(base, bit);
+        if (d.wide) {
+            while (bit < lim) {
+                const uint32_t sym = decode_sym(br, bit, lut_sh, d.lut_bits, childs + d.child_off);
+                if (sym == 0xffffffffu || o >= d.count) {
+                    atomicOr(err_word, 16u);
+                    break;
+                }
+                static_cast<int64_t *>(d.out)[o++] = (int64_t)sym + d.offset;
+            }
+            continue;
+        }
+        // int32 values go out four at a time as one 16-byte store once the position is aligned:
+        // whole sectors leave the thread instead of one value per store.
+        int32_t *out = static_cast<int32_t *>(d.out);
+        int32_t b0 = 0, b1 = 0, b2 = 0;
+        uint32_t nb = 0;  // values held, to be stored from out + o
         while (bit < lim) {
             const uint32_t sym = decode_sym(br, bit, lut_sh, d.lut_bits, childs + d.child_off);
-            if (sym == 0xffffffffu || o >= d.count) {
+            if (sym == 0xffffffffu || o + nb >= d.count) {
                 atomicOr(err_word, 16u);
                 break;
             }
-            const int64_t v = (int64_t)sym + d.offset;
-            if (d.wide) static_cast<int64_t *>(d.out)[o] = v;
-            else static_cast<int32_t *>(d.out)[o] = (int32_t)v;
-            o++;
+            const int32_t v = (int32_t)((int64_t)sym + d.offset);
+            if (nb == 0 && ((uintptr_t)(out + o) & 15u) != 0) {
+                out[o++] = v;
+            } else if (nb == 3) {
+                *reinterpret_cast<int4 *>(out + o) = make_int4(b0, b1, b2, v);
+                o += 4;
+                nb = 0;
+            } else {
+                if (nb == 0) b0 = v;
+                else if (nb == 1) b1 = v;
+                else b2 = v;
+                nb++;
+            }
         }
+        if (nb > 0) out[o] = b0;
+        if (nb > 1) out[o + 1] = b1;
+        if (nb > 2) out[o + 2] = b2;
     }
 }
 
