@@ -2387,9 +2387,10 @@ int gpu_decode_all(asz_ctx *ctx, const std::vector<DecodeJob> &jobs, const uint8
     const uint32_t *d_ts = (const uint32_t *)(dc + o_ts);
     const LutEntry *d_lut = (const LutEntry *)(dc + o_lut);
     const uint32_t *d_ch = (const uint32_t *)(dc + o_ch);
-    // Per-chunk arrays: start, end, count, off (count + 1 entries for the scan).
-    CK(ctx->chunks.reserve(4 * (nchunks + 1) * 8 + 64));
+    // Per-chunk arrays: start, end, count, off (count + 1 entries for the scan), moved (u32).
+    CK(ctx->chunks.reserve(4 * (nchunks + 1) * 8 + (nchunks + 1) * 4 + 64));
     u64 *d_start = ctx->chunks.as<u64>(), *d_end = d_start + nchunks + 1, *d_cnt = d_end + nchunks + 1, *d_off = d_cnt + nchunks + 1;
+    uint32_t *d_moved = reinterpret_cast<uint32_t *>(d_off + nchunks + 1);
     CK(cudaMemsetAsync(d_cnt + nchunks, 0, 8, st));
     const uint32_t nst = (uint32_t)ds.size();
     const u64 ntiles = tile_stream.size();
@@ -2397,10 +2398,10 @@ int gpu_decode_all(asz_ctx *ctx, const std::vector<DecodeJob> &jobs, const uint8
         {
             ProfScope ps(ctx, "huff_decode_sync", 0);
             CK(launch_decode_sync(d_base, C, d_ds, d_ts, ntiles, max_lut_bits, d_lut, d_ch, it == 0 ? 1 : 0, d_start, d_end, d_cnt,
-                                  &dm->dec_err, st));
+                                  d_moved, &dm->dec_err, st));
         }
         CK(cudaMemsetAsync(&dm->dec_changed, 0, 4, st));
-        CK(launch_decode_restart(d_ds, nst, nchunks, d_end, d_start, &dm->dec_changed, st));
+        CK(launch_decode_restart(d_ds, nst, nchunks, d_end, d_start, d_moved, &dm->dec_changed, st));
         uint32_t changed;
         CK(cudaMemcpyAsync(&changed, &dm->dec_changed, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));

@@ -293,12 +293,14 @@ __device__ __forceinline__ void stage_lut(LutEntry *lut_sh, const LutEntry *__re
 
 // Pass A over all tiles: chunk k decodes from its start until it reaches the next chunk's first
 // bit, recording where it stopped (end[k]) and how many values it produced (count[k]). On the
-// first pass the start is the chunk's first bit; later passes start where chunk k-1 ended.
+// first pass the start is the chunk's first bit; later passes start where chunk k-1 ended, and a
+// chunk whose start did not move (moved[k] == 0) keeps its end and count without decoding.
 __global__ void __launch_bounds__(256)
     decode_sync_kernel(const uint8_t *__restrict__ base, uint64_t chunk_bits, const DecStream *__restrict__ streams,
                        const uint32_t *__restrict__ tile_stream, uint64_t ntiles, const LutEntry *__restrict__ luts,
                        const uint32_t *__restrict__ childs, int first_pass, uint64_t *__restrict__ start,
-                       uint64_t *__restrict__ end, uint64_t *__restrict__ count, uint32_t *err_word) {
+                       uint64_t *__restrict__ end, uint64_t *__restrict__ count, const uint32_t *__restrict__ moved,
+                       uint32_t *err_word) {
     extern __shared__ LutEntry lut_sh[];
     uint32_t staged = 0xffffffffu;
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -313,6 +315,7 @@ __global__ void __launch_bounds__(256)
         const uint64_t kl = (tile - d.tile0) * blockDim.x + threadIdx.x;
         if (kl >= d.nchunks) continue;
         const uint64_t k = d.chunk0 + kl;
+        if (!first_pass && !moved[k]) continue;
         uint64_t bit = first_pass ? d.bit_begin + kl * chunk_bits : start[k];
         if (first_pass) start[k] = bit;
         const uint64_t lim = min(d.bit_begin + (kl + 1) * chunk_bits, d.bit_end);
@@ -344,17 +347,22 @@ __device__ __forceinline__ uint32_t stream_of_chunk(const DecStream *__restrict_
     return lo;
 }
 
-// After a pass: the start of chunk k (not the first of its stream) becomes end[k-1]. Flags
-// whether anything moved.
+// After a pass: the start of chunk k (not the first of its stream) becomes end[k-1]. Marks the
+// chunks whose start moved (moved[k]) and flags whether any did.
 __global__ void decode_restart_kernel(const DecStream *__restrict__ streams, uint32_t nstreams, uint64_t nchunks,
-                                      const uint64_t *__restrict__ end, uint64_t *__restrict__ start, uint32_t *changed) {
+                                      const uint64_t *__restrict__ end, uint64_t *__restrict__ start, uint32_t *__restrict__ moved,
+                                      uint32_t *changed) {
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nchunks; k += (uint64_t)gridDim.x * blockDim.x) {
-        if (streams[stream_of_chunk(streams, nstreams, k)].chunk0 == k) continue;
-        const uint64_t s = end[k - 1];
-        if (s != start[k]) {
-            start[k] = s;
-            *changed = 1u;
+        uint32_t m = 0;
+        if (streams[stream_of_chunk(streams, nstreams, k)].chunk0 != k) {
+            const uint64_t s = end[k - 1];
+            if (s != start[k]) {
+                start[k] = s;
+                m = 1;
+                *changed = 1u;
+            }
         }
+        moved[k] = m;
     }
 }
 
@@ -505,19 +513,20 @@ static unsigned decode_grid(uint64_t ntiles) { return (unsigned)(ntiles < 148 * 
 
 cudaError_t launch_decode_sync(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
                                uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
-                               int first_pass, uint64_t *start, uint64_t *end, uint64_t *count, uint32_t *err, cudaStream_t st) {
+                               int first_pass, uint64_t *start, uint64_t *end, uint64_t *count, const uint32_t *moved,
+                               uint32_t *err, cudaStream_t st) {
     const size_t sh = ((size_t)1 << max_lut_bits) * sizeof(LutEntry);
     decode_sync_kernel<<<decode_grid(ntiles), kDecodeTile, sh, st>>>(base, chunk_bits, streams, tile_stream, ntiles, luts,
-                                                                      childs, first_pass, start, end, count, err);
+                                                                      childs, first_pass, start, end, count, moved, err);
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_decode_restart(const DecStream *streams, uint32_t nstreams, uint64_t nchunks, const uint64_t *end,
-                                  uint64_t *start, uint32_t *changed, cudaStream_t st) {
+                                  uint64_t *start, uint32_t *moved, uint32_t *changed, cudaStream_t st) {
     const uint64_t b = (nchunks + 255) / 256;
     decode_restart_kernel<<<(unsigned)(b < 148 * 8 ? (b ? b : 1) : 148 * 8), 256, 0, st>>>(streams, nstreams, nchunks, end, start,
-                                                                                         changed);
+                                                                                         moved, changed);
     count_launch();
     return cudaGetLastError();
 }

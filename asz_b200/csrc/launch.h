@@ -176,9 +176,10 @@ cudaError_t launch_encode_tiles(const EncStream *streams, uint32_t ns, const uin
 cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st);
 cudaError_t launch_decode_sync(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
                                uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
-                               int first_pass, uint64_t *start, uint64_t *end, uint64_t *count, uint32_t *err, cudaStream_t st);
+                               int first_pass, uint64_t *start, uint64_t *end, uint64_t *count, const uint32_t *moved,
+                               uint32_t *err, cudaStream_t st);
 cudaError_t launch_decode_restart(const DecStream *streams, uint32_t nstreams, uint64_t nchunks, const uint64_t *end,
-                                  uint64_t *start, uint32_t *changed, cudaStream_t st);
+                                  uint64_t *start, uint32_t *moved, uint32_t *changed, cudaStream_t st);
 cudaError_t launch_decode_check(const DecStream *streams, uint32_t nstreams, const uint64_t *off, const uint64_t *end,
                                 uint32_t *err, cudaStream_t st);
 cudaError_t launch_decode_write(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
