@@ -349,40 +349,72 @@ __global__ void __launch_bounds__(256, 5)
 }
 
 // Decompress round (decompress.tpp:34): value = fma(-qb, 2eb, pred) in double, t = t_int/t_precision.
-__global__ void __launch_bounds__(256)
+// Two lines per step (lineB == UINT32_MAX: none): both targets' QB, t and stencil inputs are
+// loaded before either is computed and stored. Within a round no target reads a position that the
+// round writes, so the loads may run ahead of the stores.
+__device__ __forceinline__ void decompress_lines2(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
+                                                  const AxisEntry *__restrict__ ent, uint32_t tpl_log2, uint32_t sub,
+                                                  uint32_t lineA, uint32_t lineB, const int64_t *__restrict__ t_int,
+                                                  const int32_t *__restrict__ qb, float *__restrict__ rec, uint32_t *err_word,
+                                                  double eb2, float tp) {
+    const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
+    const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
+    const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
+    const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
+    const int dir = rg.dir;
+    const bool hasB = lineB != UINT32_MAX;
+    const uint32_t a0 = lineA / T1, b0 = hasB ? lineB / T1 : a0;
+    const AxisEntry e0A = load_entry(e0t + a0), e1A = load_entry(e1t + (lineA - a0 * T1));
+    const AxisEntry e0B = load_entry(e0t + b0), e1B = load_entry(e1t + (hasB ? lineB - b0 * T1 : lineA - a0 * T1));
+    const uint64_t posA0 = (uint64_t)e0A.ii * n1n2 + (uint64_t)e1A.ii * n2, posB0 = (uint64_t)e0B.ii * n1n2 + (uint64_t)e1B.ii * n2;
+    const uint32_t blkA = e0A.bb * nb1 + e1A.bb, blkB = e0B.bb * nb1 + e1B.bb;
+    const LineQB lqA = line_qb(rg, e0A, e1A), lqB = line_qb(rg, e0B, e1B);
+    for (uint32_t k2 = sub; k2 < T2; k2 += 1u << tpl_log2) {
+        const AxisEntry e2 = load_entry(e2t + k2);
+        const uint64_t posA = posA0 + e2.ii, posB = posB0 + e2.ii;
+        const uint64_t qiA = target_qb(rg, lqA, e0A, e1A, e2), qiB = target_qb(rg, lqB, e0B, e1B, e2);
+        const uint32_t scA = dir == 0 ? e0A.stencil : dir == 1 ? e1A.stencil : e2.stencil;
+        const uint32_t scB = dir == 0 ? e0B.stencil : dir == 1 ? e1B.stencil : e2.stencil;
+        const bool okA = qiA < rg.qb_total, okB = hasB && qiB < rg.qb_total;
+        if (!okA || (hasB && !okB)) atomicOr(err_word, 4u);
+        StencilIn vA{}, vB{};
+        int32_t qA = 0, qB = 0;
+        int64_t tiA = 0, tiB = 0;
+        if (okA) {
+            vA = load_stencil(rec, posA, rg.dist, scA);
+            qA = __ldg(qb + qiA);
+            if (scA == kStencilCubic) tiA = __ldg(t_int + ((uint64_t)blkA * nb2 + e2.bb) * fg.layer_num + l);
+        }
+        if (okB) {
+            vB = load_stencil(rec, posB, rg.dist, scB);
+            qB = __ldg(qb + qiB);
+            if (scB == kStencilCubic) tiB = __ldg(t_int + ((uint64_t)blkB * nb2 + e2.bb) * fg.layer_num + l);
+        }
+        if (okA) {
+            const float t = scA == kStencilCubic ? __fdiv_rn(__ll2float_rn(tiA), tp) : 0.0f;
+            const float pred = predict_loaded(vA, scA, t);
+            rec[posA] = __double2float_rn(__fma_rn(-(double)qA, eb2, (double)pred));
+        }
+        if (okB) {
+            const float t = scB == kStencilCubic ? __fdiv_rn(__ll2float_rn(tiB), tp) : 0.0f;
+            const float pred = predict_loaded(vB, scB, t);
+            rec[posB] = __double2float_rn(__fma_rn(-(double)qB, eb2, (double)pred));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 4)
     round_decompress_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
                             const int64_t *__restrict__ t_int, const int32_t *__restrict__ qb, float *__restrict__ rec,
                             uint32_t *err_word) {
     const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd);
     const float tp = (float)fg.t_precision;
-    const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
-    const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
-    const uint32_t lines = (uint32_t)rg.tcount[0] * T1;
-    const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
-    const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
+    const uint32_t lines = (uint32_t)rg.tcount[0] * (uint32_t)rg.tcount[1];
     const LineMap m = line_map(tpl_log2);
-    const int dir = rg.dir;
-    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += gridDim.x * m.lines_per_cta) {
-        const uint32_t k0 = line / T1, k1 = line - k0 * T1;
-        const AxisEntry e0 = load_entry(e0t + k0), e1 = load_entry(e1t + k1);
-        const uint64_t line_pos = (uint64_t)e0.ii * n1n2 + (uint64_t)e1.ii * n2;
-        const uint32_t line_blk = e0.bb * nb1 + e1.bb;
-        const LineQB lq = line_qb(rg, e0, e1);
-        for (uint32_t k2 = m.sub; k2 < T2; k2 += 1u << tpl_log2) {
-            const AxisEntry e2 = load_entry(e2t + k2);
-            const uint64_t pos = line_pos + e2.ii;
-            const uint64_t qi = target_qb(rg, lq, e0, e1, e2);
-            if (qi >= rg.qb_total) {
-                atomicOr(err_word, 4u);
-                continue;
-            }
-            const uint32_t sc = dir == 0 ? e0.stencil : dir == 1 ? e1.stencil : e2.stencil;
-            float t = 0.0f;
-            if (sc == kStencilCubic)
-                t = __fdiv_rn(__ll2float_rn(t_int[((uint64_t)line_blk * nb2 + e2.bb) * fg.layer_num + l]), tp);
-            const float pred = predict_case(rec, pos, rg.dist, sc, t);
-            rec[pos] = __double2float_rn(__fma_rn(-(double)qb[qi], eb2, (double)pred));
-        }
+    const uint32_t step = gridDim.x * m.lines_per_cta;
+    for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += 2 * step) {
+        const uint32_t lineB = line + step < lines ? line + step : UINT32_MAX;
+        decompress_lines2(fg, rg, l, ent, tpl_log2, m.sub, line, lineB, t_int, qb, rec, err_word, eb2, tp);
     }
 }
 
