@@ -28,6 +28,7 @@
 #include <unordered_map>
 #include <random>
 #include <string>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -157,6 +158,10 @@ struct asz_ctx {
     std::vector<cudaEvent_t> event_pool;
     // Prediction sweep (host/sweep.cpp): its buffers, owned there.
     void *sweep = nullptr;
+    // zstd contexts kept across calls (one per concurrent user), and the decompression context.
+    std::mutex zmu;
+    std::vector<ZSTD_CCtx *> zfree;
+    ZSTD_DCtx *zd = nullptr;
 };
 
 namespace {
@@ -231,6 +236,75 @@ namespace {
 int fail(asz_ctx *c, int code, const std::string &m) {
     c->err = m;
     return code;
+}
+
+// zstd level 3 through a context from the asz_ctx's pool (ZSTD_compressCCtx gives ZSTD_compress's
+// bytes); safe from several threads at once.
+size_t zstd3(asz_ctx *c, void *dst, size_t cap, const void *src, size_t n) {
+    ZSTD_CCtx *z = nullptr;
+    {
+        std::lock_guard<std::mutex> g(c->zmu);
+        if (!c->zfree.empty()) {
+            z = c->zfree.back();
+            c->zfree.pop_back();
+        }
+    }
+    if (!z) z = ZSTD_createCCtx();
+    if (!z) return ZSTD_compress(dst, cap, src, n, 3);
+    const size_t r = ZSTD_compressCCtx(z, dst, cap, src, n, 3);
+    std::lock_guard<std::mutex> g(c->zmu);
+    c->zfree.push_back(z);
+    return r;
+}
+
+// Output blocks (the .asz buffers that callers release with asz_free). Each carries a header with
+// its capacity. asz_free returns a block to a small cache that later outputs take (best fit), so a
+// caller compressing field after field reuses memory whose pages are already mapped: the first
+// writes to fresh pages and their unmapping on release cost about as much as zstd itself. The
+// cache holds at most kOutCacheBlocks blocks and kOutCacheBytes bytes; asz_release_output_cache
+// empties it.
+constexpr uint64_t kOutMagic = 0x415a534f55544255ull;
+constexpr size_t kOutHeader = 64;
+constexpr size_t kOutCacheBlocks = 64;
+constexpr uint64_t kOutCacheBytes = 2ull << 30;
+struct OutHeader {
+    uint64_t magic, cap;
+};
+std::mutex g_out_mu;
+std::vector<uint8_t *> g_out_cache;  // block starts (header), oldest first
+uint64_t g_out_cached = 0;
+
+uint8_t *out_alloc(size_t n) {
+    {
+        std::lock_guard<std::mutex> g(g_out_mu);
+        size_t best = g_out_cache.size();
+        for (size_t i = 0; i < g_out_cache.size(); i++) {
+            const uint64_t cap = reinterpret_cast<OutHeader *>(g_out_cache[i])->cap;
+            if (cap >= n && (best == g_out_cache.size() || cap < reinterpret_cast<OutHeader *>(g_out_cache[best])->cap)) best = i;
+        }
+        if (best < g_out_cache.size()) {
+            uint8_t *b = g_out_cache[best];
+            g_out_cache.erase(g_out_cache.begin() + (std::ptrdiff_t)best);
+            g_out_cached -= reinterpret_cast<OutHeader *>(b)->cap;
+            return b + kOutHeader;
+        }
+    }
+    uint8_t *b = (uint8_t *)std::malloc(kOutHeader + (n ? n : 1));
+    if (!b) return nullptr;
+    *reinterpret_cast<OutHeader *>(b) = OutHeader{kOutMagic, (uint64_t)(n ? n : 1)};
+    return b + kOutHeader;
+}
+
+void out_release(uint8_t *p) {
+    uint8_t *b = p - kOutHeader;
+    std::lock_guard<std::mutex> g(g_out_mu);
+    g_out_cache.push_back(b);
+    g_out_cached += reinterpret_cast<OutHeader *>(b)->cap;
+    while (g_out_cache.size() > kOutCacheBlocks || g_out_cached > kOutCacheBytes) {
+        g_out_cached -= reinterpret_cast<OutHeader *>(g_out_cache.front())->cap;
+        std::free(g_out_cache.front());
+        g_out_cache.erase(g_out_cache.begin());
+    }
 }
 
 #define CK(call)                                                                    \
@@ -616,6 +690,8 @@ void asz_destroy(asz_ctx *c) {
     c->raw_in.release();
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     asz::host::sweep_release(c->sweep);
+    for (ZSTD_CCtx *z : c->zfree) ZSTD_freeCCtx(z);
+    if (c->zd) ZSTD_freeDCtx(c->zd);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
 }
@@ -628,7 +704,18 @@ int asz_set_stream(asz_ctx *c, void *s) {
     return ASZ_OK;
 }
 
-void asz_free(void *p) { std::free(p); }
+void asz_free(void *p) {
+    if (!p) return;
+    // Every buffer this library hands out is an output block (out_alloc).
+    out_release(static_cast<uint8_t *>(p));
+}
+
+void asz_release_output_cache(void) {
+    std::lock_guard<std::mutex> g(g_out_mu);
+    for (uint8_t *b : g_out_cache) std::free(b);
+    g_out_cache.clear();
+    g_out_cached = 0;
+}
 
 }  // extern "C"
 
@@ -1145,7 +1232,7 @@ int plan_search(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const a
                 write_len_word(hc, bs.data() + hc.save_size());
                 if (hc.maxval != 1) std::memcpy(bs.data() + hc.save_size() + 8, pay.data() + word_off[c], (hc.bits + 7) >> 3);
                 std::vector<uint8_t> z(ZSTD_compressBound(bs.size()));
-                size_t zl = ZSTD_compress(z.data(), z.size(), bs.data(), bs.size(), 3);
+                size_t zl = zstd3(ctx, z.data(), z.size(), bs.data(), bs.size());
                 if (ZSTD_isError(zl)) z_ok[c] = 0;
                 else zlen[c] = zl;
             };
@@ -2127,11 +2214,11 @@ static int compress_entry(asz_ctx *ctx, const float *in, int in_on_device, const
     auto t_z = clk::now();
     HostScope hs_z(ctx, "host:zstd");
     size_t bound = ZSTD_compressBound(pb.len);
-    uint8_t *z = (uint8_t *)std::malloc(bound ? bound : 1);
+    uint8_t *z = out_alloc(bound);
     if (!z) return fail(ctx, ASZ_E_DATA, "out of host memory");
-    size_t zl = ZSTD_compress(z, bound, pb.p, pb.len, 3);
+    size_t zl = zstd3(ctx, z, bound, pb.p, pb.len);
     if (ZSTD_isError(zl)) {
-        std::free(z);
+        out_release(z);
         return fail(ctx, ASZ_E_DATA, std::string("ZSTD_compress: ") + ZSTD_getErrorName(zl));
     }
     R.zstd_s = secs(t_z, clk::now());
@@ -2451,7 +2538,8 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
     size_t got;
     {
         HostScope hs(ctx, "host:zstd");
-        got = ZSTD_decompress(bsp, raw, in, len);
+        if (!ctx->zd) ctx->zd = ZSTD_createDCtx();
+        got = ctx->zd ? ZSTD_decompressDCtx(ctx->zd, bsp, raw, in, len) : ZSTD_decompress(bsp, raw, in, len);
     }
     if (ZSTD_isError(got) || got != raw) return fail(ctx, ASZ_E_DATA, "ZSTD_decompress error in decompress()");
     R.zstd_s = secs(t_z, clk::now());
@@ -3319,14 +3407,14 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
             zth[k].emplace_back([&, f, src, len]() {
                 auto tz = clk::now();
                 size_t bound = ZSTD_compressBound(len);
-                uint8_t *z = (uint8_t *)std::malloc(bound ? bound : 1);
+                uint8_t *z = out_alloc(bound);
                 if (!z) {
                     zerr[f] = "out of host memory";
                     return;
                 }
-                size_t zl = ZSTD_compress(z, bound, src, len, 3);
+                size_t zl = zstd3(ctx, z, bound, src, len);
                 if (ZSTD_isError(zl)) {
-                    std::free(z);
+                    out_release(z);
                     zerr[f] = std::string("ZSTD_compress: ") + ZSTD_getErrorName(zl);
                     return;
                 }
@@ -3347,6 +3435,7 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
             size_t l1 = 0;
             frc = compress_entry(ctx, b.d_in, 1, b.dims, rel_eb, &p, plan_text, t_tables ? t_tables[f] : nullptr,
                                  t_tables ? t_lens[f] : 0, &o1, &l1, &r);
+            if (out[f]) out_release(out[f]);
             out[f] = o1;
             out_len[f] = l1;
             continue;
@@ -3374,7 +3463,7 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
     BR.encode_s = secs(t_enc, clk::now());
     if (frc) {
         for (uint32_t f = 0; f < nf; f++) {
-            std::free(out[f]);
+            if (out[f]) out_release(out[f]);
             out[f] = nullptr;
             out_len[f] = 0;
         }
@@ -3383,7 +3472,7 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
     for (uint32_t f = 0; f < nf; f++)
         if (!zerr[f].empty()) {
             for (uint32_t g = 0; g < nf; g++) {
-                std::free(out[g]);
+                if (out[g]) out_release(out[g]);
                 out[g] = nullptr;
                 out_len[g] = 0;
             }

@@ -10,6 +10,16 @@ size_t ZSTD_decompress(void *dst, size_t dstCapacity, const void *src, size_t co
 unsigned long long ZSTD_getFrameContentSize(const void *src, size_t srcSize);
 unsigned ZSTD_isError(size_t code);
 const char *ZSTD_getErrorName(size_t code);
+// Explicit contexts: ZSTD_compressCCtx compresses exactly as ZSTD_compress at the given level;
+// keeping a context avoids allocating and initialising one per call.
+typedef struct ZSTD_CCtx_s ZSTD_CCtx;
+typedef struct ZSTD_DCtx_s ZSTD_DCtx;
+ZSTD_CCtx *ZSTD_createCCtx(void);
+size_t ZSTD_freeCCtx(ZSTD_CCtx *cctx);
+size_t ZSTD_compressCCtx(ZSTD_CCtx *cctx, void *dst, size_t dstCapacity, const void *src, size_t srcSize, int compressionLevel);
+ZSTD_DCtx *ZSTD_createDCtx(void);
+size_t ZSTD_freeDCtx(ZSTD_DCtx *dctx);
+size_t ZSTD_decompressDCtx(ZSTD_DCtx *dctx, void *dst, size_t dstCapacity, const void *src, size_t srcSize);
 }
 
 #define ZSTD_CONTENTSIZE_UNKNOWN (0ULL - 1)

@@ -230,6 +230,10 @@ int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const uint64_t d
                    const asz_params *p, float *out, int out_on_device, asz_report *rep);
 
 void asz_free(void *ptr);
+/* asz_free keeps released output buffers (at most 64 of them, 2 GiB in all) for later outputs of
+ * the same or smaller size, whose memory is then already mapped. This frees them. No reference
+ * counterpart. */
+void asz_release_output_cache(void);
 
 /* Error statistics of the last asz_compress call on this context, as the reference prints them
  * after compressing (compress.tpp:307-319): max |x - x'| and PSNR in dB. The input buffer given

@@ -53,3 +53,26 @@ def test_cli_argument_errors(args, msg):
     r = subprocess.run([os.path.join(BIN, "s1_compress"), *args], capture_output=True, text=True)
     assert r.returncode == 1
     assert r.stderr.strip() == msg
+
+
+@pytest.mark.gpu
+def test_output_blocks_are_reused_and_released(gpu_ctx):
+    """Output buffers released with asz_free serve later outputs (single and batched calls give
+    the same bytes again), and asz_release_output_cache empties the cache between calls."""
+    import numpy as np
+
+    import asz_b200.api as api
+    from asz_b200 import fields
+    rng = np.random.default_rng(9)
+    a = fields.grf_field((40, 36, 44), 3.0, rng).astype(np.float32)
+    b = fields.grf_field((24, 30, 20), 2.0, rng).astype(np.float32)
+    p = api.default_params(block_pivot_ratio=3)
+    plan = "cubic0_012,cubic1_012,cubic2_012"
+    first = [gpu_ctx.compress(x, 1e-3, plan, "cubic", p)[0] for x in (a, b, a)]
+    assert first[0] == first[2]
+    again = [gpu_ctx.compress(x, 1e-3, plan, "cubic", p)[0] for x in (b, a)]
+    assert again == [first[1], first[0]]
+    blobs, _, _ = gpu_ctx.compress_batch([a, b], 1e-3, plan, "cubic", p)
+    assert blobs == [first[0], first[1]]
+    api.lib().asz_release_output_cache()
+    assert gpu_ctx.compress(a, 1e-3, plan, "cubic", p)[0] == first[0]
