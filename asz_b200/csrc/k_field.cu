@@ -297,7 +297,7 @@ __device__ __forceinline__ void reduce_range(int32_t lo, int32_t hi, int32_t *qb
 // kProbe: every axis divides, as the diagnostics instantiation that the predictor-family probe runs
 // does (one out-of-line clone for all axes), and pred_out receives each target's prediction.
 template <bool kProbe>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 3)
     round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
                           const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
                           int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out) {

@@ -29,10 +29,29 @@ __global__ void histogram_kernel(const T *__restrict__ s, uint64_t n, int64_t of
         for (uint64_t i = threadIdx.x; i < range; i += blockDim.x) sh[i] = 0;
         __syncthreads();
     }
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t v = (uint64_t)((int64_t)s[i] - offset);
-        if (use_sh) atomicAdd(&sh[v], 1u);
-        else atomicAdd(&hist[v], 1ull);
+    // A thread takes runs of kHistRun consecutive symbols and adds equal neighbours together:
+    // most symbols of a stream are a few values, often repeated, so this saves most atomics.
+    constexpr uint32_t kHistRun = 8;
+    auto add = [&](uint64_t v, uint32_t c) {
+        if (use_sh) atomicAdd(&sh[v], c);
+        else atomicAdd(&hist[v], (unsigned long long)c);
+    };
+    const uint64_t nruns = (n + kHistRun - 1) / kHistRun;
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nruns; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i0 = r * kHistRun, i1 = min(i0 + kHistRun, n);
+        uint64_t cur = (uint64_t)((int64_t)s[i0] - offset);
+        uint32_t c = 1;
+        for (uint64_t i = i0 + 1; i < i1; i++) {
+            const uint64_t v = (uint64_t)((int64_t)s[i] - offset);
+            if (v == cur) {
+                c++;
+            } else {
+                add(cur, c);
+                cur = v;
+                c = 1;
+            }
+        }
+        add(cur, c);
     }
     if (use_sh) {
         __syncthreads();
@@ -462,7 +481,7 @@ cudaError_t launch_histogram(const T *s, uint64_t n, int64_t offset, uint64_t ra
                              cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     size_t sh = range <= 8192 ? range * sizeof(unsigned int) : 0;
-    uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 8);
+    uint64_t blocks = std::min<uint64_t>((n + 8 * 256 - 1) / (8 * 256), 148 * 8);
     histogram_kernel<T><<<(unsigned)blocks, 256, sh, st>>>(s, n, offset, range, hist);
     count_launch();
     return cudaGetLastError();
