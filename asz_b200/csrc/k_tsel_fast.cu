@@ -25,7 +25,7 @@ struct GlobalSrc {
 // Selection of group g of one field and round: the fallbacks and overrides, the sample geometry
 // (get_AB_map.tpp:13-15), then fast_group. handoff(g) is called by thread 0 for a group the exact
 // path has to settle.
-template <class HandOff>
+template <int kT, class HandOff>
 __device__ void fast_one(GroupShared &sh, const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
                          const ClassInfo *__restrict__ classes, const float *__restrict__ rec, const float *__restrict__ orig,
                          const float *__restrict__ log2arena, float R2, float t_default, float *__restrict__ tval,
@@ -76,7 +76,7 @@ __device__ void fast_one(GroupShared &sh, const FieldGeom &fg, const RoundGeom &
     sg.c12 = SmallDiv{ci.cnt[1] * ci.cnt[2], ci.m12};
     const GlobalSrc src{sg, rec, orig, fg.n[1], fg.n[2], rg.dist, rg.neg_2_stat_eb};
     float t = 0.0f;
-    const uint32_t code = fast_group(sh, src, n, rg, log2arena + ci.log2_off, R2, why, t);
+    const uint32_t code = fast_group<GlobalSrc, kT>(sh, src, n, rg, log2arena + ci.log2_off, R2, why, t);
     if (tid == 0) {
         if (code == kFastDecided) {
             tval[g] = t;
@@ -95,7 +95,8 @@ struct ListHandOff {
 // One CTA per (block, round) group at a time (persistent grid). list_out receives the groups this
 // path could not settle; why[0] counts those whose bins span too many windows, why[1] those with an
 // undecidable comparison; why[2] counts the groups settled here by window-by-window counting.
-__global__ void __launch_bounds__(kThreads, 16)
+template <int kT>
+__global__ void __launch_bounds__(kT, kT == 64 ? 16 : 8)
     tsel_fast_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
                      const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
                      float R2, float t_default, float *__restrict__ tval, int64_t *__restrict__ t_int,
@@ -104,11 +105,11 @@ __global__ void __launch_bounds__(kThreads, 16)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupShared &sh = *reinterpret_cast<GroupShared *>(smem_raw);
     const uint64_t nblocks = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    for (int i = threadIdx.x; i < 5 * kWinWords; i += kThreads) (&sh.hist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < 5 * kWinWords; i += kT) (&sh.hist[0][0])[i] = 0;
     __syncthreads();
     const ListHandOff ho{list_out, list_count};
     for (uint64_t g = blockIdx.x; g < nblocks; g += gridDim.x) {
-        fast_one(sh, fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int, fb_count, overrides, n_overrides,
+        fast_one<kT>(sh, fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int, fb_count, overrides, n_overrides,
                  why, g, ho);
         __syncthreads();
     }
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 16)
         const uint32_t f = field_of(goff, nf, gi);
         const BatchField &B = F[f];
         const PairHandOff ho{handoff_list, handoff_count, f};
-        fast_one(sh, B.fg, B.rounds[l], l, B.classes + 27 * l, B.rec, B.in, log2arena, B.R2, t_default, B.tval, B.tint,
+        fast_one<kThreads>(sh, B.fg, B.rounds[l], l, B.classes + 27 * l, B.rec, B.in, log2arena, B.R2, t_default, B.tval, B.tint,
                  &B.cnt->fb, nullptr, 0, B.cnt->why, gi - goff[f], ho);
         __syncthreads();
     }
@@ -167,11 +168,20 @@ cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t 
     uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     uint64_t blocks = nb < 148 * 8 * 4 ? nb : 148 * 8 * 4;
     const int smem = (int)sizeof(GroupShared);
-    cudaError_t e = cudaFuncSetAttribute(tsel_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // Many groups: 64-thread CTAs, 16 per SM (fewer warps wait at each block barrier). Fewer
+    // groups than four waves of those: 128-thread CTAs, which finish each group sooner.
+    const bool wide = nb < 148 * 16 * 4;
+    cudaError_t e = wide ? cudaFuncSetAttribute(tsel_fast_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                         : cudaFuncSetAttribute(tsel_fast_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    tsel_fast_kernel<<<(unsigned)blocks, kThreads, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
-                                                              t_int, fb_count, list_out, list_count, overrides, n_overrides,
-                                                              why);
+    if (wide)
+        tsel_fast_kernel<128><<<(unsigned)blocks, 128, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
+                                                                  t_int, fb_count, list_out, list_count, overrides,
+                                                                  n_overrides, why);
+    else
+        tsel_fast_kernel<64><<<(unsigned)blocks, 64, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
+                                                                t_int, fb_count, list_out, list_count, overrides,
+                                                                n_overrides, why);
     count_launch();
     return cudaGetLastError();
 }

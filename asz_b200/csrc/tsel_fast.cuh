@@ -119,22 +119,25 @@ __device__ __forceinline__ uint64_t fast_sample_pos(const FastSampleGeo &sg, uin
     return (i0 * n1 + i1) * n2 + i2;
 }
 
+// Threads per group: kThreads by default; the per-round kernel also has a 128-thread form for
+// rounds with few groups, where the shorter per-group time of more threads wins.
 constexpr int kThreads = 64;
-constexpr int kWarps = kThreads / 32;
+constexpr int kMaxWarps = 4;
 
 // Shared state of one group (one CTA).
 struct GroupShared {
     uint32_t hist[5][kWinWords];
     Interval psnr[5];
-    float fmin[kWarps][2], fmax[kWarps][2];
-    double dsum[kWarps][5];
-    uint32_t cnt[kWarps][5];
-    uint32_t flag[kWarps];
+    float fmin[kMaxWarps][2], fmax[kMaxWarps][2];
+    double dsum[kMaxWarps][5];
+    uint32_t cnt[kMaxWarps][5];
+    uint32_t flag[kMaxWarps];
     uint32_t res_code;  // outcome of fast_group, broadcast to the CTA
     float res_t;
 };
 
-// Block-wide reductions over kThreads threads; every thread receives the result.
+// Block-wide reductions over kT threads; every thread receives the result.
+template <int kT>
 __device__ __forceinline__ void block_minmax(GroupShared &sh, float &amin, float &amax, float &bmin, float &bmax) {
     for (int o = 16; o; o >>= 1) {
         amin = fminf(amin, __shfl_xor_sync(0xffffffffu, amin, o));
@@ -154,7 +157,7 @@ __device__ __forceinline__ void block_minmax(GroupShared &sh, float &amin, float
     bmin = sh.fmin[0][1];
     amax = sh.fmax[0][0];
     bmax = sh.fmax[0][1];
-    for (int i = 1; i < kWarps; i++) {
+    for (int i = 1; i < kT / 32; i++) {
         amin = fminf(amin, sh.fmin[i][0]);
         bmin = fminf(bmin, sh.fmin[i][1]);
         amax = fmaxf(amax, sh.fmax[i][0]);
@@ -164,7 +167,7 @@ __device__ __forceinline__ void block_minmax(GroupShared &sh, float &amin, float
 
 // Sums of nv doubles and nv counts per thread, and the OR of a flag word. Fixed order (warp tree, then
 // warps in index order), so every thread gets the same bits.
-template <int NV>
+template <int kT, int NV>
 __device__ __forceinline__ void block_sums(GroupShared &sh, double (&v)[NV], uint32_t (&c)[NV], uint32_t &flag) {
 #pragma unroll
     for (int i = 0; i < NV; i++)
@@ -187,13 +190,13 @@ __device__ __forceinline__ void block_sums(GroupShared &sh, double (&v)[NV], uin
     for (int i = 0; i < NV; i++) {
         v[i] = sh.dsum[0][i];
         c[i] = sh.cnt[0][i];
-        for (int k = 1; k < kWarps; k++) {
+        for (int k = 1; k < kT / 32; k++) {
             v[i] += sh.dsum[k][i];
             c[i] += sh.cnt[k][i];
         }
     }
     flag = sh.flag[0];
-    for (int k = 1; k < kWarps; k++) flag |= sh.flag[k];
+    for (int k = 1; k < kT / 32; k++) flag |= sh.flag[k];
     __syncthreads();  // the staging arrays are reused by the next reduction
 }
 
@@ -202,13 +205,13 @@ enum : uint32_t { kFastDecided = 0, kFastHandoff = 1 };
 // Selects t for one group of n samples (n < 65536). Src::keys(s, af, bf, nz) gives the keys of
 // sample s. Every thread of the CTA calls this and gets the same result: kFastDecided with t_out,
 // or kFastHandoff when the exact path has to decide. The histograms are left zeroed.
-template <class Src>
+template <class Src, int kT = kThreads>
 __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, const RoundGeom &rg, const float *l2, float R2,
                                uint32_t *why, float &t_out) {
     const uint32_t tid = threadIdx.x;
     const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
     const float eb = rg.eb, neg_eb = __fdiv_rn(0.5f, eb), eb2 = __fadd_rn(eb, eb);
-    // Window placement from the first kThreads samples (one per thread): their bin range per
+    // Window placement from the first kT samples (one per thread): their bin range per
     // candidate, centred in the window. A group whose samples overflow the window is redone
     // with the exact ranges of all samples.
     // Each thread's first two samples are loaded together and kept for the main pass.
@@ -217,11 +220,11 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
     float afmin = INFINITY, afmax = -INFINITY, bfmin = INFINITY, bfmax = -INFINITY;
     if (tid < n) {
         src.keys(tid, af0, bf0, nz0);
-        if (tid + kThreads < n) src.keys(tid + kThreads, af1, bf1, nz1);
+        if (tid + kT < n) src.keys(tid + kT, af1, bf1, nz1);
         afmin = afmax = af0;
         bfmin = bfmax = bf0;
     }
-    block_minmax(sh, afmin, afmax, bfmin, bfmax);
+    block_minmax<kT>(sh, afmin, afmax, bfmin, bfmax);
     int64_t qlo[5];
     bool fits = true;
     for (int c = 0; c < 5; c++) {
@@ -240,7 +243,7 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
             afmin = bfmin = INFINITY;
             afmax = bfmax = -INFINITY;
             double ab[2] = {0.0, 0.0};
-            for (uint32_t s = tid; s < n; s += kThreads) {
+            for (uint32_t s = tid; s < n; s += kT) {
                 float af, bf;
                 bool nz;
                 src.keys(s, af, bf, nz);
@@ -251,9 +254,9 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
                 ab[0] += (double)af;
                 ab[1] += (double)bf;
             }
-            block_minmax(sh, afmin, afmax, bfmin, bfmax);
+            block_minmax<kT>(sh, afmin, afmax, bfmin, bfmax);
             uint32_t dummy[2] = {0, 0}, none = 0;
-            block_sums<2>(sh, ab, dummy, none);
+            block_sums<kT, 2>(sh, ab, dummy, none);
             for (int c = 0; c < 5; c++) {
                 const float t2 = __fadd_rn(cand[c], cand[c]);
                 const int64_t q0 = lround_f(__fmul_rn(cand_err(afmin, bfmin, t2, rg.stat_eb), neg_eb));
@@ -272,14 +275,14 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
         for (int c = 0; c < 5; c++) S[c] = 0.0;
         anz = 0;
         out = 0;
-        for (uint32_t s = tid; s < n; s += kThreads) {
+        for (uint32_t s = tid; s < n; s += kT) {
             float af, bf;
             bool nz;
             if (s == tid) {
                 af = af0;
                 bf = bf0;
                 nz = nz0;
-            } else if (s == tid + kThreads) {
+            } else if (s == tid + kT) {
                 af = af1;
                 bf = bf1;
                 nz = nz1;
@@ -303,12 +306,12 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
         {
             // One reduction: S, and the OR of the flags (overflow in bit 0, a nonzero A key in bit 1).
             uint32_t flags = out | (anz << 1), dummy[5] = {0, 0, 0, 0, 0};
-            block_sums<5>(sh, S, dummy, flags);
+            block_sums<kT, 5>(sh, S, dummy, flags);
             out = flags & 1u;
             anz = (flags >> 1) & 1u;
         }
         if (out || !anz) {
-            for (int i = tid; i < 5 * kWinWords; i += kThreads) (&sh.hist[0][0])[i] = 0;
+            for (int i = tid; i < 5 * kWinWords; i += kT) (&sh.hist[0][0])[i] = 0;
             __syncthreads();
         }
         if (!anz) break;
@@ -347,7 +350,7 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
             double h = 0.0;
             uint32_t k = 0;
             for (int64_t lo = q0c[c];; lo += kWide) {
-                for (uint32_t s = tid; s < n; s += kThreads) {
+                for (uint32_t s = tid; s < n; s += kT) {
                     float af, bf;
                     bool nz;
                     src.keys(s, af, bf, nz);
@@ -356,7 +359,7 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
                     if (bin < (uint64_t)kWide) atomicAdd(&flat[bin >> 1], 1u << (16 * (bin & 1)));
                 }
                 __syncthreads();
-                for (int i = tid; i < kWide / 2; i += kThreads) {
+                for (int i = tid; i < kWide / 2; i += kT) {
                     const uint32_t w = flat[i];
                     if (w) {
                         const uint32_t c0 = w & 0xffffu, c1 = w >> 16;
@@ -385,7 +388,7 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
         for (int c = 0; c < 5; c++) {
             double h = 0.0;
             uint32_t k = 0;
-            for (int i = tid; i < kWinWords; i += kThreads) {
+            for (int i = tid; i < kWinWords; i += kT) {
                 uint32_t w = sh.hist[c][i];
                 if (w) {
                     uint32_t c0 = w & 0xffffu, c1 = w >> 16;
@@ -408,7 +411,7 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
     }
     {
         uint32_t none = 0;
-        block_sums<5>(sh, H, mq, none);
+        block_sums<kT, 5>(sh, H, mq, none);
     }
     if (tid < 32) {
         // PSNR intervals of the five candidates in parallel, then the decision chain
