@@ -62,10 +62,21 @@ bool build_code(const std::vector<uint64_t> &hist, int64_t min_sym, int64_t max_
     // weights come out nondecreasing and internal nodes are numbered after all leaves, so the
     // leaves sorted by (frequency, index) and a FIFO of internal nodes in creation order give
     // the same pops: at each step take the smaller front, the leaf on a frequency tie.
-    std::vector<uint32_t> order(n);
-    for (uint64_t i = 0; i < n; i++) order[i] = (uint32_t)i;
-    std::sort(order.begin(), order.end(),
-              [&](uint32_t a, uint32_t b) { return freq[a] != freq[b] ? freq[a] < freq[b] : a < b; });
+    // Leaves in (frequency, index) order: a stable radix sort on the frequency, one byte per
+    // pass over the bytes that are not zero in every frequency, from leaves in index order.
+    std::vector<uint32_t> order(n), tmp(n);
+    uint64_t maxf = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        order[i] = (uint32_t)i;
+        maxf = std::max(maxf, freq[i]);
+    }
+    for (unsigned shift = 0; shift < 64 && (maxf >> shift) != 0; shift += 8) {
+        uint64_t cnt[257] = {0};
+        for (uint64_t i = 0; i < n; i++) cnt[((freq[order[i]] >> shift) & 255u) + 1]++;
+        for (int b = 0; b < 256; b++) cnt[b + 1] += cnt[b];
+        for (uint64_t i = 0; i < n; i++) tmp[cnt[(freq[order[i]] >> shift) & 255u]++] = order[i];
+        order.swap(tmp);
+    }
     std::vector<uint64_t> ifreq;
     ifreq.reserve(n);
     uint64_t ia = 0, ib = 0;
