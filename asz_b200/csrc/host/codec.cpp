@@ -28,6 +28,9 @@
 #include <unordered_map>
 #include <random>
 #include <string>
+#include <condition_variable>
+#include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -105,6 +108,67 @@ struct Geometry {
 
 }  // namespace
 
+namespace {
+// Worker threads kept for a context's host-side parallel loops: run(n, f) calls f(0..n-1) on the
+// workers and the calling thread, and returns when all calls have returned.
+class HostPool {
+public:
+    explicit HostPool(unsigned workers) {
+        for (unsigned i = 0; i < workers; i++) th_.emplace_back([this] { loop(); });
+    }
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void run(uint64_t n, const std::function<void(uint64_t)> &f) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            fn_ = &f;
+            n_ = n;
+            next_ = 0;
+            active_ = th_.size();
+            ++gen_;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> l(mu_);
+        done_.wait(l, [&] { return active_ == 0; });
+        fn_ = nullptr;
+    }
+
+private:
+    void work() {
+        for (uint64_t j; (j = next_.fetch_add(1)) < n_;) (*fn_)(j);
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> l(mu_);
+                cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            work();
+            std::lock_guard<std::mutex> g(mu_);
+            if (--active_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(uint64_t)> *fn_ = nullptr;
+    std::atomic<uint64_t> next_{0};
+    uint64_t n_ = 0, gen_ = 0;
+    size_t active_ = 0;
+    bool stop_ = false;
+};
+}  // namespace
+
 struct asz_ctx {
     int device = 0;
     cudaStream_t own = nullptr, stream = nullptr;
@@ -162,6 +226,8 @@ struct asz_ctx {
     std::mutex zmu;
     std::vector<ZSTD_CCtx *> zfree;
     ZSTD_DCtx *zd = nullptr;
+    // Host worker threads for the code builds (created on first use).
+    std::unique_ptr<HostPool> pool;
 };
 
 namespace {
@@ -1938,16 +2004,11 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
                                 code_err[j]);
         o.lo += (int64_t)a0;
     };
-    {
-        const u64 nthreads = std::min<u64>(jobs.size(), std::max(1u, std::thread::hardware_concurrency()));
-        std::atomic<u64> next{0};
-        std::vector<std::thread> pool;
-        for (u64 t = 1; t < nthreads; t++)
-            pool.emplace_back([&]() {
-                for (u64 j; (j = next.fetch_add(1)) < jobs.size();) build_one(j);
-            });
-        for (u64 j; (j = next.fetch_add(1)) < jobs.size();) build_one(j);
-        for (auto &t : pool) t.join();
+    if (jobs.size() > 1) {
+        if (!ctx->pool) ctx->pool = std::make_unique<HostPool>(std::min(15u, std::max(1u, std::thread::hardware_concurrency()) - 1));
+        ctx->pool->run(jobs.size(), build_one);
+    } else if (jobs.size() == 1) {
+        build_one(0);
     }
     for (u64 j = 0; j < jobs.size(); j++)
         if (!code_ok[j]) return fail(ctx, ASZ_E_UNSUPPORTED, code_err[j]);
