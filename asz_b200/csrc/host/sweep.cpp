@@ -42,9 +42,17 @@ namespace {
 using u64 = uint64_t;
 using clk = std::chrono::steady_clock;
 
+// Per host worker: the framed stream, the zstd output and a zstd context, kept across rows and
+// calls so that their pages are mapped once (first writes to fresh pages cost as much as zstd).
+struct WorkerScratch {
+    std::vector<uint8_t> buf, z;
+    ZSTD_CCtx *cc = nullptr;
+};
+
 struct SweepState {
     DevBuf coef, qb, part, sums, mm, hist, first, tab, pay, enc, cub;
     PinnedBuf small, counts, payload;
+    std::vector<WorkerScratch> ws;
 };
 
 struct Predictor {
@@ -211,19 +219,21 @@ void finish_row(asz_sweep_row &r, double range) {  // s2_many_prediction.cpp:423
     r.psnr = 10 * std::log10((range * range / r.mse_sum) * S);
 }
 
+u64 host_workers() { return std::max(1u, std::thread::hardware_concurrency()); }
+
+// f(i, w) for i in [0, n) on up to host_workers() threads; w is the calling worker's index.
 template <class F>
 void parallel_for(u64 n, F f) {
-    const u64 hw = std::max(1u, std::thread::hardware_concurrency());
-    const u64 nt = std::min<u64>(hw, n);
+    const u64 nt = std::min<u64>(host_workers(), n);
     if (nt <= 1) {
-        for (u64 i = 0; i < n; i++) f(i);
+        for (u64 i = 0; i < n; i++) f(i, 0);
         return;
     }
     std::atomic<u64> next{0};
     std::vector<std::thread> th;
     for (u64 t = 0; t < nt; t++)
-        th.emplace_back([&] {
-            for (u64 i; (i = next.fetch_add(1)) < n;) f(i);
+        th.emplace_back([&, t] {
+            for (u64 i; (i = next.fetch_add(1)) < n;) f(i, t);
         });
     for (auto &t : th) t.join();
 }
@@ -248,6 +258,8 @@ void sweep_release(void *state) {
     s->small.release();
     s->counts.release();
     s->payload.release();
+    for (WorkerScratch &w : s->ws)
+        if (w.cc) ZSTD_freeCCtx(w.cc);
     delete s;
 }
 }  // namespace asz::host
@@ -401,7 +413,7 @@ extern "C" int asz_sweep(asz_ctx *ctx, const float *data, int on_device, const u
             std::vector<double> h1(kc);
             std::vector<std::string> cerr(kc);
             std::vector<char> ok(kc, 1);
-            parallel_for(kc, [&](u64 k) {
+            parallel_for(kc, [&](u64 k, u64) {
                 const u64 r = hoff[k + 1] - hoff[k];
                 std::vector<u64> hv(h_hist + hoff[k], h_hist + hoff[k] + r);
                 ok[k] = build_code(hv, h_mm[2 * k], h_mm[2 * k + 1], S, true, code[k], cerr[k]);
@@ -452,17 +464,21 @@ extern "C" int asz_sweep(asz_ctx *ctx, const float *data, int on_device, const u
             // Frame each stream (save + encode, huffman.hpp) and compress it with zstd level 3.
             std::vector<u64> hb(kc), zb(kc);
             std::vector<char> zok(kc, 1);
-            parallel_for(kc, [&](u64 k) {
+            if (W.ws.size() < host_workers()) W.ws.resize(host_workers());
+            parallel_for(kc, [&](u64 k, u64 w) {
                 const HuffCode &c = code[k];
-                const u64 pay = c.maxval == 1 ? 0 : (c.bits + 7) / 8;
-                std::vector<uint8_t> buf(c.save_size() + 8 + pay);
-                write_tree(c, buf.data());
-                write_len_word(c, buf.data() + c.save_size());
-                if (pay) std::memcpy(buf.data() + c.save_size() + 8, W.payload.p + word_off[k] * 4, pay);
-                std::vector<uint8_t> z(ZSTD_compressBound(buf.size()));
-                const size_t n = ZSTD_compress(z.data(), z.size(), buf.data(), buf.size(), 3);
+                WorkerScratch &sc = W.ws[w];
+                const u64 pay = c.maxval == 1 ? 0 : (c.bits + 7) / 8, len = c.save_size() + 8 + pay;
+                if (sc.buf.size() < len) sc.buf.resize(len);
+                write_tree(c, sc.buf.data());
+                write_len_word(c, sc.buf.data() + c.save_size());
+                if (pay) std::memcpy(sc.buf.data() + c.save_size() + 8, W.payload.p + word_off[k] * 4, pay);
+                if (sc.z.size() < ZSTD_compressBound(len)) sc.z.resize(ZSTD_compressBound(len));
+                if (!sc.cc) sc.cc = ZSTD_createCCtx();
+                const size_t n = sc.cc ? ZSTD_compressCCtx(sc.cc, sc.z.data(), sc.z.size(), sc.buf.data(), len, 3)
+                                       : ZSTD_compress(sc.z.data(), sc.z.size(), sc.buf.data(), len, 3);
                 zok[k] = !ZSTD_isError(n);
-                hb[k] = buf.size();
+                hb[k] = len;
                 zb[k] = n;
             });
             const double enc_s = std::chrono::duration<double>(clk::now() - t_enc).count();
