@@ -166,7 +166,7 @@ cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t 
                              int64_t *t_int, uint32_t *fb_count, uint32_t *list_out, uint32_t *list_count,
                              const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st) {
     uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    uint64_t blocks = nb < 148 * 8 * 4 ? nb : 148 * 8 * 4;
+    uint64_t blocks = nb < 148 * 16 * 4 ? nb : 148 * 16 * 4;
     const int smem = (int)sizeof(GroupShared);
     // Many groups: 64-thread CTAs, 16 per SM (fewer warps wait at each block barrier). Fewer
     // groups than four waves of those: 128-thread CTAs, which finish each group sooner.
