@@ -2637,16 +2637,55 @@ extern "C" int asz_decompress(asz_ctx *ctx, const uint8_t *in, size_t len, const
         return true;
     };
     std::vector<HuffParsed> hp(L + 2);
-    std::vector<u64> counts(L + 2);
+    std::vector<u64> counts(L + 2), sbeg(L + 2, 0), send(L + 2, 0);
+    // Stream boundaries from the headers alone: a tree takes n (mbft + 2) - 1 bits and a payload
+    // the bits its length word gives (none for a single symbol), so every stream's start is known
+    // before any tree is read (huffman.hpp:322-338).
+    auto be64 = [&](u64 at) {
+        u64 v = 0;
+        for (int i = 0; i < 8; i++) v = (v << 8) | bsp[at + i];
+        return v;
+    };
     for (u64 s = 0; s < L + 2; s++) {
         if (!rd64(counts[s])) return fail(ctx, ASZ_E_DATA, "truncated stream length");
         if (!counts[s]) continue;
-        std::string e;
-        if (!parse_stream(bsp, raw, pos, hp[s], e)) return fail(ctx, ASZ_E_DATA, e);
-        // Every code is at least one bit, and a single-symbol stream still has to fit the field's
-        // bookkeeping: larger counts are corrupt (and would overflow the output sizing).
-        if (hp[s].single ? counts[s] > (1ull << 40) : counts[s] > hp[s].payload_bits)
-            return fail(ctx, ASZ_E_DATA, "compressed stream has an impossible value count");
+        if (pos > raw || raw - pos < 25) return fail(ctx, ASZ_E_DATA, "truncated Huffman header");
+        const unsigned mbft = bsp[pos] & 0x3f;
+        const u64 n = be64(pos + 9), maxval = be64(pos + 17);
+        if (n == 0) return fail(ctx, ASZ_E_DATA, "Huffman stream with no symbols");
+        if (n > 1 && (mbft == 0 || mbft > 63 || n > (1ull << 31))) return fail(ctx, ASZ_E_DATA, "corrupt Huffman tree header");
+        const u64 tree = n > 1 ? (n * (mbft + 2) - 1 + 7) / 8 : 0;
+        sbeg[s] = pos;
+        if (raw - pos - 25 < tree + 8) return fail(ctx, ASZ_E_DATA, "truncated Huffman payload");
+        u64 q = pos + 25 + tree;
+        const u64 w = be64(q) ^ 0x1234abcdull;
+        q += 8;
+        if (n > 1 && maxval != 1) {
+            if (w > (raw - q) * 8) return fail(ctx, ASZ_E_DATA, "truncated Huffman payload");
+            q += (w + 7) / 8;
+        }
+        send[s] = pos = q;
+    }
+    // Trees and lookup tables on the context's worker threads; each stream must end where the
+    // next one starts.
+    {
+        std::vector<std::string> perr(L + 2);
+        std::vector<char> pok(L + 2, 1);
+        auto parse_one = [&](uint64_t s) {
+            if (!counts[s]) return;
+            u64 at = sbeg[s];
+            pok[s] = parse_stream(bsp, raw, at, hp[s], perr[s]) && at == send[s];
+            if (!pok[s] && perr[s].empty()) perr[s] = "corrupt Huffman stream";
+        };
+        if (!ctx->pool) ctx->pool = std::make_unique<HostPool>(std::min(15u, std::max(1u, std::thread::hardware_concurrency()) - 1));
+        ctx->pool->run(L + 2, parse_one);
+        for (u64 s = 0; s < L + 2; s++) {
+            if (!pok[s]) return fail(ctx, ASZ_E_DATA, perr[s]);
+            // Every code is at least one bit, and a single-symbol stream still has to fit the
+            // field's bookkeeping: larger counts are corrupt (and would overflow the output sizing).
+            if (counts[s] && (hp[s].single ? counts[s] > (1ull << 40) : counts[s] > hp[s].payload_bits))
+                return fail(ctx, ASZ_E_DATA, "compressed stream has an impossible value count");
+        }
     }
     const float abs_eb = rel_eb * (mx - mn);
     Geometry G;
