@@ -743,10 +743,10 @@ def grad_tune_section(ctx, L, dev, rank, barrier):
 # doubled for the 512^3 field (the traffic grows with the number of values).
 # huff_encode is one scope of two launches (tile bit counts, then packing) per compression.
 TRAFFIC_PER_LAUNCH = {
-    "tsel_fast": 2 * (292.07e6 + 30.53e6),
-    "round_compress": 2 * (349.17e6 + 112.09e6),
-    "round_decompress": 2 * (212.82e6 + 92.56e6),
-    "huff_encode": 2 * (268.67e6 + 0.15e6 + 270.14e6 + 39.48e6),
+    "tsel_fast": 2 * (292.08e6 + 31.40e6),
+    "round_compress": 2 * (356.46e6 + 112.61e6),
+    "round_decompress": 2 * (215.93e6 + 92.74e6),
+    "huff_encode": 2 * (268.67e6 + 0.22e6 + 270.10e6 + 39.89e6),
 }
 
 
