@@ -166,6 +166,21 @@ def _is_cuda_tensor(x):
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
 
 
+def _check_device_field(x, device: int, what: str, numel: int | None = None):
+    """Refuse a CUDA tensor the library would misread: it must be float32, contiguous, on the
+    context's device and, when numel is given, hold exactly that many values. The library reads
+    and writes such buffers through raw pointers, so a mismatch would run past the tensor."""
+    import torch
+    if x.dtype != torch.float32:
+        raise ValueError(f"{what} must be a float32 tensor, not {x.dtype}")
+    if not x.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    if x.device.index != device:
+        raise ValueError(f"{what} is on {x.device}, the context uses cuda:{device}")
+    if numel is not None and x.numel() != numel:
+        raise ValueError(f"{what} holds {x.numel()} values, the shape needs {numel}")
+
+
 def error_stats_noalloc(x, y, value_range: float):
     """max |x - y| and PSNR of two equal-size float32 CUDA tensors, computed without allocating
     (fixed library scratch). Runs on torch's current stream of x's device; returns (max_err, psnr)."""
@@ -229,9 +244,7 @@ class Context:
         n = C.c_size_t(0)
         rep = Report()
         if _is_cuda_tensor(data):
-            import torch
-            if data.dtype != torch.float32 or not data.is_contiguous():
-                raise ValueError("device input must be a contiguous float32 tensor")
+            _check_device_field(data, self.device, "device input")
             self._use_torch_stream(data)
             rc = self._L.asz_compress(self._c, C.c_void_p(data.data_ptr()), 1, _dims(data.shape), C.c_float(rel_eb),
                                       C.byref(p), plan.encode() if plan else None, C.byref(out), C.byref(n), C.byref(rep))
@@ -251,8 +264,15 @@ class Context:
         """Decompress .asz bytes; returns a NumPy array, or fills the CUDA tensor `out`."""
         p = params if params is not None else default_params()
         rep = Report()
+        numel = 1
+        for s_ in shape:
+            numel *= int(s_)
+        if out is not None:
+            if not _is_cuda_tensor(out):
+                raise ValueError("out must be a CUDA tensor (omit it to get a NumPy array)")
+            _check_device_field(out, self.device, "out", numel)
         buf = C.create_string_buffer(bytes(blob), len(blob))
-        if out is not None and _is_cuda_tensor(out):
+        if out is not None:
             self._use_torch_stream(out)
             rc = self._L.asz_decompress(self._c, buf, len(blob), _dims(shape), C.c_float(rel_eb), C.byref(p),
                                         C.c_void_p(out.data_ptr()), 1, C.byref(rep))
@@ -277,6 +297,7 @@ class Context:
         n = C.c_size_t(0)
         rep = Report()
         if _is_cuda_tensor(data):
+            _check_device_field(data, self.device, "device input")
             self._use_torch_stream(data)
             rc = self._L.asz_compress_with_t(self._c, C.c_void_p(data.data_ptr()), 1, _dims(data.shape), C.c_float(rel_eb),
                                              C.byref(p), plan.encode(), C.c_void_p(codes.ctypes.data), codes.size,
@@ -308,9 +329,11 @@ class Context:
         on_dev = _is_cuda_tensor(fields[0])
         for i, x in enumerate(fields):
             if on_dev:
-                import torch
-                if x.dtype != torch.float32 or not x.is_contiguous():
-                    raise ValueError("device inputs must be contiguous float32 tensors")
+                if not _is_cuda_tensor(x):
+                    raise ValueError("fields must be all CUDA tensors or all host arrays")
+                _check_device_field(x, self.device, f"device input {i}")
+                if x.device != fields[0].device:
+                    raise ValueError("device inputs must share one device")
                 ptrs[i] = x.data_ptr()
             else:
                 a = np.ascontiguousarray(x, dtype=np.float32)

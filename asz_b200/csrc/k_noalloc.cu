@@ -16,7 +16,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/asz_b200.h"
 
@@ -26,7 +25,6 @@ constexpr size_t kScratchBytes = 1u << 20;
 constexpr size_t kControlBytes = 256;
 constexpr uint64_t kTile = 1u << 16;  // elements per tile (one CTA each)
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 struct Partial {
     float max;
@@ -109,10 +107,6 @@ void set_err(char *err, size_t err_len, const char *msg) {
     if (err && err_len) std::snprintf(err, err_len, "%s", msg);
 }
 
-unsigned char *g_scratch_ptr[kMaxDevices];
-cudaError_t g_scratch_rc[kMaxDevices];
-std::once_flag g_scratch_once[kMaxDevices];
-
 }  // namespace
 
 extern "C" int asz_error_stats_noalloc(const float *x, const float *y, uint64_t n, double value_range, void *cuda_stream,
@@ -131,21 +125,24 @@ extern "C" int asz_error_stats_noalloc(const float *x, const float *y, uint64_t 
         return ASZ_E_ARG;
     }
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         set_err(err, err_len, "error_stats_noalloc: no usable current CUDA device");
         return ASZ_E_CUDA;
     }
-    // First call on this device: look up the scratch array's address once.
-    std::call_once(g_scratch_once[dev], [dev] {
-        void *p = nullptr;
-        g_scratch_rc[dev] = cudaGetSymbolAddress(&p, g_stats_scratch);
-        g_scratch_ptr[dev] = (unsigned char *)p;
-    });
-    if (g_scratch_rc[dev] != cudaSuccess || !g_scratch_ptr[dev]) {
-        set_err(err, err_len, "error_stats_noalloc: cudaGetSymbolAddress failed for the scratch array");
+    // The array's device address in the current device's context. Host code cannot use the
+    // symbol g_stats_scratch itself (it names a host-side shadow), so the address is looked up
+    // on every call: the lookup allocates nothing, a failed lookup is not remembered, and a
+    // context created after a device reset gets its own address.
+    void *sym = nullptr;
+    const cudaError_t se = cudaGetSymbolAddress(&sym, g_stats_scratch);
+    if (se != cudaSuccess || !sym) {
+        char m[160];
+        std::snprintf(m, sizeof(m), "error_stats_noalloc: cudaGetSymbolAddress failed for the scratch array: %s",
+                      cudaGetErrorString(se));
+        set_err(err, err_len, m);
         return ASZ_E_CUDA;
     }
-    unsigned char *scratch = g_scratch_ptr[dev];
+    unsigned char *scratch = (unsigned char *)sym;
     cudaStream_t st = (cudaStream_t)cuda_stream;
     Control h;
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(Control), st);

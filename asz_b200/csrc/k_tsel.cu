@@ -118,7 +118,10 @@ __device__ uint32_t build_abmap(const SampleBox &box, const FieldRef &f, Scratch
                 int64_t bk = lround_f(__fmul_rn(B, box.neg_2_stat_eb));
                 uint64_t h = mix64((uint64_t)ak * 0x9e3779b97f4a7c15ull ^ (uint64_t)bk);
                 uint32_t slot = (uint32_t)(h & (s.tcap - 1));
-                while (true) {
+                // Linear probing over tcap > cap slots finds a free one within tcap probes; a
+                // longer walk means the table is inconsistent, reported like an overflow.
+                for (uint32_t probe = 0;; probe++) {
+                    if (probe >= s.tcap) return UINT32_MAX;
                     int32_t e = s.tab[slot];
                     if (e == kNil) {
                         if (m >= s.cap) return UINT32_MAX;
@@ -148,8 +151,9 @@ __device__ uint32_t build_abmap(const SampleBox &box, const FieldRef &f, Scratch
     return m;
 }
 
-// get_h1_psnr (get_h_psnr.tpp:6-31) as emitted. Writes h1 and the log10f argument x.
-__device__ void eval_proxy(Scratch &s, uint32_t m, float t, float abs_eb, float stat_eb, float R2,
+// get_h1_psnr (get_h_psnr.tpp:6-31) as emitted. Writes h1 and the log10f argument x. Returns
+// false if the bin table is inconsistent (no free slot within tcap probes).
+__device__ bool eval_proxy(Scratch &s, uint32_t m, float t, float abs_eb, float stat_eb, float R2,
                            const float *log2tab, float &h1_out, float &x_out) {
     const float neg_2_eb = __fdiv_rn(0.5f, abs_eb);
     const float t2 = __fadd_rn(t, t), eb2 = __fadd_rn(abs_eb, abs_eb);
@@ -165,8 +169,8 @@ __device__ void eval_proxy(Scratch &s, uint32_t m, float t, float abs_eb, float 
         float err = __fmul_rn(__fmaf_rn(bf, 2.0f, __fmul_rn(af, t2)), stat_eb);
         int64_t qb = lround_f(__fmul_rn(err, neg_2_eb));
         uint32_t slot = (uint32_t)(mix64((uint64_t)qb) & (s.tcap - 1));
-        int32_t node;
-        while (true) {
+        int32_t node = -1;
+        for (uint32_t probe = 0; probe < s.tcap; probe++) {
             int32_t q = s.qtab[slot];
             if (q == kNil) {
                 node = (int32_t)mq++;
@@ -182,6 +186,7 @@ __device__ void eval_proxy(Scratch &s, uint32_t m, float t, float abs_eb, float 
             }
             slot = (slot + 1) & (s.tcap - 1);
         }
+        if (node < 0) return false;
         uint32_t c = s.cnt[e];
         s.qc[node] += c;
         float de = __fmaf_rn(-__ll2float_rn(qb), eb2, err);
@@ -200,6 +205,7 @@ __device__ void eval_proxy(Scratch &s, uint32_t m, float t, float abs_eb, float 
     }
     h1_out = h1;
     x_out = __fmul_rn(__fdiv_rn(R2, mse), nf);
+    return true;
 }
 
 // psnr = 10*log10f(x): the float value from a double-precision log10, and bounds that cover
@@ -291,7 +297,11 @@ __device__ void v0_one(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, con
             // The five distinct t values of block_candidate_t (asz_param.hpp:203).
             const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
             float h1v[5], xv[5];
-            for (int c = 0; c < 5; c++) eval_proxy(s, m, cand[c], rg.eb, rg.stat_eb, R2, l2, h1v[c], xv[c]);
+            for (int c = 0; c < 5; c++)
+                if (!eval_proxy(s, m, cand[c], rg.eb, rg.stat_eb, R2, l2, h1v[c], xv[c])) {
+                    atomicOr(err_word, 1u);
+                    return;
+                }
             if (proxies) {
                 for (int c = 0; c < 5; c++) {
                     proxies[(g * 10) + c] = h1v[c];
@@ -403,8 +413,11 @@ __global__ void slope_v0_kernel(FieldGeom fg, const SampleBox *__restrict__ boxe
     m_out[g] = m;
     if (m == 0) return;
     for (uint32_t e = 0; e < n_evals; e++)
-        eval_proxy(s, m, evals[e].t, evals[e].abs_eb, box.stat_eb, R2, log2arena + box.log2_off, h1_out[g * n_evals + e],
-                   x_out[g * n_evals + e]);
+        if (!eval_proxy(s, m, evals[e].t, evals[e].abs_eb, box.stat_eb, R2, log2arena + box.log2_off,
+                        h1_out[g * n_evals + e], x_out[g * n_evals + e])) {
+            atomicOr(err_word, 2u);
+            return;
+        }
 }
 
 uint64_t tsel_scratch_bytes(uint32_t cap, uint32_t bcap, uint32_t tcap) { return scratch_bytes(cap, bcap, tcap); }

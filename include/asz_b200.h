@@ -267,11 +267,12 @@ int asz_profile_read(asz_ctx *ctx, asz_profile_entry *out, int max, int reset);
  * that must not allocate device memory. Scratch is a fixed 1 MiB device array in the library, so
  * n is limited to 65520 * 65536 values; larger n returns ASZ_E_ARG with a message. Squared
  * differences are summed in a fixed order, so repeated calls return identical bits.
- * Runs on the current device and on cuda_stream (NULL: the legacy default stream) and waits for
- * its result. The first call on a device looks up the scratch address (setup), so make it before
- * any stream capture. Calls on one device share the scratch: overlapping calls (from several
- * threads or streams) race and must be serialised by the caller. err (may be NULL) receives a
- * message of at most err_len bytes. */
+ * Runs on the current device and on cuda_stream (NULL: the legacy default stream), and
+ * synchronises that stream before it returns, so the figures are ready when the call ends. Each
+ * call looks up the scratch array's device address in the current context (the lookup allocates
+ * nothing). Calls on one device share the scratch: overlapping calls (from several threads or
+ * streams) race and must be serialised by the caller. err (may be NULL) receives a message of at
+ * most err_len bytes. */
 int asz_error_stats_noalloc(const float *x, const float *y, uint64_t n, double value_range, void *cuda_stream,
                             double *max_err, double *psnr, char *err, size_t err_len);
 

@@ -9,6 +9,8 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# The reference sources, for CPU tests that read its files (absent on GPU hosts).
+REFERENCE_DIR = os.environ.get("ASZ_REFERENCE_DIR", "/root/reference")
 
 
 def pytest_configure(config):

@@ -76,3 +76,38 @@ def test_output_blocks_are_reused_and_released(gpu_ctx):
     assert blobs == [first[0], first[1]]
     api.lib().asz_release_output_cache()
     assert gpu_ctx.compress(a, 1e-3, plan, "cubic", p)[0] == first[0]
+
+
+def _bare_context(device=0):
+    # A Context object that never reached asz_create: any library call through it would fail,
+    # so these tests show that the argument checks run first.
+    import asz_b200.api as api
+    ctx = object.__new__(api.Context)
+    ctx._L = None
+    ctx._c = None
+    ctx.device = device
+    return ctx
+
+
+def test_decompress_refuses_a_host_out_tensor():
+    import torch
+    ctx = _bare_context()
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        ctx.decompress(b"\0" * 16, (8, 8, 8), 1e-3, params=None, out=torch.empty(512))
+
+
+@pytest.mark.parametrize("case", ["dtype", "strided", "device", "numel"])
+def test_device_buffer_checks(case):
+    import torch
+    import asz_b200.api as api
+    x = torch.empty(8, 8, 8, dtype=torch.float32)
+    numel = 512
+    if case == "dtype":
+        x = x.double()
+    elif case == "strided":
+        x = x.transpose(0, 2)
+    elif case == "numel":
+        numel = 1000
+    # A host tensor reports no device index, so it fails the device check of any context.
+    with pytest.raises(ValueError):
+        api._check_device_field(x, 0, "out", numel)

@@ -6,6 +6,7 @@ import tempfile
 import pytest
 
 from asz_b200 import plans
+from conftest import REFERENCE_DIR
 
 
 def test_round_trip_and_launcher_layout():
@@ -66,7 +67,7 @@ def test_record_plan_replaces_the_entry():
         assert got == {1e-3: (["cubic2_012", "cubic2_021"], "quintic"), 1e-4: (["cubic1_012"], "cubic")}
 
 
-REF_PLANS = "/root/reference/plans"
+REF_PLANS = os.path.join(REFERENCE_DIR, "plans")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_PLANS), reason="reference plan files not present")
