@@ -120,6 +120,26 @@ inline void write_file(const std::string &path, const void *data, size_t n, cons
     if (!f) throw std::runtime_error(std::string("cannot write ") + what + ": " + path);
 }
 
+// The figures compress() prints after compressing (compress.tpp:306-319), in the float steps the
+// reference's build executes. The error loop there is scalar: the squared errors go into one float
+// through a fused multiply-add per value, in index order, and |d| into a running maximum. Then
+// psnr = 10*log10f(((max-min)^2 / sum) * n), the division by n folded into the product, and
+// dist = fma(-br, default_slope, psnr). The sum's order decides its last bits, so it is replayed on
+// the host here (the library's asz_compress_stats sums in double on the device).
+struct PrintedStats {
+    float max_err, mse_sum;
+};
+__attribute__((target("fma"))) inline PrintedStats printed_stats(const float *x, const float *y, uint64_t n) {
+    float sum = 0.0f, mx = 0.0f;
+    for (uint64_t i = 0; i < n; i++) {
+        const float d = x[i] - y[i];
+        sum = __builtin_fmaf(d, d, sum);
+        const float a = __builtin_fabsf(d);
+        mx = mx > a ? mx : a;
+    }
+    return {mx, sum};
+}
+
 struct Ctx {
     asz_ctx *c = nullptr;
     Ctx() {

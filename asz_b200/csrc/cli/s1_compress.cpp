@@ -154,13 +154,17 @@ int main(int argc, char *argv[]) try {
     printf("Zstd compression time: %f s\n", r.zstd_s);
     printf("Core compression time: %f s\n", r.core_s + r.zstd_s);
     printf("Compression time: %f s\n", r.data_range_s + r.core_s + r.zstd_s);
-    double max_err = 0, psnr = 0;
-    ctx.check(asz_compress_stats(ctx.c, &max_err, &psnr));
-    float cr = (float)n * sizeof(float) / (float)out_len;
-    float br = 8 * sizeof(float) / cr;
-    printf("max_err= %f (%f%%)\n", (float)max_err, (float)max_err * 100 / r.abs_eb);
-    printf("CR: %f, BR: %f, PSNR: %f\n", cr, br, (float)psnr);
-    printf("dist=%f\n", -r.default_slope * br + (float)psnr);
+    // The reconstruction comes back from the device for the reference's own error loop.
+    std::vector<float> rec(n);
+    if (asz_debug_recon(ctx.c, rec.data()) != n) throw std::runtime_error("reconstruction not available");
+    const cli::PrintedStats st = cli::printed_stats((const float *)raw.data(), rec.data(), n);
+    const float cr = (float)n * sizeof(float) / (float)out_len;
+    const float br = 8 * sizeof(float) / cr;
+    const float range = r.max_val - r.min_val;
+    const float psnr = log10f(range * range / st.mse_sum * (float)n) * 10.0f;
+    printf("max_err= %f (%f%%)\n", st.max_err, st.max_err * 100.0f / r.abs_eb);
+    printf("CR: %f, BR: %f, PSNR: %f\n", cr, br, psnr);
+    printf("dist=%f\n", std::fma(-br, r.default_slope, psnr));
     cli::write_file(a.compressed, out, out_len, "compressed output");
     asz_free(out);
     return 0;

@@ -44,34 +44,6 @@ METRIC = "compress/decompress GB/s at REL 1e-3 (bit-exact); tune time & CR vs pl
 WORKLOAD = "512^3 float32 k^-5/3 GRF + tanh front, REL 1e-3, plan cubic2_012 x9, cubic, block_pivot_ratio 3"
 
 
-def make_field_torch(seed, shape, device):
-    """The C2 recipe on the GPU (torch FFT), returned as a contiguous float32 CUDA tensor."""
-    import torch
-    g = torch.Generator(device=device).manual_seed(seed)
-    white = torch.randn(shape, generator=g, device=device, dtype=torch.float32)
-    spec = torch.fft.rfftn(white)
-    del white
-    k = [torch.fft.fftfreq(n, device=device) * n for n in shape[:-1]] + [torch.fft.rfftfreq(shape[-1], device=device) * shape[-1]]
-    kk = (k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2).sqrt_()
-    kk[0, 0, 0] = 1.0
-    amp = kk.pow_(-5.0 / 6.0)
-    amp[0, 0, 0] = 0.0
-    spec.mul_(amp)
-    del amp, kk
-    f = torch.fft.irfftn(spec, s=shape)
-    del spec
-    f -= f.mean()
-    f /= f.std()
-    gen = np.random.default_rng(seed)
-    n = gen.standard_normal(3)
-    n /= np.linalg.norm(n)
-    c = [gen.uniform(0.25 * s, 0.75 * s) for s in shape]
-    ax = [torch.arange(s, device=device, dtype=torch.float32) for s in shape]
-    d = (ax[0][:, None, None] - c[0]) * n[0] + (ax[1][None, :, None] - c[1]) * n[1] + (ax[2][None, None, :] - c[2]) * n[2]
-    f += 10.0 * f.std() * torch.tanh(d / 4.0)
-    return f.contiguous()
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
 
@@ -136,21 +108,19 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_baseline(field_np, workdir, planes=64):
-    """The reference s1_compress on the first `planes` planes of the field (same plan/eb/flags)."""
+def cpu_baseline(field_np, workdir):
+    """The reference s1_compress (one process, one thread) on the full field, same plan, error
+    bound and flags: about 20 s of host work for 512^3."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     exe = O.ref_binary("s1_compress")
-    kind = "reference"
-    sample = field_np[:planes]
-    inp = os.path.join(workdir, "slab.f32")
-    out = os.path.join(workdir, "slab.asz")
-    np.ascontiguousarray(sample).tofile(inp)
     if exe is None:
         return None
-    # The reference takes abs_eb from its own input's range; REL is applied to the slab.
-    argv = [exe, "-i", inp, "-z", out, "-3", *[str(s) for s in sample.shape], "-M", "REL", repr(REL_EB),
-            "--predictor-plan", PLAN, "--predictor-family", FAMILY, "--block-pivot-ratio", str(BPR)]
+    inp = os.path.join(workdir, "field.f32")
+    out = os.path.join(workdir, "field.asz")
+    np.ascontiguousarray(field_np).tofile(inp)
+    argv = [exe, "-f", "-i", inp, "-3", *[str(s) for s in field_np.shape], "-M", "REL", f"{REL_EB:.17g}",
+            "--block-pivot-ratio", str(BPR), "--predictor-family", FAMILY, "-z", out, "--predictor-plan", PLAN]
     t0 = time.perf_counter()
     r = subprocess.run(argv, capture_output=True, text=True)
     wall = time.perf_counter() - t0
@@ -160,43 +130,126 @@ def cpu_baseline(field_np, workdir, planes=64):
     for line in r.stdout.splitlines():
         if line.startswith("Compression time:"):
             comp = float(line.split(":")[1].split()[0])
-    return {"value": sample.nbytes / 1e9 / wall, "unit": "GB/s", "cores": 1, "kind": kind,
-            "sample": f"reference s1_compress on a {sample.shape[0]}x512x512 slab of the field, wall time "
-                      f"(its own 'Compression time' {comp:.3f} s, which excludes plan preparation)" if comp else
-                      f"reference s1_compress on a {sample.shape[0]}x512x512 slab, wall time"}
+    shape = "x".join(map(str, field_np.shape))
+    return {"value": field_np.nbytes / 1e9 / wall, "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": f"reference s1_compress on the full {shape} field of this run, one process, wall time"
+                      + (f" (its own 'Compression time' {comp:.3f} s)" if comp else "")}
+
+
+def bench_config(shape, world):
+    """The `config` object of both arms' JSON lines (identical, so the two lines compare)."""
+    n = shape[0] * shape[1] * shape[2]
+    workload = WORKLOAD if tuple(shape) == SHAPE else WORKLOAD.replace("512^3", "x".join(map(str, shape)))
+    return {"workload": workload, "field": "asz_b200.fields.c2_field(seed=2 + rank), generated on the host",
+            "inputs": f"{4 * n / 2**20:.0f} MiB per field; "
+                      + ("> L2, no flush needed" if 4 * n > 126e6 else "fits L2 (profiling size only)"),
+            "parallelism": f"replicas x{world}"}
+
+
+def make_bench_field(rank, shape):
+    """The benchmark field of `rank`: the C2 recipe from seed 2 + rank (NumPy, on the host). Rank 0's
+    512^3 field is the one tests/golden/fullsize.json records the reference's output for."""
+    from asz_b200 import fields
+    return fields.c2_field(seed=2 + rank, shape=tuple(shape))
+
+
+def reference_parity(x_host, blob, y, rank):
+    """This run's .asz and decompressed output against the reference's, recorded for the same input
+    bytes by tests/golden/make_fullsize.py (case c2_cubic_0.001: this workload). None when the field
+    is not the recorded one (other ranks, other shapes)."""
+    import hashlib
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "fullsize.json")) as f:
+            fix = json.load(f)
+    except OSError:
+        return None
+    if rank != 0 or hashlib.sha256(x_host.tobytes()).hexdigest() != fix["fields"]["c2"]["sha256"]:
+        return None
+    case = next(c for c in fix["cases"] if c["name"] == "c2_cubic_0.001")
+    dec = y.cpu().numpy().tobytes()
+    return {"case": case["name"], "asz_equal": hashlib.sha256(blob).hexdigest() == case["asz_sha256"],
+            "decompressed_equal": hashlib.sha256(dec).hexdigest() == case["decompressed_sha256"],
+            "source": "SHA-256 digests of the reference binaries' output on the same input (tests/golden/fullsize.json)"}
+
+
+def _usable_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _available_bytes():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 16 << 30
+
+
+def _run_pool(argvs, workers):
+    """Run the command lines with at most `workers` at a time; returns the wall time."""
+    import concurrent.futures as cf
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(workers) as ex:
+        for r in ex.map(lambda a: subprocess.run(a, capture_output=True, text=True), argvs):
+            if r.returncode != 0:
+                raise RuntimeError(f"reference run failed: {r.stderr.strip()[:200]}")
+    return time.perf_counter() - t0
 
 
 def run_reference_arm(args):
+    """The reference's own compressor (oracle/_ref/s1_compress, compiled from the reference sources
+    with its flags) on the same field, error bound, plan and flags as this build's arm. One step is
+    one full compression of the 512^3 field. The reference is single-threaded, so the steps run as
+    concurrent processes, as many as the host's cores and memory allow: value is the aggregate
+    input GB/s of the timed steps over their wall time. Its decompressor is timed the same way."""
     rank, world, local = dist_env()
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    exe = O.ref_binary("s1_compress")
-    if exe is None:
+    exe, dexe = O.ref_binary("s1_compress"), O.ref_binary("s1_decompress")
+    if exe is None or dexe is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference binaries not built (make -C oracle ref)"}))
         return
-    from asz_b200 import fields
-    planes = 32
-    field = fields.c2_field(seed=2, shape=(planes, 512, 512))
+    shape = tuple(int(v) for v in args.shape.split(","))
+    field = make_bench_field(0, shape)
+    nbytes = field.nbytes
+    # About 2.2 GB of host memory per 512^3 compression (input, its working copy, QB streams).
+    per_proc = 4.5 * nbytes + (64 << 20)
+    workers = max(1, min(args.steps, _usable_cores(), int(_available_bytes() * 0.8 // per_proc)))
     with tempfile.TemporaryDirectory() as wd:
-        inp = os.path.join(wd, "slab.f32")
+        inp = os.path.join(wd, "field.f32")
         field.tofile(inp)
-        argv = [exe, "-i", inp, "-z", os.path.join(wd, "o.asz"), "-3", str(planes), "512", "512", "-M", "REL", repr(REL_EB),
-                "--predictor-plan", PLAN, "--predictor-family", FAMILY, "--block-pivot-ratio", str(BPR)]
-        for _ in range(args.warmup):
-            subprocess.run(argv, capture_output=True, check=True)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            subprocess.run(argv, capture_output=True, check=True)
-        dt = time.perf_counter() - t0
-    gbs = field.nbytes * args.steps / 1e9 / dt
-    sample = f"reference s1_compress (1 thread) on a {planes}x512x512 slab of the C2 recipe per step"
+        del field
+        common = ["-f", "-i", inp, "-3", *map(str, shape), "-M", "REL", f"{REL_EB:.17g}",
+                  "--block-pivot-ratio", str(BPR), "--predictor-family", FAMILY]
+
+        def comp(k):
+            return [exe, *common, "-z", os.path.join(wd, f"o{k}.asz"), "--predictor-plan", PLAN]
+
+        def decomp(k):
+            return [dexe, *common, "-z", os.path.join(wd, f"o{k % workers}.asz"), "-o", os.path.join(wd, f"r{k % workers}.f32")]
+
+        _run_pool([comp(k) for k in range(args.warmup)], workers)
+        dt = _run_pool([comp(k) for k in range(args.steps)], workers)
+        asz_len = os.path.getsize(os.path.join(wd, "o0.asz"))
+        ddt = _run_pool([decomp(k) for k in range(args.steps)], workers)
+    gbs = nbytes * args.steps / 1e9 / dt
+    dgbs = nbytes * args.steps / 1e9 / ddt
+    sample = (f"reference s1_compress on the full {'x'.join(map(str, shape))} field per step, {workers} single-threaded "
+              f"processes at a time ({_usable_cores()} usable cores), aggregate input GB/s")
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                      "data": "synthetic", "config": {"workload": WORKLOAD, "sample_planes": planes},
-                      "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": 1, "kind": "reference", "sample": sample},
+                      "data": "synthetic", "config": bench_config(shape, 1),
+                      "decompress": {"value": dgbs, "unit": "GB/s", "ms_per_step": ddt * 1000 / args.steps},
+                      "cr": nbytes / asz_len, "concurrent_processes": workers,
+                      "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": workers, "kind": "reference", "sample": sample},
                       "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
@@ -231,8 +284,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
-    x = make_field_torch(1234 + rank, shape, dev)
-    workload = WORKLOAD if shape == SHAPE else WORKLOAD.replace("512^3", "x".join(map(str, shape)))
+    x_host = make_bench_field(rank, shape)
+    x = torch.from_numpy(x_host).to(dev)
     N = x.numel()
     p = api.default_params(block_pivot_ratio=BPR)
     ctx = api.Context(local)
@@ -319,6 +372,7 @@ def main():
     bit_exact = bool(torch.equal(rec.view(torch.int32), y.view(torch.int32)))
     max_err = float((y - x).abs().max().item())
     del rec
+    parity = reference_parity(x_host, blob, y, rank)
     # Profile of one compression and one decompression (per kernel family, CUDA events).
     L.asz_set_stream(ctx._c, C.c_void_p(stream.cuda_stream))
     L.asz_profile_enable(ctx._c, 1)
@@ -426,17 +480,15 @@ def main():
     roofline_path = {"bound": "hbm", "achieved": path_ach, "peak": peak, "unit": "GB/s", "frac": path_ach / peak,
                      "bytes_per_step": 4 * N + pre_zstd_len}
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         with tempfile.TemporaryDirectory() as wd:
-            cpu = cpu_baseline(x[:64].cpu().numpy(), wd, planes=min(64, shape[0]))
+            cpu = cpu_baseline(x_host, wd)
     out = {
         "metric": METRIC, "value": comp_gbs, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": core_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload, "inputs": f"{4 * N / 2**20:.0f} MiB per field; "
-                   + ("> L2, no flush needed" if 4 * N > 126e6 else "fits L2 (profiling size only)"),
-                   "parallelism": f"replicas x{world}",
-                   "value_excludes": "libzstd and host<->device copies (timed inside the call, reported apart)"},
+        "config": bench_config(shape, world),
+        "value_excludes": "libzstd and host<->device copies (timed inside the call, reported apart)",
         "decompress": {"value": dec_gbs, "unit": "GB/s", "ms_per_step": dec_ms / args.steps},
         "zstd_ms_per_step": zstd_s * 1000 / args.steps, "d2h_ms_per_step": d2h_s * 1000 / args.steps,
         "zstd_decompress_ms_per_step": dz_s * 1000 / args.steps,
@@ -447,6 +499,7 @@ def main():
         "e2e_decompress": {"value": e2e_dec_gbs, "unit": "GB/s", "h2d_bytes_per_step": pre_zstd_len,
                            "d2h_bytes_per_step": 4 * N, "ms_per_step": e2e_dec_ms / args.steps},
         "cr": float(4 * N / asz_len), "pre_zstd_bytes": pre_zstd_len, "bit_exact_roundtrip": bit_exact,
+        "parity_vs_reference": parity,
         "max_err_over_eb": max_err / rep1.abs_eb,
         "t_fallback_count": int(rep1.t_fallback_count), "ambiguous_decisions": int(rep1.ambiguous_decisions),
         "reruns": int(rep1.reruns),
