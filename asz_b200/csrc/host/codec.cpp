@@ -169,9 +169,68 @@ private:
 };
 }  // namespace
 
+namespace {
+// One host thread that runs submitted jobs in order: the Huffman code of a round's stream is built
+// here while the device runs the later rounds. wait() returns when every submitted job is done.
+class SerialWorker {
+public:
+    SerialWorker() : th_([this] { loop(); }) {}
+    ~SerialWorker() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        th_.join();
+    }
+    void submit(std::function<void()> f) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            q_.push_back(std::move(f));
+            pending_++;
+        }
+        cv_.notify_all();
+    }
+    void wait() {
+        std::unique_lock<std::mutex> l(mu_);
+        done_.wait(l, [&] { return pending_ == 0; });
+    }
+
+private:
+    void loop() {
+        for (;;) {
+            std::function<void()> f;
+            {
+                std::unique_lock<std::mutex> l(mu_);
+                cv_.wait(l, [&] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;
+                f = std::move(q_.front());
+                q_.erase(q_.begin());
+            }
+            f();
+            std::lock_guard<std::mutex> g(mu_);
+            if (--pending_ == 0) done_.notify_all();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    std::vector<std::function<void()>> q_;
+    size_t pending_ = 0;
+    bool stop_ = false;
+    std::thread th_;
+};
+}  // namespace
+
 struct asz_ctx {
     int device = 0;
     cudaStream_t own = nullptr, stream = nullptr;
+    // Copies of each round's histogram window run here, behind the round's kernel, while the main
+    // stream goes on with the next round; their events (two per round) order the builder thread.
+    cudaStream_t side = nullptr;
+    std::vector<cudaEvent_t> round_ev;
+    DevBuf hwin;          // per QB stream of the rounds: kHistWin 64-bit bins
+    PinnedBuf hwin_host;  // their copies, with each stream's [min, max] and overflow word
+    std::unique_ptr<SerialWorker> builder;
     std::string err;
     // Device buffers.
     DevBuf in, rec, qb, tval, tint, misc, scratch, log2arena, hist, codes, bitoff, cubtmp, payload, amb, overrides,
@@ -735,6 +794,11 @@ asz_ctx *asz_create(int device) {
         return nullptr;
     }
     c->stream = c->own;
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(c->own);
+        delete c;
+        return nullptr;
+    }
     return c;
 }
 
@@ -742,6 +806,11 @@ void asz_destroy(asz_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
+    c->builder.reset();
+    for (cudaEvent_t e : c->round_ev) cudaEventDestroy(e);
+    if (c->side) cudaStreamDestroy(c->side);
+    c->hwin.release();
+    c->hwin_host.release();
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
                       &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
@@ -806,6 +875,7 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t dec_changed;  // batched Huffman decoding: a chunk start moved in the last pass
     uint32_t resume_count;  // fused axis-2 compression: columns waiting for the exact path
     int32_t qb_range[2 * 64];
+    uint32_t hist_over[64];  // round l: a QB of its stream fell outside the histogram window
     float h1[3 * 64];
     float x[3 * 64];
     uint32_t m[3];
@@ -997,6 +1067,7 @@ struct StreamOut {
     u64 payload_word_off = 0;  // in the payload arena (32-bit words)
     int64_t lo = 0, hi = -1;   // histogram range
     u64 hist_off = 0;
+    bool prebuilt = false;     // code built during the rounds (no histogram pass here)
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -1352,11 +1423,22 @@ struct CoreArgs {
     float mn, mx, abs_eb, slope;
     const int64_t *t_given = nullptr;  // host table of block-major t codes replacing the selection
     u64 t_len = 0;
+    // Count each round's QB histogram in its kernel and build the stream's Huffman code on the
+    // context's builder thread while the later rounds run.
+    bool prebuild = false;
+};
+
+// A QB stream's code built during the rounds (ok == false: the encoder counts and builds it).
+struct PreCode {
+    bool ok = false;
+    int64_t lo = 0, hi = -1;
+    HuffCode code;
 };
 
 struct CoreOut {
     Geometry G;
     std::vector<u64> qb_off, qb_len;
+    std::vector<PreCode> pre;  // index s: QB stream s (0: pivots, 1..L: rounds)
 };
 
 int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
@@ -1480,10 +1562,81 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
         }
     }
     u64 lines_exact = 0, lines_serial = 0;
+    // Codes built during the rounds (CoreArgs::prebuild): each round's kernel counts its stream's
+    // QB histogram window; a copy on the side stream behind the kernel and a code build on the
+    // builder thread follow it, while the main stream runs the next rounds.
+    const bool prebuild = a.prebuild && !line_bytes && !a.probe && !a.origin && L > 0;
+    unsigned long long *d_hwin = nullptr;
+    u64 *h_hist = nullptr;
+    int32_t *h_rng = nullptr;
+    uint32_t *h_over = nullptr;
+    o.pre.assign(L + 1, PreCode{});
+    if (prebuild) {
+        CK(ctx->hwin.reserve(L * kHistWin * 8));
+        CK(ctx->hwin_host.reserve(L * kHistWin * 8 + L * 8 + L * 4));
+        d_hwin = ctx->hwin.as<unsigned long long>();
+        h_hist = (u64 *)ctx->hwin_host.p;
+        h_rng = (int32_t *)(h_hist + L * kHistWin);
+        h_over = (uint32_t *)(h_rng + 2 * L);
+        while (ctx->round_ev.size() < 2 * L) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ctx->round_ev.push_back(e);
+        }
+        if (!ctx->builder) ctx->builder = std::make_unique<SerialWorker>();
+    }
+    // Every return from here waits for the builder, which writes into o.pre.
+    struct BuilderWait {
+        SerialWorker *w;
+        ~BuilderWait() {
+            if (w) w->wait();
+        }
+    } builder_wait{prebuild ? ctx->builder.get() : nullptr};
+    auto schedule_code = [&](u64 l) -> int {
+        if (!prebuild) return ASZ_OK;
+        cudaEvent_t ev_r = ctx->round_ev[2 * l], ev_c = ctx->round_ev[2 * l + 1];
+        CK(cudaEventRecord(ev_r, st));
+        CK(cudaStreamWaitEvent(ctx->side, ev_r, 0));
+        CK(cudaMemcpyAsync(h_hist + l * kHistWin, d_hwin + l * kHistWin, kHistWin * 8, cudaMemcpyDeviceToHost, ctx->side));
+        CK(cudaMemcpyAsync(h_rng + 2 * l, &dm->qb_range[2 * (l + 1)], 8, cudaMemcpyDeviceToHost, ctx->side));
+        CK(cudaMemcpyAsync(h_over + l, &dm->hist_over[l], 4, cudaMemcpyDeviceToHost, ctx->side));
+        CK(cudaEventRecord(ev_c, ctx->side));
+        const u64 count = qb_len[l + 1];
+        PreCode *pc = &o.pre[l + 1];
+        const int dev = ctx->device;
+        const u64 *hl = h_hist + l * kHistWin;
+        const int32_t *rl = h_rng + 2 * l;
+        const uint32_t *ol = h_over + l;
+        ctx->builder->submit([=]() {
+            cudaSetDevice(dev);
+            if (cudaEventSynchronize(ev_c) != cudaSuccess) return;
+            const int32_t lo = rl[0], hi = rl[1];
+            if (*ol || count == 0 || lo > hi || lo < -(int32_t)kHistHalf || hi >= (int32_t)kHistHalf) return;
+            const u64 *h = hl + (int64_t)lo + kHistHalf;
+            u64 a0 = 0, b0 = (u64)(hi - lo) + 1;
+            while (a0 < b0 && h[a0] == 0) a0++;
+            while (b0 > a0 && h[b0 - 1] == 0) b0--;
+            std::vector<u64> hh(h + a0, h + b0);
+            std::string err;
+            HuffCode code;
+            if (!build_code(hh, (int64_t)lo + (int64_t)a0, (int64_t)lo + (int64_t)b0 - 1, count, false, code, err)) return;
+            pc->code = std::move(code);
+            pc->lo = (int64_t)lo + (int64_t)a0;
+            pc->hi = (int64_t)lo + (int64_t)b0 - 1;
+            pc->ok = true;
+        });
+        return ASZ_OK;
+    };
     hs_prep.reset();
     std::optional<HostScope> hs_rounds(std::in_place, ctx, "host:rounds");
     while (true) {
         // Error word, fallback count, ambiguity count, QB ranges.
+        if (prebuild) {
+            ctx->builder->wait();  // builds of a previous attempt
+            for (PreCode &pc : o.pre) pc = PreCode{};
+            CK(cudaMemsetAsync(d_hwin, 0, L * kHistWin * 8, st));
+            CK(cudaMemsetAsync(dm->hist_over, 0, sizeof(dm->hist_over), st));
+        }
         CK(cudaMemsetAsync(&dm->err, 0, 3 * sizeof(uint32_t), st));
         CK(cudaMemsetAsync(dm->why, 0, sizeof(dm->why), st));
         for (u64 s = 0; s <= L; s++)
@@ -1570,7 +1723,10 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
                 CK(launch_tval_from_codes(d_tint, G.nblocks, (uint32_t)L, (uint32_t)l, (float)p.t_precision, d_tval, st));
                 ProfScope ps(ctx, "round_compress", rg.targets * 12);
                 CK(launch_round_compress(G.fg, rg, d_ent, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
-                                         &dm->qb_range[2 * (l + 1)], &dm->err, 0, nullptr, st));
+                                         &dm->qb_range[2 * (l + 1)], &dm->err, 0, nullptr, st,
+                                         prebuild ? d_hwin + l * kHistWin : nullptr, prebuild ? &dm->hist_over[l] : nullptr));
+                rc = schedule_code(l);
+                if (rc) return rc;
                 continue;
             }
             uint32_t *d_list = ctx->tlist.as<uint32_t>(), *d_lcount = &dm->list_count[l % 64];
@@ -1618,7 +1774,10 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
             }
             ProfScope ps(ctx, "round_compress", rg.targets * 12);
             CK(launch_round_compress(G.fg, rg, d_ent, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
-                                     &dm->qb_range[2 * (l + 1)], &dm->err, a.probe ? 1 : 0, a.pred_out, st));
+                                     &dm->qb_range[2 * (l + 1)], &dm->err, a.probe ? 1 : 0, a.pred_out, st,
+                                     prebuild ? d_hwin + l * kHistWin : nullptr, prebuild ? &dm->hist_over[l] : nullptr));
+            rc = schedule_code(l);
+            if (rc) return rc;
         }
         uint32_t words[3];
         uint32_t lcounts[64], scounts[64];
@@ -1908,6 +2067,7 @@ struct EncodeArgs {
     const asz_params *p;
     const int64_t *t_given;    // a caller's t table, or nullptr
     u64 t_len, N;
+    const std::vector<PreCode> *pre = nullptr;  // QB streams' codes built during the rounds
 };
 
 // Entropy stage of several fields at once: ranges, histograms, code builds (host threads over all
@@ -1953,9 +2113,16 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
             so[s2 + 1].count = (*a.qb_len)[s2];
             so[s2 + 1].lo = ranges[f][2 * s2];
             so[s2 + 1].hi = ranges[f][2 * s2 + 1];
+            if (a.pre && s2 < a.pre->size() && (*a.pre)[s2].ok && so[s2 + 1].count) {
+                const PreCode &pc = (*a.pre)[s2];
+                so[s2 + 1].prebuilt = true;
+                so[s2 + 1].lo = pc.lo;
+                so[s2 + 1].hi = pc.hi;
+                so[s2 + 1].code = pc.code;
+            }
         }
         for (auto &o : so) {
-            if (!o.count) continue;
+            if (!o.count || o.prebuilt) continue;
             u64 range = (u64)(o.hi - o.lo) + 1;
             if (range > (1ull << 27)) return fail(ctx, ASZ_E_UNSUPPORTED, "QB range too wide for the dense histogram");
             o.hist_off = hist_total;
@@ -1974,7 +2141,7 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
             CK(launch_histogram<int64_t>(a.d_tint, so[0].count, so[0].lo, (u64)(so[0].hi - so[0].lo) + 1, d_hist + so[0].hist_off,
                                          st));
         for (u64 s2 = 0; s2 <= L; s2++)
-            if (so[s2 + 1].count)
+            if (so[s2 + 1].count && !so[s2 + 1].prebuilt)
                 CK(launch_histogram<int32_t>(a.d_qb + (*a.qb_off)[s2], (*a.qb_len)[s2], so[s2 + 1].lo,
                                              (u64)(so[s2 + 1].hi - so[s2 + 1].lo) + 1, d_hist + so[s2 + 1].hist_off, st));
     }
@@ -1988,7 +2155,7 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
     std::vector<std::pair<u64, u64>> jobs;
     for (u64 f = 0; f < nf; f++)
         for (u64 s2 = 0; s2 < SO[f].size(); s2++)
-            if (SO[f][s2].count) jobs.push_back({f, s2});
+            if (SO[f][s2].count && !SO[f][s2].prebuilt) jobs.push_back({f, s2});
     std::vector<std::string> code_err(jobs.size());
     std::vector<char> code_ok(jobs.size(), 1);
     auto build_one = [&](u64 j) {
@@ -2004,11 +2171,15 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
                                 code_err[j]);
         o.lo += (int64_t)a0;
     };
-    if (jobs.size() > 1) {
+    // Waking the pool costs more than a few small builds (the t and pivot streams, when the
+    // rounds' codes were built during the rounds), so those run here.
+    u64 job_symbols = 0;
+    for (auto &j : jobs) job_symbols += (u64)(SO[j.first][j.second].hi - SO[j.first][j.second].lo) + 1;
+    if (jobs.size() > 2 && job_symbols > 4096) {
         if (!ctx->pool) ctx->pool = std::make_unique<HostPool>(std::min(15u, std::max(1u, std::thread::hardware_concurrency()) - 1));
         ctx->pool->run(jobs.size(), build_one);
-    } else if (jobs.size() == 1) {
-        build_one(0);
+    } else {
+        for (u64 j = 0; j < jobs.size(); j++) build_one(j);
     }
     for (u64 j = 0; j < jobs.size(); j++)
         if (!code_ok[j]) return fail(ctx, ASZ_E_UNSUPPORTED, code_err[j]);
@@ -2256,6 +2427,7 @@ static int compress_entry(asz_ctx *ctx, const float *in, int in_on_device, const
     CoreOut co;
     {
         CoreArgs ca{d_in, dims, nullptr, &plan, &p, quintic, false, nullptr, mn, mx, abs_eb, slope, t_given, t_len};
+        ca.prebuild = true;
         rc = run_core(ctx, ca, co, R);
         if (rc) return rc;
     }
@@ -2263,7 +2435,7 @@ static int compress_entry(asz_ctx *ctx, const float *in, int in_on_device, const
     std::vector<u64> &qb_off = co.qb_off, &qb_len = co.qb_len;
     {
         const std::vector<EncodeArgs> ea{EncodeArgs{&G, &qb_off, &qb_len, ctx->qb.as<int32_t>(), ctx->tint.as<int64_t>(),
-                                                    dm->qb_range, mn, mx, quintic, &plan, &p, t_given, t_len, N}};
+                                                    dm->qb_range, mn, mx, quintic, &plan, &p, t_given, t_len, N, &co.pre}};
         std::vector<asz_report *> rs{&R};
         std::vector<std::pair<u64, u64>> span;
         rc = encode_fields(ctx, ea, rs, span, ctx->pre_zstd);

@@ -220,13 +220,20 @@ __device__ __forceinline__ void compress_lines2(const FieldGeom &fg, const Round
                                                 const float *__restrict__ tval, const float *__restrict__ in,
                                                 float *__restrict__ rec, int32_t *__restrict__ qb, uint32_t *err_word,
                                                 float *__restrict__ pred_out, double ebd, double eb2, double rinv, double r0,
-                                                int32_t &lo, int32_t &hi) {
+                                                int32_t &lo, int32_t &hi, uint32_t *hsh, bool &hover) {
     const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
     const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
     const uint64_t n1n2 = fg.n[1] * fg.n[2], n2 = fg.n[2];
     const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
     const int dir = rg.dir;
     const bool hasB = lineB != UINT32_MAX;
+    // The stream's histogram window in shared memory (hsh == nullptr: not counted here).
+    auto count = [&](int32_t v) {
+        if (!hsh) return;
+        const uint32_t b = (uint32_t)(v + kHistHalf);
+        if (b < kHistWin) atomicAdd(&hsh[b], 1u);
+        else hover = true;
+    };
     const uint32_t a0 = lineA / T1, b0 = hasB ? lineB / T1 : a0;
     const AxisEntry e0A = load_entry(e0t + a0), e1A = load_entry(e1t + (lineA - a0 * T1));
     const AxisEntry e0B = load_entry(e0t + b0), e1B = load_entry(e1t + (hasB ? lineB - b0 * T1 : lineA - a0 * T1));
@@ -264,6 +271,7 @@ __device__ __forceinline__ void compress_lines2(const FieldGeom &fg, const Round
             rec[posA] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
             lo = min(lo, v);
             hi = max(hi, v);
+            count(v);
         }
         if (okB) {
             const float pred = predict_loaded(vB, scB, tB);
@@ -276,6 +284,7 @@ __device__ __forceinline__ void compress_lines2(const FieldGeom &fg, const Round
             rec[posB] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
             lo = min(lo, v);
             hi = max(hi, v);
+            count(v);
         }
     }
 }
@@ -296,22 +305,40 @@ __device__ __forceinline__ void reduce_range(int32_t lo, int32_t hi, int32_t *qb
 // axes 1 and 2 divide (diff*0.5)/eb (out-of-line clone); value = fma(-qb, 2eb, pred) in double.
 // kProbe: every axis divides, as the diagnostics instantiation that the predictor-family probe runs
 // does (one out-of-line clone for all axes), and pred_out receives each target's prediction.
+//
+// hist (optional) receives the QB histogram of the round's stream over the window
+// [-kHistHalf, kHistHalf): each CTA counts in shared memory and adds its nonzero bins at the end;
+// a QB outside the window sets *hist_over, and the caller then counts that stream separately.
 template <bool kProbe>
 __global__ void __launch_bounds__(256, 3)
     round_compress_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, uint32_t tpl_log2,
                           const float *__restrict__ tval, const float *__restrict__ in, float *__restrict__ rec,
-                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out) {
+                          int32_t *__restrict__ qb, int32_t *qb_range, uint32_t *err_word, float *__restrict__ pred_out,
+                          unsigned long long *__restrict__ hist, uint32_t *hist_over) {
+    extern __shared__ uint32_t hsh_raw[];
+    uint32_t *hsh = hist ? hsh_raw : nullptr;
+    if (hsh) {
+        for (uint32_t i = threadIdx.x; i < kHistWin; i += blockDim.x) hsh[i] = 0;
+        __syncthreads();
+    }
     const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd), r0 = __dmul_rn(rinv, 0.5);
     const uint32_t lines = (uint32_t)rg.tcount[0] * (uint32_t)rg.tcount[1];
     const LineMap m = line_map(tpl_log2);
     int32_t lo = INT32_MAX, hi = INT32_MIN;
+    bool hover = false;
     const uint32_t step = gridDim.x * m.lines_per_cta;
     for (uint32_t line = blockIdx.x * m.lines_per_cta + m.row; line < lines; line += 2 * step) {
         const uint32_t lineB = line + step < lines ? line + step : UINT32_MAX;
         compress_lines2<kProbe>(fg, rg, ent, tpl_log2, m.sub, line, lineB, tval, in, rec, qb, err_word, pred_out, ebd, eb2, rinv,
-                                r0, lo, hi);
+                                r0, lo, hi, hsh, hover);
     }
     reduce_range(lo, hi, qb_range);
+    if (hsh) {
+        if (hover) atomicOr(hist_over, 1u);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kHistWin; i += blockDim.x)
+            if (hsh[i]) atomicAdd(&hist[i], (unsigned long long)hsh[i]);
+    }
 }
 
 // Batched form: one work queue over the (field, item) pairs of a round, an item being
@@ -526,15 +553,16 @@ static unsigned round_grid(const RoundGeom &rg, uint32_t tpl_log2) {
 
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
                                   const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, int div_all,
-                                  float *pred_out, cudaStream_t st) {
+                                  float *pred_out, cudaStream_t st, unsigned long long *hist, uint32_t *hist_over) {
     if (rg.targets == 0) return cudaSuccess;
     const uint32_t lg = round_lines_log2(rg.tcount[2]);
+    const size_t smem = hist ? kHistWin * sizeof(uint32_t) : 0;
     if (div_all)
-        round_compress_kernel<true><<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
-                                                                        pred_out);
+        round_compress_kernel<true><<<round_grid(rg, lg), 256, smem, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
+                                                                           pred_out, hist, hist_over);
     else
-        round_compress_kernel<false><<<round_grid(rg, lg), 256, 0, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
-                                                                         nullptr);
+        round_compress_kernel<false><<<round_grid(rg, lg), 256, smem, st>>>(fg, rg, ent, lg, tval, in, rec, qb, qb_range, err,
+                                                                            nullptr, hist, hist_over);
     count_launch();
     return cudaGetLastError();
 }

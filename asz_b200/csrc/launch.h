@@ -87,9 +87,13 @@ cudaError_t launch_pivot_compress(const PivotGeom &pg, const float *in, float *r
 cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, float *rec, cudaStream_t st);
 // One round over every target; `ent` holds the per-axis AxisEntry tables (RoundGeom::ent_off).
 // Requires tcount[0] * tcount[1] < 2^32 and tcount[2] < 2^32 (checked by the host).
+// hist (optional, kHistWin zeroed 64-bit bins): the QB histogram of the round's stream over
+// [-kHistHalf, kHistHalf), added to hist; a QB outside the window sets *hist_over.
+constexpr uint32_t kHistWin = 4096, kHistHalf = kHistWin / 2;
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
                                   const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, int div_all,
-                                  float *pred_out, cudaStream_t st);
+                                  float *pred_out, cudaStream_t st, unsigned long long *hist = nullptr,
+                                  uint32_t *hist_over = nullptr);
 cudaError_t launch_round_decompress(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const AxisEntry *ent,
                                     const int64_t *t_int, const int32_t *qb, float *rec, uint32_t *err, cudaStream_t st);
 
