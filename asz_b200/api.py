@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libasz_b200.so")
 _LIB = None
 
 ASZ_FAMILY_AUTO, ASZ_FAMILY_CUBIC, ASZ_FAMILY_QUINTIC = -1, 0, 1
-ASZ_OK, ASZ_E_ARG, ASZ_E_DATA, ASZ_E_CUDA, ASZ_E_DEVICE, ASZ_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
+ASZ_OK, ASZ_E_ARG, ASZ_E_DATA, ASZ_E_CUDA, ASZ_E_DEVICE, ASZ_E_UNSUPPORTED, ASZ_E_COMM = 0, -1, -2, -3, -4, -5, -6
 
 
 class AszError(RuntimeError):
@@ -136,6 +136,11 @@ def lib():
     L.asz_debug_proxies.restype = C.c_uint64
     L.asz_error_stats_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
                                           C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_char_p, C.c_size_t]
+    L.asz_slab_planes.argtypes = [C.POINTER(C.c_uint64), C.c_void_p, C.c_char_p, C.c_uint64, C.c_uint64,
+                                  C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.asz_compress_slab.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_uint64,
+                                    C.c_uint64, C.c_float, C.POINTER(Params), C.c_char_p,
+                                    C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.c_size_t), C.POINTER(Report)]
     _LIB = L
     return L
 

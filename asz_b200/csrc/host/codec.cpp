@@ -229,6 +229,7 @@ struct asz_ctx {
     cudaStream_t side = nullptr;
     std::vector<cudaEvent_t> round_ev;
     DevBuf hwin;          // per QB stream of the rounds: kHistWin 64-bit bins
+    DevBuf slab_idx, slab_val, slab_cmp;  // slabs: slope-sample indices, gathered values, compact copy
     PinnedBuf hwin_host;  // their copies, with each stream's [min, max] and overflow word
     std::unique_ptr<SerialWorker> builder;
     std::string err;
@@ -500,8 +501,17 @@ bool kernel_limits_ok(const struct Geometry &G);
 
 // Geometry of a compression of `dims` with `plan`; blocks and pivots start at `origin` (all zero
 // for a whole field; the predictor-family probe's local contexts start past a halo).
+// Slab of a field cut along axis 0 at block boundaries (asz_compress_slab): axis 0 has exactly
+// `blocks0` blocks (the last one ends at the array's last plane, the slab's upper face), and with
+// `skip_face` the plane at the origin belongs to the slab below, so the pivot lattice starts one
+// pivot stride above it.
+struct SlabGeom {
+    u64 blocks0 = 0;
+    bool skip_face = false;
+};
+
 void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &p, float abs_eb, float default_slope,
-                    bool quintic, Geometry &G, const uint64_t origin[3] = nullptr) {
+                    bool quintic, Geometry &G, const uint64_t origin[3] = nullptr, const SlabGeom *slab = nullptr) {
     FieldGeom &fg = G.fg;
     const u64 L = plan.pred.size();
     for (int a = 0; a < 3; a++) {
@@ -515,6 +525,7 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
         const u64 span = fg.n[a] > fg.origin[a] ? fg.n[a] - fg.origin[a] : 0;
         fg.block_num[a] = (span + fg.block_shape[a] - 1) / fg.block_shape[a];
     }
+    if (slab && slab->blocks0) fg.block_num[0] = slab->blocks0;
     fg.layer_num = (uint32_t)L;
     fg.quintic = quintic ? 1 : 0;
     fg.t_precision = p.t_precision;
@@ -522,10 +533,11 @@ void build_geometry(const uint64_t dims[3], const Plan &plan, const asz_params &
     // Pivots (compress.tpp:162-175).
     G.pivots = 1;
     for (int a = 0; a < 3; a++) {
-        const u64 span = fg.n[a] > fg.origin[a] ? fg.n[a] - fg.origin[a] : 0;
+        const u64 o = fg.origin[a] + (a == 0 && slab && slab->skip_face ? fg.pivot_stride[0] : 0);
+        const u64 span = fg.n[a] > o ? fg.n[a] - o : 0;
         G.pg.cnt[a] = (span + fg.pivot_stride[a] - 1) / fg.pivot_stride[a];
         G.pg.stride[a] = fg.pivot_stride[a];
-        G.pg.origin[a] = fg.origin[a];
+        G.pg.origin[a] = o;
         G.pivots *= G.pg.cnt[a];
     }
     G.pg.n1n2 = fg.n[1] * fg.n[2];
@@ -811,6 +823,9 @@ void asz_destroy(asz_ctx *c) {
     if (c->side) cudaStreamDestroy(c->side);
     c->hwin.release();
     c->hwin_host.release();
+    c->slab_idx.release();
+    c->slab_val.release();
+    c->slab_cmp.release();
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
                       &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
@@ -923,17 +938,12 @@ int compute_range(asz_ctx *ctx, const float *d_in, u64 N, float &mn, float &mx, 
 }
 
 // get_default_slope (c_codes/asz_core/get_default_slope.tpp:6-83).
-int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const asz_params &p, float abs_eb, float mn,
-                  float mx, const std::vector<float> &cand_t, float &slope_out, float &max_invalid_out, int &reason_out) {
-    FieldGeom fg{};
-    for (int a = 0; a < 3; a++) fg.n[a] = dims[a];
-    const float ebs[2] = {abs_eb * p.default_slope_eb_span, abs_eb / p.default_slope_eb_span};
+// The three whole-field sample boxes of get_default_slope (get_default_slope.tpp:13-22): along
+// direction d, [3, n_d - 3) with stride 2, the other axes whole, thinned by the sampling stride.
+void slope_boxes(const uint64_t dims[3], const asz_params &p, float abs_eb, SampleBox boxes[3]) {
     const float two_stat = abs_eb * p.stat_eb_ratio;
     const float stat_eb = two_stat * 0.5f;
     const float neg = 1.0f / two_stat;
-    MiscLayout *dm = ctx->misc.as<MiscLayout>();
-    SampleBox boxes[3];
-    uint32_t cap = 1;
     for (int d = 0; d < 3; d++) {
         SampleBox &b = boxes[d];
         u64 lo[3] = {0, 0, 0}, hi[3] = {dims[0], dims[1], dims[2]}, st[3] = {1, 1, 1};
@@ -956,8 +966,24 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
         b.neg_2_stat_eb = neg;
         b.stat_eb = stat_eb;
         b.n = (uint32_t)n;
-        b.log2_off = n ? log2_table(ctx, (uint32_t)n) : 0;
-        cap = std::max<uint32_t>(cap, (uint32_t)n);
+    }
+}
+
+// get_default_slope on given boxes over `field` (dims fdims): the whole field, or a compact copy of
+// the boxes' samples whose boxes keep the samples' order.
+int default_slope_on(asz_ctx *ctx, const float *field, const uint64_t fdims[3], SampleBox boxes[3], const asz_params &p,
+                     float abs_eb, float mn, float mx, const std::vector<float> &cand_t, float &slope_out,
+                     float &max_invalid_out, int &reason_out) {
+    FieldGeom fg{};
+    for (int a = 0; a < 3; a++) fg.n[a] = fdims[a];
+    const uint64_t *dims = fdims;
+    const float *d_in = field;
+    const float ebs[2] = {abs_eb * p.default_slope_eb_span, abs_eb / p.default_slope_eb_span};
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    uint32_t cap = 1;
+    for (int d = 0; d < 3; d++) {
+        boxes[d].log2_off = boxes[d].n ? log2_table(ctx, boxes[d].n) : 0;
+        cap = std::max<uint32_t>(cap, boxes[d].n);
     }
     const uint32_t ne = (uint32_t)(2 * cand_t.size());
     if (ne > 64) return fail(ctx, ASZ_E_UNSUPPORTED, "too many t candidates for the default slope");
@@ -970,7 +996,7 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
     u64 sstride;
     scratch_dims(cap, bcap, tcap, sstride);
     CK(ctx->scratch.reserve(3 * sstride));
-    CK(cudaMemcpyAsync(dm->boxes, boxes, sizeof(boxes), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dm->boxes, boxes, 3 * sizeof(SampleBox), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(dm->evals, evals, sizeof(ProxyEval) * ne, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
     const float R = mx - mn;
@@ -1052,6 +1078,13 @@ int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const
         slope_out = psnr_diff / h1_diff;
     }
     return ASZ_OK;
+}
+
+int default_slope(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const asz_params &p, float abs_eb, float mn,
+                  float mx, const std::vector<float> &cand_t, float &slope_out, float &max_invalid_out, int &reason_out) {
+    SampleBox boxes[3];
+    slope_boxes(dims, p, abs_eb, boxes);
+    return default_slope_on(ctx, d_in, dims, boxes, p, abs_eb, mn, mx, cand_t, slope_out, max_invalid_out, reason_out);
 }
 
 std::vector<float> candidate_t(const asz_params &p) {
@@ -1426,6 +1459,12 @@ struct CoreArgs {
     // Count each round's QB histogram in its kernel and build the stream's Huffman code on the
     // context's builder thread while the later rounds run.
     bool prebuild = false;
+    // Slabs (asz_compress_slab): the geometry options, a hook run before each round's selection
+    // (the halo exchange before axis-0 rounds), and one that makes a rerun decision the same on
+    // every rank (it receives this rank's and returns the agreed one).
+    const SlabGeom *slab = nullptr;
+    std::function<int(u64)> before_round = nullptr;
+    std::function<int(bool &)> agree = nullptr;
 };
 
 // A QB stream's code built during the rounds (ok == false: the encoder counts and builds it).
@@ -1455,7 +1494,7 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
     int rc = 0;
     std::optional<HostScope> hs_prep(std::in_place, ctx, "host:prepare");
     Geometry &G = o.G;
-    build_geometry(dims, plan, p, abs_eb, slope, quintic, G, a.origin);
+    build_geometry(dims, plan, p, abs_eb, slope, quintic, G, a.origin, a.slab);
     if (!kernel_limits_ok(G)) return fail(ctx, ASZ_E_UNSUPPORTED, "field too large for the round kernels' 32-bit line indexing");
     u64 qb_sum = G.pivots;
     for (auto &rg : G.rounds) qb_sum += rg.qb_total;
@@ -1718,6 +1757,10 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
             const RoundGeom &rg = G.rounds[l];
             const ClassInfo *cls = ctx->classes.as<ClassInfo>() + 27 * l;
             const uint32_t nov = (uint32_t)(overrides.size() / 3);
+            if (a.before_round) {
+                rc = a.before_round(l);
+                if (rc) return rc;
+            }
             if (a.t_given) {
                 // The caller's t codes replace the coefficient selection.
                 CK(launch_tval_from_codes(d_tint, G.nblocks, (uint32_t)L, (uint32_t)l, (float)p.t_precision, d_tval, st));
@@ -1804,9 +1847,8 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
         fb_total = words[1];
         uint32_t namb = words[2];
         if (namb > amb_cap) return fail(ctx, ASZ_E_UNSUPPORTED, "too many ambiguous coefficient decisions");
-        if (namb == 0) break;
         ambs.resize(namb);
-        CK(cudaMemcpy(ambs.data(), ctx->amb.p, namb * sizeof(AmbiguousRecord), cudaMemcpyDeviceToHost));
+        if (namb) CK(cudaMemcpy(ambs.data(), ctx->amb.p, namb * sizeof(AmbiguousRecord), cudaMemcpyDeviceToHost));
         bool changed = false;
         for (const AmbiguousRecord &r : ambs) {
             float t = replay_decision(r, G.rounds[r.round].slope);
@@ -1820,6 +1862,10 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
                 overrides.push_back(bits);
                 changed = true;
             }
+        }
+        if (a.agree) {
+            rc = a.agree(changed);
+            if (rc) return rc;
         }
         if (!changed) break;
         if (++reruns > 16) return fail(ctx, ASZ_E_DEVICE, "coefficient decisions did not settle");
@@ -3803,6 +3849,679 @@ extern "C" int asz_compress_batch_with_t(asz_ctx *ctx, uint32_t count, const flo
 
 // ---------------------------------------------------------------------------------------------
 // Internal interface for the other C-ABI translation units (host/internal.h).
+
+// ---------------------------------------------------------------------------------------------
+// One field over several ranks (asz_compress_slab). Each rank holds a slab of axis-0 blocks and
+// runs the single-field core on a frame: [halo planes | the face plane of the slab below | its
+// planes], with the frame origin at the face, so blocks, targets, sample boxes and stencil cases
+// are those of the same blocks in the whole field (compress.tpp:179-209 walks the blocks in raster
+// order; a slab's blocks are contiguous in every stream). The halo is at least two pivot strides
+// deep (quintic stencils reach 2.5 strides below a target, cubic 1.5) or reaches plane 0.
+
+namespace {
+
+struct SlabLayout {
+    u64 ps0 = 1, bs0 = 1, blocks0 = 0;  // axis 0: pivot stride, block shape, block count
+    u64 s0 = 0;                          // global plane of the slab's lower face (block_begin * bs0)
+    u64 last = 0;                        // global plane of its upper face (inclusive)
+    u64 plane_begin = 0, plane_count = 0;
+    u64 halo = 0;                        // planes below the face in the frame (0 for the first slab)
+    u64 local0 = 0;                      // frame planes: halo + face + owned
+};
+
+int slab_layout(const uint64_t dims[3], const Plan &plan, const asz_params &p, u64 b0, u64 b1, SlabLayout &S,
+                std::string &err) {
+    S = SlabLayout{};
+    for (int d : plan.dir)
+        if (d == 0) S.ps0 *= 2;
+    S.bs0 = S.ps0 * p.block_pivot_ratio;
+    S.blocks0 = (dims[0] + S.bs0 - 1) / S.bs0;
+    if (b0 >= b1 || b1 > S.blocks0) {
+        err = "slab blocks [" + std::to_string(b0) + ", " + std::to_string(b1) + ") outside the field's " +
+              std::to_string(S.blocks0) + " axis-0 blocks";
+        return ASZ_E_ARG;
+    }
+    S.s0 = b0 * S.bs0;
+    S.last = b1 == S.blocks0 ? dims[0] - 1 : b1 * S.bs0;
+    S.plane_begin = b0 == 0 ? 0 : S.s0 + 1;
+    S.plane_count = S.last + 1 - S.plane_begin;
+    S.halo = b0 == 0 ? 0 : std::min<u64>(S.s0, 2 * S.ps0);
+    S.local0 = b0 == 0 ? S.plane_count : S.halo + 1 + S.plane_count;
+    return ASZ_OK;
+}
+
+// The caller's collectives (a single rank needs none).
+struct SlabComm {
+    asz_ctx *ctx;
+    const asz_comm *c;
+    int allreduce(void *buf, u64 n, int dtype, int op) {
+        if (c->size == 1 || n == 0) return ASZ_OK;
+        return c->allreduce(c->user, buf, n, dtype, op) ? fail(ctx, ASZ_E_COMM, "slab: allreduce failed") : ASZ_OK;
+    }
+    int allgather(const void *send, u64 bytes, void *recv) {
+        if (c->size == 1) {
+            std::memcpy(recv, send, bytes);
+            return ASZ_OK;
+        }
+        return c->allgather(c->user, send, bytes, recv) ? fail(ctx, ASZ_E_COMM, "slab: allgather failed") : ASZ_OK;
+    }
+    int send(const void *buf, u64 bytes, int dst) {
+        return c->send(c->user, buf, bytes, dst) ? fail(ctx, ASZ_E_COMM, "slab: send failed") : ASZ_OK;
+    }
+    int recv(void *buf, u64 bytes, int src) {
+        return c->recv(c->user, buf, bytes, src) ? fail(ctx, ASZ_E_COMM, "slab: recv failed") : ASZ_OK;
+    }
+    // Every rank learns whether any rank failed (rc nonzero), so that none waits in a later
+    // exchange for a rank that returned.
+    int agree_ok(int rc) {
+        int32_t bad = rc ? 1 : 0;
+        const int e = allreduce(&bad, 1, 2, 2);
+        if (e) return e;
+        if (rc) return rc;
+        return bad ? fail(ctx, ASZ_E_COMM, "slab: another rank failed") : ASZ_OK;
+    }
+};
+
+// The field's range from every slab's: the first smallest and the last largest value in raster
+// order (std::minmax_element, s1_compress.cpp:131-137), so equal extremes keep the sign of zero of
+// the lowest rank's minimum and the highest rank's maximum.
+int slab_range(SlabComm &cm, float mn, float mx, float &gmn, float &gmx) {
+    const int R = cm.c->size;
+    float mine[2] = {mn, mx};
+    std::vector<float> all(2 * R);
+    int rc = cm.allgather(mine, sizeof(mine), all.data());
+    if (rc) return rc;
+    gmn = all[0];
+    gmx = all[1];
+    for (int r = 1; r < R; r++) {
+        if (all[2 * r] < gmn) gmn = all[2 * r];
+        if (all[2 * r + 1] >= gmx) gmx = all[2 * r + 1];
+    }
+    return ASZ_OK;
+}
+
+// get_default_slope over the whole field from the slabs: the three global sample boxes
+// (slope_boxes) and, per sample, the seven values along the box's direction around it (offsets
+// -3..3; the AB map reads -3, -1, 0, 1, 3). Each rank gathers the values in its planes, all ranks
+// exchange them, and each evaluates the boxes on one compact array that keeps the samples' order:
+// direction d's block holds its samples' lattice with axis d widened seven-fold, the blocks
+// stacked along axis 0. Every rank computes the same slope.
+int slab_slope(asz_ctx *ctx, SlabComm &cm, const float *d_local, const uint64_t ldims[3], u64 local_first_plane,
+               u64 own_lo, u64 own_hi, const uint64_t dims[3], const asz_params &p, float abs_eb, float mn, float mx,
+               const std::vector<float> &cand, float &slope, float &max_invalid, int &reason) {
+    SampleBox gb[3];
+    slope_boxes(dims, p, abs_eb, gb);
+    u64 cnt[3][3], D[3][3], off0[3], M1 = 1, M2 = 1, T0 = 0;
+    for (int d = 0; d < 3; d++) {
+        for (int a = 0; a < 3; a++) {
+            cnt[d][a] = gb[d].hi[a] > gb[d].lo[a] ? (gb[d].hi[a] - gb[d].lo[a] + gb[d].step[a] - 1) / gb[d].step[a] : 0;
+            D[d][a] = cnt[d][a] * (a == d ? 7 : 1);
+        }
+        off0[d] = T0;
+        T0 += D[d][0];
+        M1 = std::max<u64>(M1, D[d][1]);
+        M2 = std::max<u64>(M2, D[d][2]);
+    }
+    const u64 total = std::max<u64>(T0, 1) * M1 * M2;
+    // Entries of this rank: compact index and local field index.
+    std::vector<u64> cidx, lidx;
+    const u64 n1n2 = dims[1] * dims[2];
+    for (int d = 0; d < 3; d++)
+        for (u64 k0 = 0; k0 < cnt[d][0]; k0++)
+            for (u64 k1 = 0; k1 < cnt[d][1]; k1++)
+                for (u64 k2 = 0; k2 < cnt[d][2]; k2++)
+                    for (int o = 0; o < 7; o++) {
+                        const u64 kk[3] = {k0, k1, k2};
+                        int64_t g[3];
+                        u64 c[3];
+                        for (int a = 0; a < 3; a++) {
+                            g[a] = (int64_t)(gb[d].lo[a] + kk[a] * gb[d].step[a]) + (a == d ? o - 3 : 0);
+                            c[a] = a == d ? 7 * kk[a] + o : kk[a];
+                        }
+                        if (g[0] < (int64_t)own_lo || g[0] > (int64_t)own_hi) continue;
+                        if (g[d] < 0 || g[d] >= (int64_t)dims[d]) continue;
+                        cidx.push_back(((off0[d] + c[0]) * M1 + c[1]) * M2 + c[2]);
+                        lidx.push_back(((u64)g[0] - local_first_plane) * n1n2 + (u64)g[1] * dims[2] + (u64)g[2]);
+                    }
+    cudaStream_t st = ctx->stream;
+    std::vector<float> vals(cidx.size());
+    if (!cidx.empty()) {
+        CK(ctx->slab_idx.reserve(lidx.size() * sizeof(u64)));
+        CK(ctx->slab_val.reserve(lidx.size() * sizeof(float)));
+        CK(cudaMemcpyAsync(ctx->slab_idx.p, lidx.data(), lidx.size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+        CK(launch_gather(d_local, ctx->slab_idx.as<u64>(), lidx.size(), ctx->slab_val.as<float>(), st));
+        CK(cudaMemcpyAsync(vals.data(), ctx->slab_val.p, vals.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    (void)ldims;
+    // Exchange: every rank's (count, then indices and values padded to the largest count).
+    const int R = cm.c->size;
+    u64 mine = cidx.size();
+    std::vector<u64> counts(R);
+    int rc = cm.allgather(&mine, sizeof(u64), counts.data());
+    if (rc) return rc;
+    const u64 cmax = *std::max_element(counts.begin(), counts.end());
+    std::vector<u64> sidx(cmax, 0), ridx(cmax * R);
+    std::vector<float> sval(cmax, 0.0f), rval(cmax * R);
+    std::copy(cidx.begin(), cidx.end(), sidx.begin());
+    std::copy(vals.begin(), vals.end(), sval.begin());
+    if ((rc = cm.allgather(sidx.data(), cmax * sizeof(u64), ridx.data()))) return rc;
+    if ((rc = cm.allgather(sval.data(), cmax * sizeof(float), rval.data()))) return rc;
+    std::vector<float> cmp(total, 0.0f);
+    for (int r = 0; r < R; r++)
+        for (u64 k = 0; k < counts[r]; k++) {
+            const u64 ci = ridx[(u64)r * cmax + k];
+            if (ci >= total) return fail(ctx, ASZ_E_COMM, "slab: default-slope sample index out of range");
+            cmp[ci] = rval[(u64)r * cmax + k];
+        }
+    CK(ctx->slab_cmp.reserve(total * sizeof(float)));
+    CK(cudaMemcpyAsync(ctx->slab_cmp.p, cmp.data(), total * sizeof(float), cudaMemcpyHostToDevice, st));
+    SampleBox cb[3];
+    const uint64_t cdims[3] = {std::max<u64>(T0, 1), M1, M2};
+    for (int d = 0; d < 3; d++) {
+        cb[d] = gb[d];
+        for (int a = 0; a < 3; a++) {
+            const u64 base = a == 0 ? off0[d] : 0;
+            cb[d].lo[a] = base + (a == d ? 3 : 0);
+            cb[d].step[a] = a == d ? 7 : 1;
+            cb[d].hi[a] = cnt[d][a] ? cb[d].lo[a] + (cnt[d][a] - 1) * cb[d].step[a] + 1 : cb[d].lo[a];
+        }
+        cb[d].dist = d == 0 ? M1 * M2 : d == 1 ? M2 : 1;
+    }
+    return default_slope_on(ctx, ctx->slab_cmp.as<float>(), cdims, cb, p, abs_eb, mn, mx, cand, slope, max_invalid, reason);
+}
+
+}  // namespace
+
+namespace {
+
+// Appends `bits` bits of src (LSB-first, zero past the last bit) to dst at bit offset off; dst is
+// zero from off on and holds dst_len bytes.
+void bit_append(uint8_t *dst, u64 dst_len, u64 off, const uint8_t *src, u64 bits) {
+    const u64 nb = (bits + 7) / 8;
+    const unsigned sh = (unsigned)(off & 7);
+    const u64 b0 = off / 8;
+    for (u64 i = 0; i < nb && b0 + i < dst_len; i++) {
+        dst[b0 + i] |= (uint8_t)(src[i] << sh);
+        if (sh && b0 + i + 1 < dst_len) dst[b0 + i + 1] |= (uint8_t)(src[i] >> (8 - sh));
+    }
+}
+
+// The entropy stage of a slab (compress.tpp:233-291 over the whole field): global ranges, counts
+// and histograms from every rank's, the same codes on every rank, each rank's pieces encoded on
+// its device, and on rank 0 the pieces concatenated bit-exactly in rank order (each stream's
+// pieces are consecutive symbols of it) and the stream assembled.
+int slab_encode(asz_ctx *ctx, SlabComm &cm, const CoreOut &co, const Plan &plan, const asz_params &p, float mn, float mx,
+                bool quintic, asz_report &R) {
+    cudaStream_t st = ctx->stream;
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    const Geometry &G = co.G;
+    const u64 L = plan.pred.size(), NS = L + 2;
+    const int rank = cm.c->rank, nr = cm.c->size;
+    auto t_huff = clk::now();
+    // Per stream (0: t codes, 1..L+1: QB streams): local count, global range and count.
+    std::vector<StreamOut> so(NS);
+    std::vector<u64> local(NS), global(NS);
+    std::vector<int32_t> rng(2 * (L + 1));
+    CK(cudaMemcpyAsync(rng.data(), dm->qb_range, rng.size() * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int32_t> rlo(L + 1), rhi(L + 1);
+    for (u64 s = 0; s <= L; s++) {
+        rlo[s] = rng[2 * s];
+        rhi[s] = rng[2 * s + 1];
+    }
+    int rc;
+    if ((rc = cm.allreduce(rlo.data(), L + 1, 2, 1))) return rc;
+    if ((rc = cm.allreduce(rhi.data(), L + 1, 2, 2))) return rc;
+    local[0] = G.nblocks * L;
+    for (u64 s = 0; s <= L; s++) local[s + 1] = co.qb_len[s];
+    global = local;
+    if ((rc = cm.allreduce(global.data(), NS, 1, 0))) return rc;
+    {
+        const float t_default = 4.0f / 16;
+        const float tv[6] = {t_default, 1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+        for (float t : tv) {
+            const int64_t c = host_lround_f(t * (float)p.t_precision);
+            lo = std::min(lo, c);
+            hi = std::max(hi, c);
+        }
+        so[0].lo = lo;
+        so[0].hi = hi;
+    }
+    for (u64 s = 0; s <= L; s++) {
+        so[s + 1].lo = rlo[s];
+        so[s + 1].hi = rhi[s];
+    }
+    u64 hist_total = 0;
+    for (u64 s = 0; s < NS; s++) {
+        so[s].count = global[s];
+        if (!global[s]) continue;
+        const u64 range = (u64)(so[s].hi - so[s].lo) + 1;
+        if (range > (1ull << 27)) return fail(ctx, ASZ_E_UNSUPPORTED, "QB range too wide for the dense histogram");
+        so[s].hist_off = hist_total;
+        hist_total += range;
+    }
+    CK(ctx->hist.reserve(std::max<u64>(hist_total, 1) * 8));
+    CK(cudaMemsetAsync(ctx->hist.p, 0, std::max<u64>(hist_total, 1) * 8, st));
+    unsigned long long *d_hist = ctx->hist.as<unsigned long long>();
+    for (u64 s = 0; s < NS; s++) {
+        if (!global[s] || !local[s]) continue;
+        const u64 range = (u64)(so[s].hi - so[s].lo) + 1;
+        if (s == 0) CK(launch_histogram<int64_t>(ctx->tint.as<int64_t>(), local[0], so[0].lo, range, d_hist + so[0].hist_off, st));
+        else
+            CK(launch_histogram<int32_t>(ctx->qb.as<int32_t>() + co.qb_off[s - 1], local[s], so[s].lo, range,
+                                         d_hist + so[s].hist_off, st));
+    }
+    std::vector<u64> lhist(hist_total), ghist;
+    if (hist_total) CK(cudaMemcpyAsync(lhist.data(), d_hist, hist_total * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ghist = lhist;
+    if ((rc = cm.allreduce(ghist.data(), hist_total, 1, 0))) return rc;
+    // The same codes on every rank, and this rank's payload bits per stream.
+    std::vector<u64> lbits(NS, 0);
+    for (u64 s = 0; s < NS; s++) {
+        StreamOut &o = so[s];
+        if (!o.count) continue;
+        const u64 range = (u64)(o.hi - o.lo) + 1;
+        const u64 *h = ghist.data() + o.hist_off;
+        u64 a0 = 0, b0 = range;
+        while (a0 < b0 && h[a0] == 0) a0++;
+        while (b0 > a0 && h[b0 - 1] == 0) b0--;
+        std::vector<u64> hh(h + a0, h + b0);
+        std::string err;
+        if (!build_code(hh, o.lo + (int64_t)a0, o.lo + (int64_t)b0 - 1, o.count, s == 0, o.code, err))
+            return fail(ctx, ASZ_E_UNSUPPORTED, err);
+        const int64_t old_lo = o.lo;
+        o.lo += (int64_t)a0;
+        if (o.code.maxval == 1) continue;
+        const u64 *lh = lhist.data() + o.hist_off;
+        for (u64 k = a0; k < b0; k++)
+            if (lh[k]) lbits[s] += lh[k] * o.code.table[(u64)(old_lo + (int64_t)k - o.code.offset)].len;
+    }
+    // Encode this rank's pieces.
+    u64 code_total = 0, words_total = 0;
+    std::vector<u64> code_off(NS, 0), word_off(NS, 0);
+    for (u64 s = 0; s < NS; s++) {
+        if (!so[s].count) continue;
+        code_off[s] = code_total;
+        code_total += so[s].code.table.size();
+        word_off[s] = words_total;
+        words_total += (lbits[s] + 31) / 32 + 2;
+    }
+    std::vector<CodeEntry> codes(std::max<u64>(code_total, 1));
+    for (u64 s = 0; s < NS; s++)
+        if (so[s].count) std::copy(so[s].code.table.begin(), so[s].code.table.end(), codes.begin() + code_off[s]);
+    CK(ctx->codes.reserve(codes.size() * sizeof(CodeEntry)));
+    CK(cudaMemcpyAsync(ctx->codes.p, codes.data(), codes.size() * sizeof(CodeEntry), cudaMemcpyHostToDevice, st));
+    CK(ctx->payload.reserve(std::max<u64>(words_total, 1) * 4));
+    CK(cudaMemsetAsync(ctx->payload.p, 0, std::max<u64>(words_total, 1) * 4, st));
+    uint32_t *d_pay = ctx->payload.as<uint32_t>();
+    CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
+    {
+        std::vector<EncStream> es[2];
+        std::vector<u64> toff[2] = {{0}, {0}};
+        for (u64 s = 0; s < NS; s++) {
+            if (!so[s].count || so[s].code.maxval == 1 || !local[s]) continue;
+            const int k = s == 0 ? 1 : 0;
+            const void *sym = s == 0 ? (const void *)ctx->tint.as<int64_t>() : (const void *)(ctx->qb.as<int32_t>() + co.qb_off[s - 1]);
+            es[k].push_back(EncStream{sym, local[s], so[s].lo, d_codes + code_off[s], d_pay + word_off[s]});
+            const u64 tile = k ? enc_tile<int64_t>() : enc_tile<int32_t>();
+            toff[k].push_back(toff[k].back() + (local[s] + tile - 1) / tile);
+        }
+        u64 off[2][4], bytes = 0;
+        auto place = [&](u64 n) {
+            const u64 o = bytes;
+            bytes += (n + 15) / 16 * 16;
+            return o;
+        };
+        size_t tmp_bytes = 0;
+        for (int k = 0; k < 2; k++) {
+            const u64 nt = toff[k].back();
+            off[k][0] = place(es[k].size() * sizeof(EncStream));
+            off[k][1] = place(toff[k].size() * sizeof(u64));
+            off[k][2] = place((nt + 1) * sizeof(u64));
+            off[k][3] = place((nt + 1) * sizeof(u64));
+            size_t tb = 0;
+            if (k == 0) CK(launch_encode_tiles<int32_t>(nullptr, 0, nullptr, nt, nullptr, nullptr, nullptr, tb, st));
+            else CK(launch_encode_tiles<int64_t>(nullptr, 0, nullptr, nt, nullptr, nullptr, nullptr, tb, st));
+            tmp_bytes = std::max(tmp_bytes, tb);
+        }
+        CK(ctx->enc.reserve(std::max<u64>(bytes, 16)));
+        CK(ctx->cubtmp.reserve(std::max<size_t>(tmp_bytes, 16)));
+        uint8_t *eb = ctx->enc.as<uint8_t>();
+        for (int k = 0; k < 2; k++) {
+            const u64 nt = toff[k].back();
+            if (!nt) continue;
+            CK(cudaMemcpyAsync(eb + off[k][0], es[k].data(), es[k].size() * sizeof(EncStream), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(eb + off[k][1], toff[k].data(), toff[k].size() * sizeof(u64), cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(eb + off[k][2] + nt * sizeof(u64), 0, sizeof(u64), st));
+            size_t tb = ctx->cubtmp.cap;
+            const EncStream *E = (const EncStream *)(eb + off[k][0]);
+            const u64 *T = (const u64 *)(eb + off[k][1]);
+            u64 *tbits = (u64 *)(eb + off[k][2]), *tscan = (u64 *)(eb + off[k][3]);
+            if (k == 0) CK(launch_encode_tiles<int32_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
+            else CK(launch_encode_tiles<int64_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
+        }
+    }
+    // This rank's pieces, back on the host: per stream its bits, then the bytes.
+    u64 piece_bytes = 0;
+    for (u64 s = 0; s < NS; s++) piece_bytes += (lbits[s] + 7) / 8;
+    std::vector<uint8_t> piece(std::max<u64>(piece_bytes, 1));
+    {
+        u64 w = 0;
+        for (u64 s = 0; s < NS; s++) {
+            const u64 nb = (lbits[s] + 7) / 8;
+            if (nb) CK(cudaMemcpyAsync(piece.data() + w, d_pay + word_off[s], nb, cudaMemcpyDeviceToHost, st));
+            w += nb;
+        }
+        CK(cudaStreamSynchronize(st));
+    }
+    auto t_d2h = clk::now();
+    if (rank != 0) {
+        if ((rc = cm.send(lbits.data(), NS * sizeof(u64), 0))) return rc;
+        if (piece_bytes && (rc = cm.send(piece.data(), piece_bytes, 0))) return rc;
+        R.huffman_s = secs(t_huff, clk::now());
+        return ASZ_OK;
+    }
+    // Rank 0: every stream's payload from the ranks' pieces, then the stream (compress.tpp:233-291).
+    std::vector<std::vector<uint8_t>> pay(NS);
+    std::vector<u64> at(NS, 0);
+    for (u64 s = 0; s < NS; s++)
+        if (so[s].count && so[s].code.maxval != 1) pay[s].assign((so[s].code.bits + 7) / 8, 0);
+    for (int r = 0; r < nr; r++) {
+        std::vector<u64> bits(NS);
+        std::vector<uint8_t> in;
+        if (r == 0) {
+            bits = lbits;
+            in = piece;
+        } else {
+            if ((rc = cm.recv(bits.data(), NS * sizeof(u64), r))) return rc;
+            u64 nbytes = 0;
+            for (u64 s = 0; s < NS; s++) nbytes += (bits[s] + 7) / 8;
+            in.assign(std::max<u64>(nbytes, 1), 0);
+            if (nbytes && (rc = cm.recv(in.data(), nbytes, r))) return rc;
+        }
+        u64 rd = 0;
+        for (u64 s = 0; s < NS; s++) {
+            const u64 nb = (bits[s] + 7) / 8;
+            if (bits[s]) {
+                if (pay[s].empty() || at[s] + bits[s] > so[s].code.bits)
+                    return fail(ctx, ASZ_E_COMM, "slab: a rank's payload does not fit its stream");
+                bit_append(pay[s].data(), pay[s].size(), at[s], in.data() + rd, bits[s]);
+                at[s] += bits[s];
+            }
+            rd += nb;
+        }
+    }
+    for (u64 s = 0; s < NS; s++)
+        if (so[s].count && so[s].code.maxval != 1 && at[s] != so[s].code.bits)
+            return fail(ctx, ASZ_E_COMM, "slab: the ranks' payload bits do not add up to the stream's");
+    u64 total_len = 9 + 2 * L;
+    for (auto &o : so) total_len += 8 + (o.count ? o.code.save_size() + o.code.encode_size() : 0);
+    PinnedBuf &pb = ctx->pre_zstd;
+    CK(pb.reserve(total_len));
+    pb.len = total_len;
+    uint8_t *w = pb.p;
+    std::memcpy(w, &mn, 4);
+    std::memcpy(w + 4, &mx, 4);
+    w[8] = (uint8_t)(L | 0x40 | (quintic ? 0x80 : 0));
+    w += 9;
+    for (u64 l = 0; l < L; l++) {
+        w[0] = (uint8_t)plan.pred[l][5];
+        w[1] = (uint8_t)plan.pred[l][9];
+        w += 2;
+    }
+    for (u64 s = 0; s < NS; s++) {
+        const StreamOut &o = so[s];
+        for (int i = 0; i < 8; i++) w[i] = (uint8_t)(o.count >> (8 * i));
+        w += 8;
+        if (!o.count) continue;
+        write_tree(o.code, w);
+        w += o.code.save_size();
+        write_len_word(o.code, w);
+        w += 8;
+        if (o.code.maxval != 1) {
+            std::memcpy(w, pay[s].data(), pay[s].size());
+            w += pay[s].size();
+        }
+    }
+    if ((u64)(w - pb.p) != total_len) return fail(ctx, ASZ_E_DEVICE, "Huffman encoded size mismatch");
+    R.d2h_s = secs(t_d2h, clk::now());
+    R.huffman_s = secs(t_huff, clk::now());
+    return ASZ_OK;
+}
+
+}  // namespace
+
+extern "C" int asz_slab_planes(const uint64_t dims[3], const asz_params *pp, const char *plan_text, uint64_t block_begin,
+                               uint64_t block_end, uint64_t *plane_begin, uint64_t *plane_count, uint64_t *blocks0) {
+    if (!dims || !plan_text || !plane_begin || !plane_count) return ASZ_E_ARG;
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    if (p.block_pivot_ratio == 0) return ASZ_E_ARG;
+    Plan plan;
+    std::string err;
+    if (!parse_plan(plan_text, plan, err)) return ASZ_E_ARG;
+    SlabLayout S;
+    const int rc = slab_layout(dims, plan, p, block_begin, block_end, S, err);
+    if (rc) return rc;
+    *plane_begin = S.plane_begin;
+    *plane_count = S.plane_count;
+    if (blocks0) *blocks0 = S.blocks0;
+    return ASZ_OK;
+}
+
+extern "C" int asz_compress_slab(asz_ctx *ctx, const asz_comm *comm, const float *planes, int on_device,
+                                 const uint64_t dims[3], uint64_t block_begin, uint64_t block_end, float rel_eb,
+                                 const asz_params *pp, const char *plan_text, uint8_t **out, size_t *out_len,
+                                 asz_report *rep) {
+    if (!ctx) return ASZ_E_ARG;
+    auto t_start = clk::now();
+    const uint64_t launches0 = launch_counter();
+    ctx->err.clear();
+    ctx->have_last = false;
+    if (!comm || !planes || !out || !out_len || !plan_text) return fail(ctx, ASZ_E_ARG, "null argument");
+    if (comm->size < 1 || comm->rank < 0 || comm->rank >= comm->size ||
+        (comm->size > 1 && (!comm->allreduce || !comm->allgather || !comm->send || !comm->recv)))
+        return fail(ctx, ASZ_E_ARG, "invalid communicator");
+    *out = nullptr;
+    *out_len = 0;
+    asz_params p;
+    if (pp) p = *pp;
+    else asz_default_params(&p);
+    SlabComm cm{ctx, comm};
+    // Argument checks run on every rank before the first exchange, and their outcome is agreed.
+    int rc = validate(ctx, p, true);
+    if (!rc) rc = validate_dims(ctx, dims, rel_eb);
+    Plan plan;
+    std::string perr;
+    if (!rc && !parse_plan(plan_text, plan, perr)) rc = fail(ctx, ASZ_E_ARG, perr);
+    if (!rc && plan.pred.size() > 63) rc = fail(ctx, ASZ_E_ARG, "predictor plan cannot contain more than 63 layers");
+    if (!rc && p.predictor_family == ASZ_FAMILY_AUTO)
+        rc = fail(ctx, ASZ_E_ARG, "a slab needs the predictor family (the selector samples the whole field)");
+    SlabLayout S;
+    if (!rc) {
+        rc = slab_layout(dims, plan, p, block_begin, block_end, S, perr);
+        if (rc) rc = fail(ctx, rc, perr);
+    }
+    // Blocks of consecutive ranks must follow each other: rank r's first block is rank r-1's end.
+    std::vector<u64> bounds(2 * comm->size);
+    {
+        const u64 mine[2] = {block_begin, block_end};
+        const int e = cm.allgather(mine, sizeof(mine), bounds.data());
+        if (e) return e;
+        if (!rc) {
+            if (bounds[0] != 0 || bounds[2 * comm->size - 1] != S.blocks0)
+                rc = fail(ctx, ASZ_E_ARG, "the ranks' slabs must cover the axis-0 blocks from the first to the last");
+            for (int r = 1; r < comm->size && !rc; r++)
+                if (bounds[2 * r] != bounds[2 * r - 1]) rc = fail(ctx, ASZ_E_ARG, "the ranks' slabs must follow each other");
+        }
+    }
+    if (!rc && cudaSetDevice(ctx->device) != cudaSuccess) rc = fail(ctx, ASZ_E_CUDA, "cudaSetDevice");
+    if ((rc = cm.agree_ok(rc))) return rc;
+    const bool quintic = p.predictor_family == ASZ_FAMILY_QUINTIC;
+    const u64 L = plan.pred.size();
+    const u64 n1n2 = dims[1] * dims[2];
+    const int rank = comm->rank, nr = comm->size;
+    cudaStream_t st = ctx->stream;
+    asz_report R{};
+    // The frame: [halo | face | owned planes] (rank 0: its planes from plane 0).
+    const u64 first_plane = rank == 0 || block_begin == 0 ? 0 : S.s0 - S.halo;  // global plane of frame plane 0
+    const u64 own_off = block_begin == 0 ? 0 : S.halo + 1;                      // frame plane of the first owned plane
+    const uint64_t ldims[3] = {S.local0, dims[1], dims[2]};
+    const uint64_t origin[3] = {block_begin == 0 ? 0 : S.halo, 0, 0};
+    auto t0 = clk::now();
+    rc = ASZ_OK;
+    {
+        const cudaError_t e1 = ctx->misc.reserve(sizeof(MiscLayout));
+        const cudaError_t e2 = ctx->in.reserve(S.local0 * n1n2 * sizeof(float));
+        if (e1 != cudaSuccess || e2 != cudaSuccess) rc = fail(ctx, ASZ_E_CUDA, "slab: device allocation failed");
+    }
+    float *d_local = ctx->in.as<float>();
+    if (!rc && own_off) {
+        const cudaError_t e = cudaMemsetAsync(d_local, 0, own_off * n1n2 * sizeof(float), st);
+        if (e != cudaSuccess) rc = fail(ctx, ASZ_E_CUDA, cudaGetErrorString(e));
+    }
+    if (!rc) {
+        const cudaError_t e = cudaMemcpyAsync(d_local + own_off * n1n2, planes, S.plane_count * n1n2 * sizeof(float),
+                                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) rc = fail(ctx, ASZ_E_CUDA, cudaGetErrorString(e));
+        else if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(ctx, ASZ_E_CUDA, "slab: input copy failed");
+    }
+    R.h2d_s = secs(t0, clk::now());
+    // Data range over the owned planes, then over the field.
+    float mn = 0, mx = 0, gmn = 0, gmx = 0;
+    auto t_range = clk::now();
+    if (!rc) rc = compute_range(ctx, d_local + own_off * n1n2, S.plane_count * n1n2, mn, mx);
+    if ((rc = cm.agree_ok(rc))) return rc;
+    if ((rc = slab_range(cm, mn, mx, gmn, gmx))) return rc;
+    R.data_range_s = secs(t_range, clk::now());
+    if (gmn == gmx) return fail(ctx, ASZ_E_DATA, "max_val==min_val");
+    const float abs_eb = rel_eb * (gmx - gmn);
+    // Default slope from the whole field's samples.
+    auto t_slope = clk::now();
+    const std::vector<float> cand = candidate_t(p);
+    float slope = 0, max_invalid = 0;
+    int reason = 0;
+    rc = slab_slope(ctx, cm, d_local, ldims, first_plane, S.plane_begin, S.last, dims, p, abs_eb, gmn, gmx, cand, slope,
+                    max_invalid, reason);
+    if ((rc = cm.agree_ok(rc))) return rc;
+    R.default_slope_s = secs(t_slope, clk::now());
+    // Rounds on the frame; before each axis-0 round, the reconstructed planes below each slab
+    // come from the rank below (received first, then this rank's top planes go up).
+    auto t_core = clk::now();
+    SlabGeom sg{block_end - block_begin, block_begin > 0};
+    CoreOut co;
+    CoreArgs ca{d_local, ldims, origin, &plan, &p, quintic, false, nullptr, gmn, gmx, abs_eb, slope, nullptr, 0};
+    ca.slab = &sg;
+    ca.before_round = [&](u64 l) -> int {
+        if (plan.dir[l] != 0 || nr == 1) return ASZ_OK;
+        float *rec = ctx->rec.as<float>();
+        int e;
+        if (rank > 0) {
+            std::vector<float> h((S.halo + 1) * n1n2);
+            if ((e = cm.recv(h.data(), h.size() * sizeof(float), rank - 1))) return e;
+            CK(cudaMemcpyAsync(rec, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        if (rank < nr - 1) {
+            const u64 up = std::min<u64>(S.last, 2 * S.ps0);  // the halo of the rank above
+            std::vector<float> h((up + 1) * n1n2);
+            CK(cudaMemcpyAsync(h.data(), rec + (S.last - up - first_plane) * n1n2, h.size() * sizeof(float),
+                               cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if ((e = cm.send(h.data(), h.size() * sizeof(float), rank + 1))) return e;
+        }
+        return ASZ_OK;
+    };
+    ca.agree = [&](bool &changed) -> int {
+        int32_t c = changed ? 1 : 0;
+        const int e = cm.allreduce(&c, 1, 2, 2);
+        changed = c != 0;
+        return e;
+    };
+    rc = run_core(ctx, ca, co, R);
+    if ((rc = cm.agree_ok(rc))) return rc;
+    rc = slab_encode(ctx, cm, co, plan, p, gmn, gmx, quintic, R);
+    if ((rc = cm.agree_ok(rc))) return rc;
+    R.core_s = secs(t_core, clk::now());
+    // zstd level 3 on rank 0 (compress.tpp:294-299).
+    u64 lens[2] = {0, 0};
+    if (rank == 0) {
+        auto t_z = clk::now();
+        PinnedBuf &pb = ctx->pre_zstd;
+        const size_t bound = ZSTD_compressBound(pb.len);
+        uint8_t *z = out_alloc(bound);
+        size_t zl = 0;
+        if (!z) rc = fail(ctx, ASZ_E_DATA, "out of host memory");
+        else {
+            zl = zstd3(ctx, z, bound, pb.p, pb.len);
+            if (ZSTD_isError(zl)) {
+                out_release(z);
+                rc = fail(ctx, ASZ_E_DATA, std::string("ZSTD_compress: ") + ZSTD_getErrorName(zl));
+            } else {
+                *out = z;
+                *out_len = zl;
+                lens[0] = pb.len;
+                lens[1] = zl;
+            }
+        }
+        R.zstd_s = secs(t_z, clk::now());
+    }
+    {
+        const int e = cm.agree_ok(rc);
+        if (e) {
+            if (*out) out_release(*out);
+            *out = nullptr;
+            *out_len = 0;
+            return e;
+        }
+    }
+    // The whole field's figures on every rank.
+    u64 sums[8] = {lens[0], lens[1], R.t_fallback_count, R.ambiguous_decisions, R.exact_groups, R.serial_groups,
+                   R.exact_undecided, R.wide_groups};
+    if ((rc = cm.allreduce(sums, 8, 1, 0))) return rc;
+    if (rep) {
+        R.min_val = gmn;
+        R.max_val = gmx;
+        R.abs_eb = abs_eb;
+        R.default_slope = slope;
+        R.slope_max_invalid_ratio = max_invalid;
+        R.slope_fallback_reason = reason;
+        R.pre_zstd_len = sums[0];
+        R.asz_len = sums[1];
+        R.t_fallback_count = sums[2];
+        R.ambiguous_decisions = sums[3];
+        R.exact_groups = sums[4];
+        R.serial_groups = sums[5];
+        R.exact_undecided = sums[6];
+        R.wide_groups = sums[7];
+        R.layer_num = L;
+        R.quintic = quintic ? 1 : 0;
+        R.pivot_stride[0] = (uint32_t)co.G.fg.pivot_stride[0];
+        R.block_shape[0] = (uint32_t)co.G.fg.block_shape[0];
+        R.block_num[0] = (uint32_t)S.blocks0;
+        for (int a = 1; a < 3; a++) {
+            R.pivot_stride[a] = (uint32_t)co.G.fg.pivot_stride[a];
+            R.block_shape[a] = (uint32_t)co.G.fg.block_shape[a];
+            R.block_num[a] = (uint32_t)co.G.fg.block_num[a];
+        }
+        std::string pl;
+        for (u64 l = 0; l < L; l++) pl += (l ? "," : "") + plan.pred[l];
+        std::snprintf(R.plan, sizeof(R.plan), "%s", pl.c_str());
+        const u64 N = dims[0] * n1n2;
+        if (sums[1]) {
+            R.cr = (float)N * sizeof(float) / (float)sums[1];
+            R.br = 8 * sizeof(float) / R.cr;
+        }
+        R.kernel_launches = launch_counter() - launches0;
+        R.total_s = secs(t_start, clk::now());
+        *rep = R;
+    }
+    return ASZ_OK;
+}
 
 namespace asz::host {
 

@@ -646,6 +646,20 @@ __global__ void copy_box_kernel(const float *__restrict__ in, uint64_t n1, uint6
 }
 }  // namespace
 
+// out[k] = in[idx[k]]: the default slope's sample neighbourhoods of a slab (asz_compress_slab).
+__global__ void gather_kernel(const float *__restrict__ in, const uint64_t *__restrict__ idx, uint64_t n,
+                              float *__restrict__ out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        out[k] = in[idx[k]];
+}
+
+cudaError_t launch_gather(const float *in, const uint64_t *idx, uint64_t n, float *out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    gather_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(in, idx, n, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_copy_box(const float *in, const uint64_t n[3], const uint64_t lo[3], const uint64_t m[3], float *out,
                             cudaStream_t st) {
     const uint64_t total = m[0] * m[1] * m[2];

@@ -143,6 +143,8 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
                               uint32_t cap, unsigned grid, cudaStream_t st);
 cudaError_t launch_copy_box(const float *in, const uint64_t n[3], const uint64_t lo[3], const uint64_t m[3], float *out,
                             cudaStream_t st);
+// out[k] = in[idx[k]] for k < n.
+cudaError_t launch_gather(const float *in, const uint64_t *idx, uint64_t n, float *out, cudaStream_t st);
 cudaError_t launch_plan_sample(const float *d, uint64_t n1, uint64_t n2, const PlanCand *cands, uint32_t ncands, uint64_t total,
                                int32_t *qb, float *e, int32_t *qb_range, cudaStream_t st);
 cudaError_t launch_plan_mse(const PlanCand *cands, uint32_t ncands, const float *e, float *mse, cudaStream_t st);

@@ -35,6 +35,7 @@ extern "C" {
 #define ASZ_E_CUDA -3     /* CUDA runtime error */
 #define ASZ_E_DEVICE -4   /* a kernel reported an inconsistency through its error word */
 #define ASZ_E_UNSUPPORTED -5
+#define ASZ_E_COMM -6     /* a caller's collective (asz_comm) failed */
 
 /* Predictor family: ASZ_FAMILY_AUTO runs the reference's selector (predictor_family.tpp). */
 #define ASZ_FAMILY_AUTO -1
@@ -223,6 +224,49 @@ int asz_compress_batch_with_t(asz_ctx *ctx, uint32_t count, const float *const *
                               const uint64_t *dims, float rel_eb, const asz_params *p, const char *plan,
                               const int64_t *const *t_tables, const uint64_t *t_lens, uint8_t **out, size_t *out_len,
                               asz_report *reps, asz_batch_report *brep);
+
+/* ---------------------------------------------------------------------------------------------
+ * One field compressed by several ranks (one process per GPU), each holding a slab of axis-0
+ * planes cut at block boundaries, for fields larger than one GPU's memory. The reference walks
+ * the blocks of one field in raster order (compress.tpp:179-209); a slab is a run of axis-0
+ * blocks, whose blocks are contiguous in every stream, so the ranks' stream pieces concatenated in
+ * rank order are the single-field streams and rank 0's .asz is byte-identical to asz_compress's.
+ * Exchanges: the data range (all ranks), the default slope's samples (all ranks), before each
+ * axis-0 round the reconstructed planes just below each slab (from the rank below), the rerun
+ * decision of the coefficient replay, the QB ranges and histograms (all ranks build the same
+ * codes), and each rank's encoded pieces (to rank 0). The plan and the family must be given
+ * (the plan search and the family selector sample the whole field). */
+
+/* The caller's collectives over host buffers; each returns 0 on success. The library stages
+ * device data through host memory and calls them in the same order on every rank. */
+typedef struct asz_comm {
+    int rank, size;
+    void *user;
+    /* In-place reduction over all ranks of count values: dtype 0 float32, 1 uint64, 2 int32;
+     * op 0 sum, 1 min, 2 max. */
+    int (*allreduce)(void *user, void *buf, uint64_t count, int dtype, int op);
+    /* Each rank contributes `bytes` bytes; recv (size * bytes) receives them in rank order. */
+    int (*allgather)(void *user, const void *send, uint64_t bytes, void *recv);
+    int (*send)(void *user, const void *buf, uint64_t bytes, int dst);
+    int (*recv)(void *user, void *buf, uint64_t bytes, int src);
+} asz_comm;
+
+/* The axis-0 planes a rank passes for its blocks [block_begin, block_end) of the plan's axis-0
+ * blocks: planes [plane_begin, plane_begin + plane_count). Rank 0's slab starts at plane 0; any
+ * other slab starts one plane past its first block's lower face, which belongs to the slab below.
+ * blocks0 (optional) receives the field's number of axis-0 blocks. */
+int asz_slab_planes(const uint64_t dims[3], const asz_params *p, const char *plan, uint64_t block_begin,
+                    uint64_t block_end, uint64_t *plane_begin, uint64_t *plane_count, uint64_t *blocks0);
+
+/* Compress this rank's slab: `planes` holds plane_count x dims[1] x dims[2] floats (host, or
+ * device when on_device) as asz_slab_planes gives them; dims are the whole field's. Every rank
+ * calls it with its own blocks; the blocks of all ranks, in rank order, cover the axis-0 blocks
+ * exactly. Rank 0 receives the .asz in out/out_len (asz_free it); other ranks receive NULL/0.
+ * rep (optional): the whole field's figures on every rank. A rank that fails returns nonzero;
+ * the others then fail in their next exchange (the caller's collectives should time out). */
+int asz_compress_slab(asz_ctx *ctx, const asz_comm *comm, const float *planes, int on_device, const uint64_t dims[3],
+                      uint64_t block_begin, uint64_t block_end, float rel_eb, const asz_params *p, const char *plan,
+                      uint8_t **out, size_t *out_len, asz_report *rep);
 
 /* Decompress .asz bytes into `out` (prod(dims) floats; host pointer, or device pointer when
  * out_on_device is nonzero). */
