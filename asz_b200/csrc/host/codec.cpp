@@ -230,6 +230,7 @@ struct asz_ctx {
     std::vector<cudaEvent_t> round_ev;
     DevBuf hwin;          // per QB stream of the rounds: kHistWin 64-bit bins
     DevBuf slab_idx, slab_val, slab_cmp;  // slabs: slope-sample indices, gathered values, compact copy
+    DevBuf gscratch, spill2;  // exact replay of groups larger than shared memory: working sets, what is left
     PinnedBuf hwin_host;  // their copies, with each stream's [min, max] and overflow word
     std::unique_ptr<SerialWorker> builder;
     std::string err;
@@ -748,6 +749,15 @@ uint32_t exact_cap() {
     return cap;
 }
 
+// Bytes of one CTA's slice of the global scratch for exact replays of up to cap samples.
+u64 exact_global_stride(uint32_t cap) { return ((u64)exact_smem_bytes(cap) + 255) / 256 * 256; }
+
+// AB maps larger than shared memory holds (dm->boxes, dm->evals uploaded): the exact kernel with
+// each box's working set in global scratch, a CTA per box. done is false when a box needs the
+// serial kernel (a key outside int32); the error word is then cleared for it.
+int abmap_exact_global(asz_ctx *ctx, uint32_t ne, const float *field, u64 n1n2, u64 n2, float R2, uint32_t cap, uint32_t nb,
+                       const char *prof_name, bool &done);
+
 // Replays one ambiguous decision with glibc log10f (compress.tpp:127-142).
 float replay_decision(const AmbiguousRecord &r, float slope) {
     const float cand[5] = {1.0f / 16, 1.0f / 4, 9.0f / 32, 5.0f / 16, 11.0f / 32};
@@ -826,6 +836,8 @@ void asz_destroy(asz_ctx *c) {
     c->slab_idx.release();
     c->slab_val.release();
     c->slab_cmp.release();
+    c->gscratch.release();
+    c->spill2.release();
     for (DevBuf *b : {&c->in, &c->rec, &c->qb, &c->tval, &c->tint, &c->misc, &c->scratch, &c->log2arena, &c->hist, &c->codes,
                       &c->bitoff, &c->cubtmp, &c->payload, &c->amb, &c->overrides, &c->classes, &c->axis, &c->pre, &c->chunks,
                       &c->out, &c->proxies, &c->tlist, &c->spill, &c->iota, &c->plan_qb, &c->plan_e, &c->plan_aux,
@@ -884,6 +896,7 @@ struct MiscLayout {  // small device words, one allocation
     uint32_t changed;
     uint32_t list_count[64];
     uint32_t spill_count[64];
+    uint32_t spill2_count[64];  // groups the global-scratch exact kernel left to the serial one
     uint32_t all_count;
     uint32_t why[3];  // fast path: [0] handed off (bins too spread), [1] handed off (undecided), [2] settled window by window
     uint32_t dec_err;      // batched Huffman decoding: error bits
@@ -897,6 +910,26 @@ struct MiscLayout {  // small device words, one allocation
     SampleBox boxes[3];
     ProxyEval evals[64];
 };
+
+int abmap_exact_global(asz_ctx *ctx, uint32_t ne, const float *field, u64 n1n2, u64 n2, float R2, uint32_t cap, uint32_t nb,
+                       const char *prof_name, bool &done) {
+    MiscLayout *dm = ctx->misc.as<MiscLayout>();
+    cudaStream_t st = ctx->stream;
+    const u64 stride = exact_global_stride(cap);
+    CK(ctx->gscratch.reserve(nb * stride));
+    CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+    {
+        ProfScope ps(ctx, prof_name, 0);
+        CK(launch_slope_exact_global(dm->boxes, dm->evals, ne, field, n1n2, n2, ctx->log2arena.as<float>(), R2, dm->h1, dm->x,
+                                     dm->m, &dm->err, ctx->gscratch.as<uint8_t>(), stride, cap, nb, st));
+    }
+    uint32_t e1 = 0;
+    CK(cudaMemcpyAsync(&e1, &dm->err, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    done = e1 == 0;
+    if (!done) CK(cudaMemsetAsync(&dm->err, 0, 4, st));
+    return ASZ_OK;
+}
 
 // first_max: a zero maximum takes the sign of the first largest element (std::max_element)
 // instead of the last one (std::minmax_element).
@@ -1000,8 +1033,8 @@ int default_slope_on(asz_ctx *ctx, const float *field, const uint64_t fdims[3], 
     CK(cudaMemcpyAsync(dm->evals, evals, sizeof(ProxyEval) * ne, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
     const float R = mx - mn;
-    // The shared-memory exact kernel when the maps fit; the serial kernel otherwise, or when a
-    // key exceeds int32 (the exact kernel then reports error bit 2).
+    // The shared-memory exact kernel when the maps fit, else the same kernel with global scratch;
+    // the serial kernel when a key exceeds int32 (the exact kernels then report error bit 2).
     bool serial = cap > exact_cap();
     if (!serial) {
         {
@@ -1016,6 +1049,12 @@ int default_slope_on(asz_ctx *ctx, const float *field, const uint64_t fdims[3], 
             serial = true;
             CK(cudaMemsetAsync(&dm->err, 0, 4, ctx->stream));
         }
+    }
+    if (serial) {
+        bool done = false;
+        rc = abmap_exact_global(ctx, ne, d_in, dims[1] * dims[2], dims[2], R * R, cap, 3, "slope_global", done);
+        if (rc) return rc;
+        serial = !done;
     }
     if (serial) {
         ProfScope ps_slope(ctx, "slope_serial", 0);
@@ -1207,6 +1246,13 @@ int plan_search(asz_ctx *ctx, const float *d_in, const uint64_t dims[3], const a
                         serial = true;
                         CK(cudaMemsetAsync(&dm->err, 0, 4, st));
                     }
+                }
+                if (serial) {
+                    bool done = false;
+                    int rc2 = abmap_exact_global(ctx, ne, d_in, dims[1] * dims[2], dims[2], R * R, cap, nb,
+                                                 "plan_abmap_global", done);
+                    if (rc2) return rc2;
+                    serial = !done;
                 }
                 if (serial) {
                     uint32_t bcap, tcap;
@@ -1543,6 +1589,15 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
     CK(ctx->scratch.reserve(slots * sstride));
     CK(ctx->tlist.reserve(G.nblocks * sizeof(uint32_t)));
     CK(ctx->spill.reserve(G.nblocks * sizeof(uint32_t)));
+    // Global scratch of the exact replay for groups above the shared-memory capacity: a slice per
+    // CTA, at most 148 CTAs and 512 MiB.
+    const u64 gstride = exact_global_stride(capmax);
+    unsigned ggrid = 0;
+    if (capmax > exact_cap()) {
+        ggrid = (unsigned)std::max<u64>(1, std::min<u64>(148, (512ull << 20) / gstride));
+        CK(ctx->gscratch.reserve(ggrid * gstride));
+        CK(ctx->spill2.reserve(G.nblocks * sizeof(uint32_t)));
+    }
     if (ctx->tsel_mode == 1) {
         std::vector<uint32_t> iota(G.nblocks);
         for (u64 i = 0; i < G.nblocks; i++) iota[i] = (uint32_t)i;
@@ -1807,13 +1862,27 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
                                      ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10,
                                      d_list, d_lcount, d_spill, d_scount, exact_cap(), 148, st));
             }
+            // Groups larger than shared memory holds: the same replay with global scratch, a CTA
+            // per group; only what that cannot take (keys outside int32) reaches the serial kernel.
+            uint32_t *d_left = d_spill, *d_lcnt = d_scount;
+            if (G.cap[l] > exact_cap()) {
+                d_left = ctx->spill2.as<uint32_t>();
+                d_lcnt = &dm->spill2_count[l % 64];
+                CK(cudaMemsetAsync(d_lcnt, 0, 4, st));
+                ProfScope ps(ctx, "tsel_exact_global", 0);
+                CK(launch_tsel_exact_global(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default,
+                                            d_tval, d_tint, &dm->fb, ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap,
+                                            &dm->amb_count, ctx->overrides.as<uint32_t>(), nov,
+                                            ctx->proxies.as<float>() + G.nblocks * l * 10, d_spill, d_scount, d_left, d_lcnt,
+                                            ctx->gscratch.as<uint8_t>(), gstride, G.cap[l], ggrid, st));
+            }
             {
                 ProfScope ps(ctx, "tsel_serial", 0);
                 CK(launch_tsel_v0(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default,
                                   ctx->scratch.as<uint8_t>(), sstride, capmax, bcap, tcap, d_tval, d_tint, &dm->fb,
                                   ctx->amb.as<AmbiguousRecord>(), (uint32_t)amb_cap, &dm->amb_count,
-                                  ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10, d_spill,
-                                  d_scount, slots, &dm->err, st));
+                                  ctx->overrides.as<uint32_t>(), nov, ctx->proxies.as<float>() + G.nblocks * l * 10, d_left,
+                                  d_lcnt, slots, &dm->err, st));
             }
             ProfScope ps(ctx, "round_compress", rg.targets * 12);
             CK(launch_round_compress(G.fg, rg, d_ent, d_tval, d_in, d_rec, d_qb + qb_off[l + 1],
@@ -1827,6 +1896,8 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
         CK(cudaMemcpyAsync(words, &dm->err, sizeof(words), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(lcounts, dm->list_count, sizeof(lcounts), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(scounts, dm->spill_count, sizeof(scounts), cudaMemcpyDeviceToHost, st));
+        uint32_t s2counts[64];
+        CK(cudaMemcpyAsync(s2counts, dm->spill2_count, sizeof(s2counts), cudaMemcpyDeviceToHost, st));
         uint32_t why[3];
         CK(cudaMemcpyAsync(why, dm->why, sizeof(why), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1837,7 +1908,7 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
         R.serial_groups = 0;
         for (u64 l = 0; l < L && l < 64; l++) {
             if (tsel_mode == 0) R.exact_groups += lcounts[l];
-            R.serial_groups += scounts[l];
+            R.serial_groups += !line_bytes && G.cap[l] > exact_cap() ? s2counts[l] : scounts[l];
         }
         if (line_bytes) {
             R.exact_groups = lines_exact;

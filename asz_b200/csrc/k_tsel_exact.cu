@@ -586,8 +586,81 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-// Shared-memory bytes the exact kernels need for groups of up to `cap` samples.
+// The same exact replay for groups larger than shared memory holds: each CTA works in its own
+// slice of a global scratch arena (stride bytes, L2-resident) instead of shared memory, so a group
+// of up to `cap` samples is still replayed by a whole CTA rather than by one thread. Groups it
+// cannot take (more samples than cap, keys outside int32) go to `spill` for the serial kernel.
+__global__ void __launch_bounds__(kThreads)
+    tsel_exact_global_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
+                             const float *__restrict__ rec, const float *__restrict__ orig,
+                             const float *__restrict__ log2arena, float R2, float t_default, float *__restrict__ tval,
+                             int64_t *__restrict__ t_int, uint32_t *__restrict__ fb_count, AmbiguousRecord *amb,
+                             uint32_t amb_cap, uint32_t *amb_count, const uint32_t *__restrict__ overrides,
+                             uint32_t n_overrides, float *__restrict__ proxies, const uint32_t *__restrict__ list,
+                             const uint32_t *__restrict__ list_count, uint32_t *spill, uint32_t *spill_count,
+                             uint8_t *scratch, uint64_t stride, uint32_t cap) {
+    uint8_t *mine = scratch + blockIdx.x * stride;
+    const uint32_t items = *list_count;
+    __shared__ float h1v[kMaxEvals], xv[kMaxEvals];
+    __shared__ uint32_t m_sh;
+    const ListSpill sp{spill, spill_count};
+    for (uint32_t it = blockIdx.x; it < items; it += gridDim.x)
+        exact_one(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int, fb_count, amb, amb_cap, amb_count,
+                  overrides, n_overrides, proxies, list[it], mine, cap, h1v, xv, m_sh, sp);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    slope_exact_global_kernel(const SampleBox *__restrict__ boxes, const ProxyEval *__restrict__ evals, uint32_t n_evals,
+                              const float *__restrict__ orig, uint64_t n1n2, uint64_t n2,
+                              const float *__restrict__ log2arena, float R2, float *__restrict__ h1_out,
+                              float *__restrict__ x_out, uint32_t *__restrict__ m_out, uint32_t *__restrict__ err_word,
+                              uint8_t *scratch, uint64_t stride, uint32_t cap) {
+    __shared__ float h1v[kMaxEvals], xv[kMaxEvals];
+    const uint32_t g = blockIdx.x;
+    ExactGroup eg;
+    eg.box = boxes[g];
+    eg.n = eg.box.n;
+    bool ok = exact_eval(eg, orig, orig, n1n2, n2, evals, (int)n_evals, R2, log2arena + eg.box.log2_off,
+                         scratch + g * stride, cap, h1v, xv, m_out + g);
+    __syncthreads();
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(err_word, 2u);
+        return;
+    }
+    for (uint32_t e = threadIdx.x; e < n_evals; e += blockDim.x) {
+        h1_out[g * n_evals + e] = h1v[e];
+        x_out[g * n_evals + e] = xv[e];
+    }
+}
+
+// Shared-memory bytes the exact kernels need for groups of up to `cap` samples (also the size of
+// a global-scratch slice).
 uint32_t exact_smem_bytes(uint32_t cap) { return Layout(cap).total; }
+
+cudaError_t launch_tsel_exact_global(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes,
+                                     const float *rec, const float *orig, const float *log2arena, float R2, float t_default,
+                                     float *tval, int64_t *t_int, uint32_t *fb_count, AmbiguousRecord *amb, uint32_t amb_cap,
+                                     uint32_t *amb_count, const uint32_t *overrides, uint32_t n_overrides, float *proxies,
+                                     const uint32_t *list, const uint32_t *list_count, uint32_t *spill, uint32_t *spill_count,
+                                     uint8_t *scratch, uint64_t stride, uint32_t cap, unsigned grid, cudaStream_t st) {
+    if (grid == 0) return cudaSuccess;
+    tsel_exact_global_kernel<<<grid, kThreads, 0, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int,
+                                                        fb_count, amb, amb_cap, amb_count, overrides, n_overrides, proxies,
+                                                        list, list_count, spill, spill_count, scratch, stride, cap);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slope_exact_global(const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals, const float *orig,
+                                      uint64_t n1n2, uint64_t n2, const float *log2arena, float R2, float *h1, float *x,
+                                      uint32_t *m_out, uint32_t *err, uint8_t *scratch, uint64_t stride, uint32_t cap,
+                                      uint32_t nboxes, cudaStream_t st) {
+    if (nboxes == 0) return cudaSuccess;
+    slope_exact_global_kernel<<<nboxes, kThreads, 0, st>>>(boxes, evals, n_evals, orig, n1n2, n2, log2arena, R2, h1, x, m_out,
+                                                           err, scratch, stride, cap);
+    count_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
                               const float *orig, const float *log2arena, float R2, float t_default, float *tval,

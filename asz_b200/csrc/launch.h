@@ -141,6 +141,18 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
                               uint32_t *amb_count, const uint32_t *overrides, uint32_t n_overrides, float *proxies,
                               const uint32_t *list, const uint32_t *list_count, uint32_t *spill, uint32_t *spill_count,
                               uint32_t cap, unsigned grid, cudaStream_t st);
+// The exact replay with each CTA's working set in a slice of `scratch` (stride bytes, at least
+// exact_smem_bytes(cap)) instead of shared memory, for groups of up to cap samples.
+cudaError_t launch_tsel_exact_global(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes,
+                                     const float *rec, const float *orig, const float *log2arena, float R2, float t_default,
+                                     float *tval, int64_t *t_int, uint32_t *fb_count, AmbiguousRecord *amb, uint32_t amb_cap,
+                                     uint32_t *amb_count, const uint32_t *overrides, uint32_t n_overrides, float *proxies,
+                                     const uint32_t *list, const uint32_t *list_count, uint32_t *spill, uint32_t *spill_count,
+                                     uint8_t *scratch, uint64_t stride, uint32_t cap, unsigned grid, cudaStream_t st);
+cudaError_t launch_slope_exact_global(const SampleBox *boxes, const ProxyEval *evals, uint32_t n_evals, const float *orig,
+                                      uint64_t n1n2, uint64_t n2, const float *log2arena, float R2, float *h1, float *x,
+                                      uint32_t *m_out, uint32_t *err, uint8_t *scratch, uint64_t stride, uint32_t cap,
+                                      uint32_t nboxes, cudaStream_t st);
 cudaError_t launch_copy_box(const float *in, const uint64_t n[3], const uint64_t lo[3], const uint64_t m[3], float *out,
                             cudaStream_t st);
 // out[k] = in[idx[k]] for k < n.

@@ -94,7 +94,7 @@ typedef struct asz_report {
     uint64_t ambiguous_decisions; /* per-block t decisions re-checked on the host */
     uint64_t reruns;              /* compressions repeated after a host re-check */
     uint64_t exact_groups;        /* (block, round) groups the certified fast path handed to the exact path */
-    uint64_t serial_groups;       /* groups too large for the shared-memory exact kernel (serial kernel) */
+    uint64_t serial_groups;       /* groups the exact kernels could not take (serial kernel) */
     uint64_t exact_window;        /* of exact_groups: errors spread wider than the fast path's histogram */
     uint64_t exact_undecided;     /* of exact_groups: a comparison the fast path's bounds could not settle */
     uint64_t wide_groups;         /* groups the fast path settled by counting their bins window by window */

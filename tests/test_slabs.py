@@ -167,3 +167,47 @@ def test_slab_compression_equals_whole_field(case_index):
     assert int(rep[0]) == len(slab)
     assert rep[2] == rep[3], "default slope differs from the whole field's"
     assert slab == whole, ".asz of the slabs differs from the whole-field compression"
+
+
+def _fullsize_worker(rank, world, port, outdir):
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import datetime
+    import hashlib
+
+    import torch.distributed as dist
+
+    import make_fullsize
+    from asz_b200 import api, slabs
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
+    x = make_fullsize.make_field("c2")
+    plan = ",".join(["cubic2_012"] * 9)
+    p = api.default_params(block_pivot_ratio=3)
+    b0, b1 = slabs.split_blocks(slabs.blocks_of(x.shape, plan, p), world)[rank]
+    pb, pc, _ = slabs.slab_planes(x.shape, plan, b0, b1, p)
+    with api.Context(0) as ctx:
+        blob, _ = slabs.compress_slab(ctx, slabs.TorchComm(dist), x[pb:pb + pc], x.shape, b0, b1, 1e-3, plan, "cubic",
+                                      api.default_params(block_pivot_ratio=3))
+    if rank == 0:
+        with open(os.path.join(outdir, "digest.txt"), "w") as f:
+            f.write(hashlib.sha256(x.tobytes()).hexdigest() + " " + hashlib.sha256(blob).hexdigest() + "\n")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_slabs_at_full_size_match_the_reference_record():
+    """The 512^3 C2 field at REL 1e-3 (cubic2_012 x9, block pivot ratio 3) over 2 ranks: rank 0's
+    .asz has the digest the reference binaries' output has (tests/golden/fullsize.json)."""
+    import json
+    fix = json.load(open(os.path.join(ROOT, "tests", "golden", "fullsize.json")))
+    case = next(c for c in fix["cases"] if c["name"] == "c2_cubic_0.001")
+    port = _free_port()
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_fullsize_worker, args=(2, port, d), nprocs=2, join=True, start_method="spawn")
+        field_sha, asz_sha = open(os.path.join(d, "digest.txt")).read().split()
+    if field_sha != fix["fields"]["c2"]["sha256"]:
+        pytest.skip("generated input differs from the recorded one (other NumPy build)")
+    assert asz_sha == case["asz_sha256"]
