@@ -1667,7 +1667,7 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
     o.pre.assign(L + 1, PreCode{});
     if (prebuild) {
         CK(ctx->hwin.reserve(L * kHistWin * 8));
-        CK(ctx->hwin_host.reserve(L * kHistWin * 8 + L * 8 + L * 4));
+        CK(ctx->hwin_host.reserve(L * kHistWin * 8 + L * 8 + L * 4 + 8 + G.pivots * 4));
         d_hwin = ctx->hwin.as<unsigned long long>();
         h_hist = (u64 *)ctx->hwin_host.p;
         h_rng = (int32_t *)(h_hist + L * kHistWin);
@@ -1721,6 +1721,49 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
         });
         return ASZ_OK;
     };
+    // The pivot stream's code, from a host copy of its QBs taken behind the pivot kernel (its
+    // range is known only then, and it is small: one value per pivot).
+    auto schedule_pivot_code = [&]() -> int {
+        if (!prebuild || G.pivots == 0) return ASZ_OK;
+        int32_t *h_prng = (int32_t *)(h_over + L);
+        int32_t *h_piv = h_prng + 2;
+        if (ctx->round_ev.size() < 2 * L + 2) {
+            for (int k = 0; k < 2; k++) {
+                cudaEvent_t e;
+                CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                ctx->round_ev.push_back(e);
+            }
+        }
+        cudaEvent_t ev_r = ctx->round_ev[2 * L], ev_c = ctx->round_ev[2 * L + 1];
+        CK(cudaEventRecord(ev_r, st));
+        CK(cudaStreamWaitEvent(ctx->side, ev_r, 0));
+        CK(cudaMemcpyAsync(h_piv, d_qb + qb_off[0], G.pivots * 4, cudaMemcpyDeviceToHost, ctx->side));
+        CK(cudaMemcpyAsync(h_prng, &dm->qb_range[0], 8, cudaMemcpyDeviceToHost, ctx->side));
+        CK(cudaEventRecord(ev_c, ctx->side));
+        const u64 count = G.pivots;
+        PreCode *pc = &o.pre[0];
+        const int dev = ctx->device;
+        ctx->builder->submit([=]() {
+            cudaSetDevice(dev);
+            if (cudaEventSynchronize(ev_c) != cudaSuccess) return;
+            const int32_t lo = h_prng[0], hi = h_prng[1];
+            if (lo > hi || (u64)((int64_t)hi - lo) >= (1ull << 24)) return;
+            std::vector<u64> h((u64)((int64_t)hi - lo) + 1, 0);
+            for (u64 i = 0; i < count; i++) {
+                const int64_t v = (int64_t)h_piv[i] - lo;
+                if (v < 0 || v >= (int64_t)h.size()) return;
+                h[(u64)v]++;
+            }
+            std::string err;
+            HuffCode code;
+            if (!build_code(h, lo, hi, count, false, code, err)) return;
+            pc->code = std::move(code);
+            pc->lo = lo;
+            pc->hi = hi;
+            pc->ok = true;
+        });
+        return ASZ_OK;
+    };
     hs_prep.reset();
     std::optional<HostScope> hs_rounds(std::in_place, ctx, "host:rounds");
     while (true) {
@@ -1745,6 +1788,8 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
             ProfScope ps(ctx, "pivot_compress", G.pivots * 12);
             CK(launch_pivot_compress(G.pg, d_in, d_rec, d_qb + qb_off[0], &dm->qb_range[0], st));
         }
+        rc = schedule_pivot_code();
+        if (rc) return rc;
         if (line_bytes) {
             // Fused pass over all columns. Blocks the certified fast path cannot settle stop their
             // column at that round; the exact path then settles them round by round, and their

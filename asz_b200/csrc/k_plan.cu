@@ -82,8 +82,19 @@ __global__ void plan_sample_kernel(const float *__restrict__ d, uint64_t n1, uin
     }
 }
 
-// mse = fmaf(e, e, mse) over each candidate's samples in loop order (one warp per candidate): the
-// warp stages 32 values per step with a coalesced load and lane 0 runs the dependent chain.
+// mse = fmaf(e, e, mse) over each candidate's samples in loop order (one warp per candidate), the
+// reference's float sum (generate_config.tpp:227-254), bit for bit.
+//
+// Batches of kBatch terms, kPer consecutive ones per lane. While the running sum s stays in one
+// binade [2^E, 2^(E+1)), with ulp u = 2^(E-23) and s = m*u (m in [2^23, 2^24)), every step
+// s' = RN(s + x*x) equals (m + r)*u with r = x*x/u rounded to the nearest integer, unless the
+// fraction of x*x/u is exactly one half (round-half-even then depends on m). The terms are not
+// negative, so the partial sums grow: if the batch's total stays below 2^24 no step leaves the
+// binade, and the batch adds sum(r)*u in one step. x*x is exact in double and u a power of two,
+// so r and the tie test are exact. A batch with a tie, a crossing, or a sum below the normal range
+// is replayed term by term (the exact chain).
+constexpr uint32_t kPer = 8, kBatch = 32 * kPer;
+
 __global__ void plan_mse_kernel(const PlanCand *__restrict__ cands, uint32_t ncands, const float *__restrict__ e,
                                 float *__restrict__ mse_out) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -92,11 +103,41 @@ __global__ void plan_mse_kernel(const PlanCand *__restrict__ cands, uint32_t nca
     const uint64_t n = c.cnt[0] * c.cnt[1] * c.cnt[2];
     const float *p = e + c.off;
     float mse = 0.0f;
-    for (uint64_t b = 0; b < n; b += 32) {
-        const float v = b + lane < n ? p[b + lane] : 0.0f;
-        const uint32_t m = n - b < 32 ? (uint32_t)(n - b) : 32u;
-        for (uint32_t j = 0; j < m; j++) {
-            const float x = __shfl_sync(0xffffffffu, v, j);
+    for (uint64_t b = 0; b < n; b += kBatch) {
+        float v[kPer];
+#pragma unroll
+        for (uint32_t i = 0; i < kPer; i++) {
+            const uint64_t k = b + lane * kPer + i;
+            v[i] = k < n ? p[k] : 0.0f;
+        }
+        if (mse >= 0x1p-100f) {
+            int ex;
+            frexpf(mse, &ex);  // mse = f * 2^ex, f in [0.5, 1): binade 2^(ex-1), ulp 2^(ex-24)
+            const double inv_u = ldexp(1.0, 24 - ex);
+            const uint32_t m = (uint32_t)__double2uint_rz((double)mse * inv_u);
+            bool ok = true;
+            uint32_t sum = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < kPer; i++) {
+                const double t = __dmul_rn(__dmul_rn((double)v[i], (double)v[i]), inv_u);
+                const double r = rint(t);
+                ok = ok && r < 0x1p24 && fabs(t - r) != 0.5;
+                sum += ok ? (uint32_t)r : 0u;
+            }
+            ok = __all_sync(0xffffffffu, ok);
+            const uint32_t tot = __reduce_add_sync(0xffffffffu, sum);
+            if (ok && (uint64_t)m + tot < (1ull << 24)) {
+                mse = ldexpf((float)(m + tot), ex - 24);
+                continue;
+            }
+        }
+        const uint32_t cnt = n - b < kBatch ? (uint32_t)(n - b) : kBatch;
+        for (uint32_t j = 0; j < cnt; j++) {
+            const uint32_t i = j % kPer;
+            float vi = v[0];
+#pragma unroll
+            for (uint32_t q = 1; q < kPer; q++) vi = i == q ? v[q] : vi;
+            const float x = __shfl_sync(0xffffffffu, vi, j / kPer);
             mse = __fmaf_rn(x, x, mse);
         }
     }
