@@ -7,6 +7,8 @@
 // an earlier round or a pivot.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "dev_common.cuh"
 #include "geometry.cuh"
 #include "launch.h"
@@ -341,6 +343,116 @@ __global__ void __launch_bounds__(256, 3)
     }
 }
 
+// The finest round along axis 2 (dir == 2, hs == 1): a warp per target line. The warp copies the
+// whole line of the reconstruction and of the input (n2 floats each) into shared memory with
+// 16-byte loads, then predicts its targets from there. The targets (odd points) and their stencil
+// points (even points) cover the line, so the copy fetches no DRAM sector that per-target loads
+// would not, with a quarter as many load instructions and no scattered ones. At hs >= 2 the
+// per-target kernel measured as fast or faster (a line then holds fewer targets per staged byte),
+// and so did a two-stage form with asynchronous copies and a form with two targets per lane step.
+// Results are those of round_compress_kernel<false>: same entries, stencils, arithmetic and QB
+// indices. A line's own targets are written to global memory only; the staged copy is read-only,
+// and no target of the round reads a position that the round writes.
+__device__ __forceinline__ void stencil_reach(uint32_t sc, uint32_t &neg, uint32_t &pos) {
+    // Multiples of hs that the case reads below and above the target (predict_case).
+    switch (sc) {
+    case kStencilQuintic: neg = 5; pos = 5; break;
+    case kStencilLeft1: neg = 1; pos = 0; break;
+    case kStencilLeft2: neg = 1; pos = 1; break;
+    case kStencilLeft3: neg = 1; pos = 3; break;
+    case kStencilRight1: neg = 3; pos = 0; break;
+    case kStencilRight2: neg = 3; pos = 1; break;
+    default: neg = 3; pos = 3; break;
+    }
+}
+
+__global__ void __launch_bounds__(256, 3)
+    round_compress_line_kernel(FieldGeom fg, RoundGeom rg, const AxisEntry *__restrict__ ent, const float *__restrict__ tval,
+                               const float *__restrict__ in, float *__restrict__ rec, int32_t *__restrict__ qb,
+                               int32_t *qb_range, uint32_t *err_word, unsigned long long *__restrict__ hist,
+                               uint32_t *hist_over) {
+    extern __shared__ __align__(16) float line_smem[];
+    const uint32_t n2 = (uint32_t)fg.n[2], n4 = n2 / 4;
+    const uint32_t warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t *hsh = hist ? reinterpret_cast<uint32_t *>(line_smem + (size_t)warps * 2 * n2) : nullptr;
+    float *s_rec = line_smem + (size_t)warp * 2 * n2, *s_in = s_rec + n2;
+    if (hsh) {
+        for (uint32_t i = threadIdx.x; i < kHistWin; i += blockDim.x) hsh[i] = 0;
+        __syncthreads();
+    }
+    bool hover = false;
+    // Axis 2 divides (diff*0.5)/eb, as round_compress_kernel does off axis 0.
+    const double ebd = (double)rg.eb, eb2 = __dadd_rn(ebd, ebd), rinv = __ddiv_rn(1.0, ebd);
+    const AxisEntry *e0t = ent + rg.ent_off[0], *e1t = ent + rg.ent_off[1], *e2t = ent + rg.ent_off[2];
+    const uint32_t T1 = (uint32_t)rg.tcount[1], T2 = (uint32_t)rg.tcount[2];
+    const uint32_t lines = (uint32_t)rg.tcount[0] * T1;
+    const uint64_t n1n2 = fg.n[1] * fg.n[2];
+    const uint32_t nb1 = (uint32_t)fg.block_num[1], nb2 = (uint32_t)fg.block_num[2];
+    const uint32_t hs = (uint32_t)rg.hs;
+    int32_t lo = INT32_MAX, hi = INT32_MIN;
+    for (uint32_t line = blockIdx.x * warps + warp; line < lines; line += gridDim.x * warps) {
+        const uint32_t k0 = line / T1, k1 = line - k0 * T1;
+        const AxisEntry e0 = load_entry(e0t + k0), e1 = load_entry(e1t + k1);
+        const uint64_t line_pos = (uint64_t)e0.ii * n1n2 + (uint64_t)e1.ii * n2;
+        const uint32_t blk = e0.bb * nb1 + e1.bb;
+        const LineQB lq = line_qb(rg, e0, e1);
+        // Stage the line: four 16-byte loads per lane in flight before their stores.
+        const float4 *g_rec4 = reinterpret_cast<const float4 *>(rec + line_pos);
+        const float4 *g_in4 = reinterpret_cast<const float4 *>(in + line_pos);
+        float4 *s_rec4 = reinterpret_cast<float4 *>(s_rec), *s_in4 = reinterpret_cast<float4 *>(s_in);
+        for (uint32_t b = lane; b < n4; b += 64) {
+            float4 a[2], c[2];
+#pragma unroll
+            for (uint32_t j = 0; j < 2; j++)
+                if (b + 32 * j < n4) {
+                    a[j] = g_rec4[b + 32 * j];
+                    c[j] = __ldg(g_in4 + b + 32 * j);
+                }
+#pragma unroll
+            for (uint32_t j = 0; j < 2; j++)
+                if (b + 32 * j < n4) {
+                    s_rec4[b + 32 * j] = a[j];
+                    s_in4[b + 32 * j] = c[j];
+                }
+        }
+        __syncwarp();
+        for (uint32_t k2 = lane; k2 < T2; k2 += 32) {
+            const AxisEntry e2 = load_entry(e2t + k2);
+            const uint64_t qi = target_qb(rg, lq, e0, e1, e2);
+            const uint32_t sc = e2.stencil, ii = e2.ii;
+            uint32_t rn, rp;
+            stencil_reach(sc, rn, rp);
+            if (qi >= rg.qb_total || ii < rn * hs || ii + rp * hs >= n2) {
+                atomicOr(err_word, 4u);
+                continue;
+            }
+            const float t = sc == kStencilCubic ? __ldg(tval + (uint64_t)blk * nb2 + e2.bb) : 0.0f;
+            const float pred = predict_case(s_rec, ii, hs, sc, t);
+            const double pd = (double)pred;
+            const double diff = __dsub_rn(pd, (double)s_in[ii]);
+            const double q = quot_for_lround(__dmul_rn(diff, 0.5), ebd, rinv);
+            const int32_t v = (int32_t)lround_d(q);
+            qb[qi] = v;
+            rec[line_pos + ii] = __double2float_rn(__fma_rn(-(double)v, eb2, pd));
+            lo = min(lo, v);
+            hi = max(hi, v);
+            if (hsh) {
+                const uint32_t bin = (uint32_t)(v + kHistHalf);
+                if (bin < kHistWin) atomicAdd(&hsh[bin], 1u);
+                else hover = true;
+            }
+        }
+        __syncwarp();
+    }
+    reduce_range(lo, hi, qb_range);
+    if (hsh) {
+        if (hover) atomicOr(hist_over, 1u);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kHistWin; i += blockDim.x)
+            if (hsh[i]) atomicAdd(&hist[i], (unsigned long long)hsh[i]);
+    }
+}
+
 // Batched form: one work queue over the (field, item) pairs of a round, an item being
 // kBatchChunks CTA-sized chunks of one field's target lines (256 >> tpl_log2 lines each).
 constexpr uint32_t kBatchChunks = 8;
@@ -551,10 +663,44 @@ static unsigned round_grid(const RoundGeom &rg, uint32_t tpl_log2) {
     return grid_for(lines, (unsigned)(2 * per_cta), 148 * 32);
 }
 
+// round_compress_line_kernel takes the finest round along axis 2 when it can stage the lines with
+// 16-byte loads: n2 a multiple of 4 (so every line starts on a 16-byte boundary) and both arrays
+// 16-byte aligned; n2 <= 4096 bounds the staging buffers (32 KB a warp).
+static bool line_kernel_fits(const FieldGeom &fg, const RoundGeom &rg, const float *in, const float *rec) {
+    return rg.dir == 2 && rg.hs == 1 && fg.n[2] % 4 == 0 && fg.n[2] <= 4096 && (uintptr_t)in % 16 == 0 &&
+           (uintptr_t)rec % 16 == 0 && rg.tcount[0] * rg.tcount[1] < (1ull << 32);
+}
+
+static cudaError_t launch_round_compress_lines(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent,
+                                               const float *tval, const float *in, float *rec, int32_t *qb, int32_t *qb_range,
+                                               uint32_t *err, cudaStream_t st, unsigned long long *hist, uint32_t *hist_over) {
+    constexpr size_t kStageBudget = 96 * 1024;  // staging buffers of one CTA
+    const size_t per_warp = 8 * fg.n[2];
+    const unsigned warps = (unsigned)std::max<size_t>(1, std::min<size_t>(8, kStageBudget / per_warp));
+    const size_t smem = warps * per_warp + (hist ? kHistWin * sizeof(uint32_t) : 0);
+    cudaError_t e;
+    if (smem > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(round_compress_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+        return e;
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, round_compress_line_kernel, (int)(32 * warps), smem)) !=
+        cudaSuccess)
+        return e;
+    const uint64_t lines = rg.tcount[0] * rg.tcount[1];
+    const uint64_t ctas = std::min<uint64_t>((lines + warps - 1) / warps, 148ull * (uint64_t)std::max(occ, 1));
+    round_compress_line_kernel<<<(unsigned)ctas, 32 * warps, smem, st>>>(fg, rg, ent, tval, in, rec, qb, qb_range, err, hist,
+                                                                         hist_over);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
                                   const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, int div_all,
                                   float *pred_out, cudaStream_t st, unsigned long long *hist, uint32_t *hist_over) {
     if (rg.targets == 0) return cudaSuccess;
+    if (!div_all && line_kernel_fits(fg, rg, in, rec))
+        return launch_round_compress_lines(fg, rg, ent, tval, in, rec, qb, qb_range, err, st, hist, hist_over);
     const uint32_t lg = round_lines_log2(rg.tcount[2]);
     const size_t smem = hist ? kHistWin * sizeof(uint32_t) : 0;
     if (div_all)

@@ -206,6 +206,37 @@ def test_device_resident_input(gpu_ctx):
     assert np.array_equal(y.cpu().numpy().view(np.uint32), out.view(np.uint32))
 
 
+def test_device_input_not_16_byte_aligned(gpu_ctx):
+    """The finest round along axis 2 stages whole lines with 16-byte loads when the input allows; a
+    device input 4 bytes past a 16-byte boundary takes the per-target kernel. Both match the oracle."""
+    import torch
+
+    import asz_b200.api as api
+    from asz_b200 import fields
+    f = fields.c2_field(seed=9, shape=(24, 32, 64))
+    plan = ",".join(["cubic2_012"] * 5)
+    o = O.compress(f, 1e-3, plan, False, O.default_params(block_pivot_ratio=3))
+    aligned = torch.from_numpy(f).cuda()
+    flat = torch.empty(f.size + 1, dtype=torch.float32, device="cuda")
+    flat[1:].copy_(aligned.view(-1))
+    shifted = flat[1:].view(f.shape)
+    assert aligned.data_ptr() % 16 == 0 and shifted.data_ptr() % 16 == 4
+    for x in (aligned, shifted):
+        blob, _ = gpu_ctx.compress(x, 1e-3, plan, "cubic", api.default_params(block_pivot_ratio=3))
+        assert blob == o.asz
+        assert np.array_equal(gpu_ctx.debug_recon().view(np.uint32), o.recon.ravel().view(np.uint32))
+
+
+@pytest.mark.parametrize("shape", [(9, 7, 1024), (7, 7, 4096)], ids=["n2_1024", "n2_4096"])
+@pytest.mark.parametrize("family", ["cubic", "quintic"])
+def test_long_lines_against_oracle(gpu_ctx, shape, family):
+    """Lines of 1024 and 4096 points: the finest round's line-staging kernel with more than 48 KB of
+    shared memory per CTA (eight and three warps)."""
+    from asz_b200 import fields
+    f = fields.c2_field(seed=11, shape=shape)
+    _check_against_oracle(gpu_ctx, f, 1e-3, ",".join(["cubic2_012"] * 4), family, 3)
+
+
 @pytest.mark.parametrize("case", golden_cases()[:3], ids=lambda c: c["name"])
 def test_cli_drop_in(case):
     data, blob, out = load_golden(case)
