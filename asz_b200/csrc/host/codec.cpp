@@ -1876,26 +1876,33 @@ int run_core(asz_ctx *ctx, const CoreArgs &a, CoreOut &o, asz_report &R) {
             uint32_t *d_spill = ctx->spill.as<uint32_t>(), *d_scount = &dm->spill_count[l % 64];
             CK(cudaMemsetAsync(d_scount, 0, 4, st));
             if (tsel_mode == 0) {
-                // Algorithmic bytes: one read of the 5 operands (4 neighbours + original) per sample.
-                u64 sample_bytes = 0;
-                if (ctx->prof) {
-                    u64 per_axis[3][3];
-                    for (int a = 0; a < 3; a++) {
-                        const u64 nb = G.fg.block_num[a];
-                        per_axis[a][0] = 1;
-                        per_axis[a][1] = nb > 2 ? nb - 2 : 0;
-                        per_axis[a][2] = nb >= 2 ? 1 : 0;
-                    }
-                    for (int c = 0; c < 27; c++) {
-                        const ClassInfo &ci = G.classes[l][c];
-                        if (ci.fallback || !ci.n) continue;
-                        sample_bytes += per_axis[0][c / 9] * per_axis[1][(c / 3) % 3] * per_axis[2][c % 3] * ci.n * 20;
+                // Blocks per class (first, middle, last along each axis), for the algorithmic bytes
+                // (one read of the 5 operands, 4 neighbours + original, per sample) and the group
+                // size of the most populous class, which picks the kernel's CTA width.
+                u64 per_axis[3][3];
+                for (int a = 0; a < 3; a++) {
+                    const u64 nb = G.fg.block_num[a];
+                    per_axis[a][0] = 1;
+                    per_axis[a][1] = nb > 2 ? nb - 2 : 0;
+                    per_axis[a][2] = nb >= 2 ? 1 : 0;
+                }
+                u64 sample_bytes = 0, most = 0;
+                uint32_t common_samples = 0;
+                for (int c = 0; c < 27; c++) {
+                    const ClassInfo &ci = G.classes[l][c];
+                    if (ci.fallback || !ci.n) continue;
+                    const u64 blocks = per_axis[0][c / 9] * per_axis[1][(c / 3) % 3] * per_axis[2][c % 3];
+                    sample_bytes += blocks * ci.n * 20;
+                    if (blocks > most || (blocks == most && ci.n > common_samples)) {
+                        most = blocks;
+                        common_samples = ci.n;
                     }
                 }
                 ProfScope ps(ctx, "tsel_fast", sample_bytes);
                 CK(cudaMemsetAsync(d_lcount, 0, 4, st));
                 CK(launch_tsel_fast(G.fg, rg, (uint32_t)l, cls, d_rec, d_in, ctx->log2arena.as<float>(), R2, t_default, d_tval,
-                                    d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, dm->why, st));
+                                    d_tint, &dm->fb, d_list, d_lcount, ctx->overrides.as<uint32_t>(), nov, dm->why, st,
+                                    common_samples));
             } else {
                 d_list = ctx->iota.as<uint32_t>();
                 d_lcount = &dm->all_count;

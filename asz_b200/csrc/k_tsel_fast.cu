@@ -3,6 +3,8 @@
 // The sample positions follow get_AB_map's loops (get_AB_map.tpp:13-15).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "tsel_fast.cuh"
 
 namespace asz {
@@ -96,7 +98,7 @@ struct ListHandOff {
 // path could not settle; why[0] counts those whose bins span too many windows, why[1] those with an
 // undecidable comparison; why[2] counts the groups settled here by window-by-window counting.
 template <int kT>
-__global__ void __launch_bounds__(kT, kT == 64 ? 16 : 8)
+__global__ void __launch_bounds__(kT, kT == 32 ? 20 : kT == 64 ? 16 : 8)
     tsel_fast_kernel(FieldGeom fg, RoundGeom rg, uint32_t l, const ClassInfo *__restrict__ classes,
                      const float *__restrict__ rec, const float *__restrict__ orig, const float *__restrict__ log2arena,
                      float R2, float t_default, float *__restrict__ tval, int64_t *__restrict__ t_int,
@@ -164,24 +166,31 @@ cudaError_t launch_tsel_fast_batch(const BatchField *F, const uint64_t *goff, ui
 cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
                              const float *orig, const float *log2arena, float R2, float t_default, float *tval,
                              int64_t *t_int, uint32_t *fb_count, uint32_t *list_out, uint32_t *list_count,
-                             const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st) {
-    uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
-    uint64_t blocks = nb < 148 * 16 * 4 ? nb : 148 * 16 * 4;
+                             const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st,
+                             uint32_t common_samples) {
+    const uint64_t nb = fg.block_num[0] * fg.block_num[1] * fg.block_num[2];
     const int smem = (int)sizeof(GroupShared);
-    // Many groups: 64-thread CTAs, 16 per SM (fewer warps wait at each block barrier). Fewer
-    // groups than four waves of those: 128-thread CTAs, which finish each group sooner.
-    const bool wide = nb < 148 * 16 * 4;
-    cudaError_t e = wide ? cudaFuncSetAttribute(tsel_fast_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                         : cudaFuncSetAttribute(tsel_fast_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // Many groups: 64-thread CTAs, 16 per SM (fewer warps wait at each block barrier), or one-warp
+    // CTAs, 20 per SM, when the most common group size (common_samples) is at most 32 samples
+    // (measured: one-warp CTAs win at 9 samples a group and lose at 45; any size is handled).
+    // Fewer groups than four waves of 64-thread CTAs: 128-thread CTAs, which finish each group sooner.
+    const bool wide = nb < 148 * 16 * 4, narrow = !wide && common_samples <= 32;
+    cudaError_t e = wide     ? cudaFuncSetAttribute(tsel_fast_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                    : narrow ? cudaFuncSetAttribute(tsel_fast_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                             : cudaFuncSetAttribute(tsel_fast_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     if (wide)
-        tsel_fast_kernel<128><<<(unsigned)blocks, 128, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
-                                                                  t_int, fb_count, list_out, list_count, overrides,
-                                                                  n_overrides, why);
+        tsel_fast_kernel<128><<<(unsigned)nb, 128, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
+                                                              t_int, fb_count, list_out, list_count, overrides, n_overrides,
+                                                              why);
+    else if (narrow)
+        tsel_fast_kernel<32><<<(unsigned)std::min<uint64_t>(nb, 148 * 20 * 4), 32, smem, st>>>(
+            fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int, fb_count, list_out, list_count, overrides,
+            n_overrides, why);
     else
-        tsel_fast_kernel<64><<<(unsigned)blocks, 64, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval,
-                                                                t_int, fb_count, list_out, list_count, overrides,
-                                                                n_overrides, why);
+        tsel_fast_kernel<64><<<(unsigned)std::min<uint64_t>(nb, 148 * 16 * 4), 64, smem, st>>>(
+            fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int, fb_count, list_out, list_count, overrides,
+            n_overrides, why);
     count_launch();
     return cudaGetLastError();
 }

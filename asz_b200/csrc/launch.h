@@ -133,7 +133,8 @@ cudaError_t launch_tsel_v0(const FieldGeom &fg, const RoundGeom &rg, uint32_t l,
 cudaError_t launch_tsel_fast(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
                              const float *orig, const float *log2arena, float R2, float t_default, float *tval,
                              int64_t *t_int, uint32_t *fb_count, uint32_t *list_out, uint32_t *list_count,
-                             const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st);
+                             const uint32_t *overrides, uint32_t n_overrides, uint32_t *why, cudaStream_t st,
+                             uint32_t common_samples);
 uint32_t exact_smem_bytes(uint32_t cap);
 cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t l, const ClassInfo *classes, const float *rec,
                               const float *orig, const float *log2arena, float R2, float t_default, float *tval,

@@ -383,6 +383,33 @@ __device__ uint32_t fast_group(GroupShared &sh, const Src &src, uint32_t n, cons
             mq[c] = k;
         }
         if (tid == 0) atomicAdd(&why[2], 1u);
+    } else if (n <= 2 * (uint32_t)kT) {
+        // Every sample is held in registers: each one clears its bin with an atomic AND, and the
+        // one that finds the count still there adds that bin's term. The window ends up zeroed
+        // without a scan of all its bins, which dominates the cost of a small group.
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+            H[c] = 0.0;
+            mq[c] = 0;
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < 2; j++) {
+            if (tid + j * kT >= n) break;
+            const float af = j ? af1 : af0, bf = j ? bf1 : bf0;
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                const float t2 = __fadd_rn(cand[c], cand[c]);
+                const int64_t q = lround_f(__fmul_rn(cand_err(af, bf, t2, rg.stat_eb), neg_eb));
+                const uint64_t bin = (uint64_t)q - (uint64_t)qlo[c];  // < kWin: no sample left the window
+                const uint32_t sh16 = 16u * (uint32_t)(bin & 1);
+                const uint32_t cnt = (atomicAnd(&sh.hist[c][bin >> 1], ~(0xffffu << sh16)) >> sh16) & 0xffffu;
+                if (cnt) {
+                    const float p = __fmul_rn(__ull2float_rn((uint64_t)cnt), r);
+                    H[c] = __fma_rn(-(double)p, (double)l2[cnt], H[c]);
+                    mq[c]++;
+                }
+            }
+        }
     } else {
 #pragma unroll
         for (int c = 0; c < 5; c++) {
