@@ -2379,9 +2379,10 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
     uint32_t *d_pay = ctx->payload.as<uint32_t>();
     CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
     hs_codes.reset();
+    u64 enc_err[2] = {0, 0};  // the encoder's error words, read back with the sync below
     {
-        // Every stream of every field in two sets of launches, one per symbol type (the t streams
-        // are int64, the QB streams int32).
+        // Every stream of every field in two launches, one per symbol type (the t streams are
+        // int64, the QB streams int32).
         std::vector<EncStream> es[2];
         std::vector<u64> toff[2] = {{0}, {0}};
         u64 enc_bytes = 0;
@@ -2433,6 +2434,7 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
             u64 *tbits = (u64 *)(eb + off[k][2]), *tscan = (u64 *)(eb + off[k][3]);
             if (k == 0) CK(launch_encode_tiles<int32_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
             else CK(launch_encode_tiles<int64_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
+            CK(cudaMemcpyAsync(&enc_err[k], tscan, sizeof(u64), cudaMemcpyDeviceToHost, st));
         }
     }
     // Stream assembly (compress.tpp:233-291) in pinned memory: the host writes the headers and
@@ -2451,6 +2453,7 @@ int encode_fields(asz_ctx *ctx, const std::vector<EncodeArgs> &A, std::vector<as
     // The encoding launches finish before the copy timer starts, so that d2h_s holds the copies
     // (and the host's header writing between them) and none of the kernels' time.
     CK(cudaStreamSynchronize(st));
+    if (enc_err[0] | enc_err[1]) return fail(ctx, ASZ_E_DEVICE, "Huffman encoder: a tile's wait for the tiles before it timed out");
     auto t_d2h = clk::now();
     {
         HostScope hs(ctx, "host:assembly");
@@ -4281,6 +4284,7 @@ int slab_encode(asz_ctx *ctx, SlabComm &cm, const CoreOut &co, const Plan &plan,
     CK(cudaMemsetAsync(ctx->payload.p, 0, std::max<u64>(words_total, 1) * 4, st));
     uint32_t *d_pay = ctx->payload.as<uint32_t>();
     CodeEntry *d_codes = ctx->codes.as<CodeEntry>();
+    u64 enc_err[2] = {0, 0};  // the encoder's error words, read back with the pieces
     {
         std::vector<EncStream> es[2];
         std::vector<u64> toff[2] = {{0}, {0}};
@@ -4325,6 +4329,7 @@ int slab_encode(asz_ctx *ctx, SlabComm &cm, const CoreOut &co, const Plan &plan,
             u64 *tbits = (u64 *)(eb + off[k][2]), *tscan = (u64 *)(eb + off[k][3]);
             if (k == 0) CK(launch_encode_tiles<int32_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
             else CK(launch_encode_tiles<int64_t>(E, (uint32_t)es[k].size(), T, nt, tbits, tscan, ctx->cubtmp.p, tb, st));
+            CK(cudaMemcpyAsync(&enc_err[k], tscan, sizeof(u64), cudaMemcpyDeviceToHost, st));
         }
     }
     // This rank's pieces, back on the host: per stream its bits, then the bytes.
@@ -4339,6 +4344,8 @@ int slab_encode(asz_ctx *ctx, SlabComm &cm, const CoreOut &co, const Plan &plan,
             w += nb;
         }
         CK(cudaStreamSynchronize(st));
+        if (enc_err[0] | enc_err[1])
+            return fail(ctx, ASZ_E_DEVICE, "Huffman encoder: a tile's wait for the tiles before it timed out");
     }
     auto t_d2h = clk::now();
     if (rank != 0) {

@@ -458,8 +458,11 @@ extern "C" int asz_sweep(asz_ctx *ctx, const float *data, int on_device, const u
                 tb = W.cub.cap;
                 CK(launch_encode_tiles<int64_t>((const EncStream *)(eb + o_es), (uint32_t)es.size(), (const u64 *)(eb + o_toff),
                                                 nt, (u64 *)(eb + o_bits), (u64 *)(eb + o_scan), W.cub.p, tb, st));
+                u64 enc_err = 0;
+                CK(cudaMemcpyAsync(&enc_err, eb + o_scan, sizeof(u64), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(W.payload.p, W.pay.p, word_off[kc] * 4, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                if (enc_err) return host::ctx_fail(ctx, ASZ_E_DEVICE, "Huffman encoder: a tile's wait for the tiles before it timed out");
             }
             // Frame each stream (save + encode, huffman.hpp) and compress it with zstd level 3.
             std::vector<u64> hb(kc), zb(kc);

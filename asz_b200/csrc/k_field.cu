@@ -32,20 +32,30 @@ __global__ void range_kernel(const float4 *__restrict__ x4, uint64_t n4, const f
     int32_t mn = INT32_MAX, mx = INT32_MIN;
     unsigned long long bad = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += stride) {
-        float4 v = x4[i];
-        float a[4] = {v.x, v.y, v.z, v.w};
+    auto take = [&](float4 v) {
+        const float a[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             if (!isfinite(a[k])) {
                 bad++;
                 continue;
             }
-            int32_t o = ord_key(a[k]);
+            const int32_t o = ord_key(a[k]);
             mn = min(mn, o);
             mx = max(mx, o);
         }
+    };
+    // Four 16-byte loads per thread in flight per step, then the remainder one at a time.
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n4; i += 4 * stride) {
+        const float4 v0 = __ldg(x4 + i), v1 = __ldg(x4 + i + stride), v2 = __ldg(x4 + i + 2 * stride),
+                     v3 = __ldg(x4 + i + 3 * stride);
+        take(v0);
+        take(v1);
+        take(v2);
+        take(v3);
     }
+    for (; i < n4; i += stride) take(__ldg(x4 + i));
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ntail; i += stride) {
         float v = tail[i];
         if (!isfinite(v)) bad++;

@@ -84,12 +84,15 @@ __global__ void encode_kernel(const T *__restrict__ s, uint64_t n, int64_t offse
 }
 
 // ---------------------------------------------------------------------------------------------
-// Tiled encoding of several streams in one set of launches: per tile of kEncTile symbols its bit
-// count (tile_bits_kernel), an exclusive scan over all tiles, and a packing pass
-// (encode_tile_kernel) that builds each tile's bits in shared memory and writes them as whole
-// words, with atomicOr only on its first and last word, which it may share with the neighbouring
-// tiles. A stream's tiles are consecutive; a tile's bit offset in its stream is the scan at the tile
-// minus the scan at the stream's first tile.
+// Tiled encoding of several streams in one launch: tiles of enc_tile<T>() symbols, a stream's
+// tiles consecutive. A CTA takes tiles in order from a ticket counter and copies the next tile's
+// symbols into shared memory (asynchronous copies) while it encodes the current one. Per tile it
+// counts the tile's bits, publishes the count, and finds the tile's bit offset in its stream by
+// looking back over the tiles before it (decoupled look-back: each tile's state word holds its
+// count, then its inclusive prefix); it then builds the tile's bits in shared memory and writes
+// them as whole words, with atomicOr only on its first and last word, which it may share with the
+// neighbouring tiles. Tiles are handed out in order, so every tile a CTA waits for is held by a
+// CTA that is running; every wait is bounded and a wait that runs out sets the error word.
 
 __device__ __forceinline__ uint32_t stream_of(const uint64_t *toff, uint32_t ns, uint64_t t) {
     uint32_t lo = 0, hi = ns;  // toff[lo] <= t < toff[hi]
@@ -101,60 +104,75 @@ __device__ __forceinline__ uint32_t stream_of(const uint64_t *toff, uint32_t ns,
     return lo;
 }
 
+// Tile state words: status in the top two bits, bits (count or inclusive prefix) below.
+constexpr unsigned long long kTileCount = 1ull << 62, kTilePrefix = 2ull << 62, kTileValue = (1ull << 62) - 1;
+constexpr uint32_t kLookbackPolls = 1u << 22;
+
 template <class T>
-__global__ void __launch_bounds__(kEncThreads)
-    tile_bits_kernel(const EncStream *__restrict__ S, uint32_t ns, const uint64_t *__restrict__ toff, uint64_t ntiles,
-                     uint64_t *__restrict__ tile_bits) {
-    __shared__ uint32_t red[kEncThreads / 32];
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const EncStream &E = S[stream_of(toff, ns, t)];
-        const T *sym = reinterpret_cast<const T *>(E.s);
-        const uint64_t i0 = (t - toff[stream_of(toff, ns, t)]) * enc_tile<T>();
-        const uint64_t i1 = min(i0 + enc_tile<T>(), E.n);
-        uint32_t bits = 0;
-        for (uint64_t i = i0 + threadIdx.x; i < i1; i += kEncThreads)
-            bits += E.tab[(uint64_t)((int64_t)sym[i] - E.offset)].len;
-        for (int o = 16; o; o >>= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bits;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint64_t sum = 0;
-            for (int w = 0; w < kEncThreads / 32; w++) sum += red[w];
-            tile_bits[t] = sum;
-        }
-        __syncthreads();
-    }
+__device__ __forceinline__ void cp_async_sym(T *dst, const T *src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_older() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <class T>
 __global__ void __launch_bounds__(kEncThreads, 4)
-    encode_tile_kernel(const EncStream *__restrict__ S, uint32_t ns, const uint64_t *__restrict__ toff, uint64_t ntiles,
-                       const uint64_t *__restrict__ tile_scan) {
+    encode_tiles_kernel(const EncStream *__restrict__ S, uint32_t ns, const uint64_t *__restrict__ toff, uint64_t ntiles,
+                        unsigned long long *state, unsigned long long *err) {
     constexpr uint32_t kTile = enc_tile<T>(), kPer = kTile / kEncThreads;
-    // Symbol i sits at i + i / kPer: each thread reads its own kPer consecutive symbols, and the
-    // one-slot gap between runs spreads a warp's reads over all banks.
-    __shared__ T sym_sh[kTile + kEncThreads];
-    __shared__ uint32_t buf[kTile + 2];  // codes are at most 32 bits, plus the leading shift
+    // Symbol i of a tile sits at i + i / kPer: each thread reads its own kPer consecutive symbols,
+    // and the one-slot gap between runs spreads a warp's reads over all banks.
+    // Dynamic shared memory: two stages of symbols, then the tile's words (codes are at most 32
+    // bits, plus the leading shift).
+    extern __shared__ __align__(16) unsigned char enc_smem[];
+    T(*sym_sh)[kTile + kEncThreads] = reinterpret_cast<T(*)[kTile + kEncThreads]>(enc_smem);
+    uint32_t *buf = reinterpret_cast<uint32_t *>(enc_smem + 2 * (kTile + kEncThreads) * sizeof(T));
     __shared__ uint32_t wsum[kEncThreads / 32];
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    __shared__ unsigned long long s_next, s_excl;
+    unsigned long long *const ticket = state + ntiles;
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    // Copies of tile t's symbols into stage b (this thread's share), committed as one group.
+    auto issue = [&](uint64_t t, uint32_t b) {
+        if (t < ntiles) {
+            const uint32_t si = stream_of(toff, ns, t);
+            const EncStream &E = S[si];
+            const T *sym = reinterpret_cast<const T *>(E.s);
+            const uint64_t i0 = (t - toff[si]) * kTile;
+            const uint32_t cnt = (uint32_t)min((uint64_t)kTile, E.n - i0);
+            for (uint32_t i = tid; i < cnt; i += kEncThreads) cp_async_sym(&sym_sh[b][i + i / kPer], sym + i0 + i);
+        }
+        cp_async_commit_group();
+    };
+    if (tid == 0) s_next = atomicAdd(ticket, 1ull);
+    __syncthreads();
+    uint64_t t = s_next;
+    issue(t, 0);
+    uint32_t b = 0;
+    while (t < ntiles) {
+        // Every thread has read s_next and is done with stage b ^ 1 (the tile before this one).
+        __syncthreads();
+        if (tid == 0) s_next = atomicAdd(ticket, 1ull);
+        for (uint32_t i = tid; i < kTile + 2; i += kEncThreads) buf[i] = 0u;
+        __syncthreads();
+        const uint64_t tn = s_next;
+        issue(tn, b ^ 1);
+        cp_async_wait_older();
+        __syncthreads();  // this tile's symbols, copied by every thread, are in place
         const uint32_t si = stream_of(toff, ns, t);
         const EncStream &E = S[si];
-        const T *sym = reinterpret_cast<const T *>(E.s);
-        const uint64_t i0 = (t - toff[si]) * kTile;
+        const uint64_t t0 = toff[si];
+        const uint64_t i0 = (t - t0) * kTile;
         const uint32_t cnt = (uint32_t)min((uint64_t)kTile, E.n - i0);
-        const uint64_t bit0 = tile_scan[t] - tile_scan[toff[si]];
-        const uint32_t shift = (uint32_t)(bit0 & 31);
-        for (uint32_t i = threadIdx.x; i < cnt; i += kEncThreads) sym_sh[i + i / kPer] = sym[i0 + i];
-        for (uint32_t i = threadIdx.x; i < kTile + 2; i += kEncThreads) buf[i] = 0u;
-        __syncthreads();
         // This thread's symbols: kPer consecutive ones, so its bits are one consecutive run.
-        const uint32_t j0 = threadIdx.x * kPer;
+        const uint32_t j0 = tid * kPer;
         uint32_t code[kPer], len[kPer];
         uint32_t mine = 0;
 #pragma unroll
         for (uint32_t k = 0; k < kPer; k++) {
             CodeEntry e{0u, 0u};
-            if (j0 + k < cnt) e = E.tab[(uint64_t)((int64_t)sym_sh[j0 + k + threadIdx.x] - E.offset)];
+            if (j0 + k < cnt) e = E.tab[(uint64_t)((int64_t)sym_sh[b][j0 + k + tid] - E.offset)];
             code[k] = e.code;
             len[k] = e.len;
             mine += e.len;
@@ -163,15 +181,20 @@ __global__ void __launch_bounds__(kEncThreads, 4)
         uint32_t incl = mine;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if ((threadIdx.x & 31) >= (uint32_t)o) incl += v;
+            if (lane >= (uint32_t)o) incl += v;
         }
-        if ((threadIdx.x & 31) == 31) wsum[threadIdx.x >> 5] = incl;
+        if (lane == 31) wsum[tid >> 5] = incl;
         __syncthreads();
-        uint32_t before = 0;
-        for (uint32_t w = 0; w < (threadIdx.x >> 5); w++) before += wsum[w];
-        // Pack the run in a register: the run's first and last words may be shared with the
-        // neighbouring runs and are or-ed in; the words between belong to this thread alone.
-        const uint32_t pos = shift + before + incl - mine;
+        uint32_t before = 0, total = 0;
+        for (uint32_t w = 0; w < kEncThreads / 32; w++) {
+            if (w < (tid >> 5)) before += wsum[w];
+            total += wsum[w];
+        }
+        // Pack the run at bit 0 of the tile's words (the tile's offset in its stream is applied when
+        // the words are written, so the packing need not wait for it): the run's first and last
+        // words may be shared with the neighbouring runs and are or-ed in; the words between belong
+        // to this thread alone.
+        const uint32_t pos = before + incl - mine;
         if (mine) {
             uint32_t w = pos >> 5, nacc = pos & 31;
             uint64_t acc = 0;
@@ -191,20 +214,58 @@ __global__ void __launch_bounds__(kEncThreads, 4)
             }
             if (nacc) atomicOr(&buf[w], (uint32_t)acc);
         }
-        __syncthreads();
-        uint32_t total = 0;
-        for (uint32_t w = 0; w < kEncThreads / 32; w++) total += wsum[w];
-        const uint32_t nw = (shift + total + 31) >> 5;
-        uint32_t *out = E.out + (bit0 >> 5);
-        for (uint32_t i = threadIdx.x; i < nw; i += kEncThreads) {
-            if (i == 0 || i == nw - 1) {
-                if (buf[i]) atomicOr(&out[i], buf[i]);
+        // The tile's bit offset in its stream: publish the count, then add up the counts back to
+        // the nearest published prefix (or the stream's first tile).
+        if (tid < 32) {
+            unsigned long long excl = 0;
+            if (t == t0) {
+                if (lane == 0) atomicExch(&state[t], kTilePrefix | total);
             } else {
-                out[i] = buf[i];
+                if (lane == 0) atomicExch(&state[t], kTileCount | total);
+                for (int64_t j = (int64_t)t - 1;; j -= 32) {
+                    const int64_t pidx = j - (int64_t)lane;
+                    unsigned long long v = kTilePrefix;  // before the stream's first tile: prefix 0
+                    if (pidx >= (int64_t)t0) {
+                        const volatile unsigned long long *w = state + pidx;
+                        v = *w;
+                        for (uint32_t polls = 0; !(v >> 62) && polls < kLookbackPolls; polls++) {
+                            __nanosleep(64);
+                            v = *w;
+                        }
+                        if (!(v >> 62)) {
+                            atomicOr(err, 1ull);
+                            v = kTilePrefix;
+                        }
+                    }
+                    const uint32_t pref = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+                    const uint32_t upto = pref ? (uint32_t)(__ffs(pref) - 1) : 31u;
+                    unsigned long long x = lane <= upto ? (v & kTileValue) : 0ull;
+                    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                    excl += x;
+                    if (pref) break;
+                }
+                if (lane == 0) atomicExch(&state[t], kTilePrefix | (excl + total));
             }
+            if (lane == 0) s_excl = excl;
         }
         __syncthreads();
+        // Words out, shifted to the tile's offset: word i takes the high bits of packed word i - 1.
+        const uint64_t bit0 = s_excl;
+        const uint32_t shift = (uint32_t)(bit0 & 31);
+        const uint32_t nw = (shift + total + 31) >> 5;
+        uint32_t *out = E.out + (bit0 >> 5);
+        for (uint32_t i = tid; i < nw; i += kEncThreads) {
+            const uint32_t v = shift ? (buf[i] << shift) | (i ? buf[i - 1] >> (32 - shift) : 0u) : buf[i];
+            if (i == 0 || i == nw - 1) {
+                if (v) atomicOr(&out[i], v);
+            } else {
+                out[i] = v;
+            }
+        }
+        t = tn;
+        b ^= 1;
     }
+    cp_async_wait_older();  // the last committed group (past the end) holds no copies
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -503,16 +564,23 @@ cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntr
 }
 
 template <class T>
-cudaError_t launch_encode_tiles(const EncStream *streams, uint32_t ns, const uint64_t *toff, uint64_t ntiles, uint64_t *tile_bits,
-                                uint64_t *tile_scan, void *tmp, size_t &tmp_bytes, cudaStream_t st) {
-    if (tmp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, tile_bits, tile_scan, (int64_t)ntiles + 1, st);
+cudaError_t launch_encode_tiles(const EncStream *streams, uint32_t ns, const uint64_t *toff, uint64_t ntiles, uint64_t *tile_state,
+                                uint64_t *err, void *tmp, size_t &tmp_bytes, cudaStream_t st) {
+    if (tmp == nullptr) {
+        tmp_bytes = 0;
+        return cudaSuccess;
+    }
     if (ntiles == 0) return cudaSuccess;
-    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, 148 * 8);
-    tile_bits_kernel<T><<<grid, kEncThreads, 0, st>>>(streams, ns, toff, ntiles, tile_bits);
-    count_launch();
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, tile_bits, tile_scan, (int64_t)ntiles + 1, st);
+    cudaError_t e = cudaMemsetAsync(tile_state, 0, (ntiles + 1) * sizeof(uint64_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(uint64_t), st);
     if (e != cudaSuccess) return e;
-    encode_tile_kernel<T><<<grid, kEncThreads, 0, st>>>(streams, ns, toff, ntiles, tile_scan);
+    constexpr uint32_t kTile = enc_tile<T>();
+    const int smem = (int)(2 * (kTile + kEncThreads) * sizeof(T) + (kTile + 2) * sizeof(uint32_t));
+    e = cudaFuncSetAttribute(encode_tiles_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, 148 * 4);
+    encode_tiles_kernel<T><<<grid, kEncThreads, smem, st>>>(streams, ns, toff, ntiles, (unsigned long long *)tile_state,
+                                                            (unsigned long long *)err);
     count_launch();
     return cudaGetLastError();
 }

@@ -175,10 +175,12 @@ cudaError_t launch_histogram(const T *s, uint64_t n, int64_t offset, uint64_t ra
 template <class T>
 cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntry *tab, uint64_t *bitoff, void *tmp,
                           size_t &tmp_bytes, uint32_t *out, cudaStream_t st);
-// Tiled encoding of several streams of one symbol type at once (k_huff.cu). toff: exclusive
-// prefix of the streams' tile counts (ns + 1 entries, tiles of enc_tile<T>() symbols); tile_bits
-// needs ntiles + 1 entries (the last one zero: the scan's total), tile_scan the same; each stream's
-// out is zeroed beforehand. With tmp == nullptr, only sets tmp_bytes.
+// Tiled encoding of several streams of one symbol type in one launch (k_huff.cu). toff: exclusive
+// prefix of the streams' tile counts (ns + 1 entries, tiles of enc_tile<T>() symbols);
+// tile_state needs ntiles + 1 entries and err one, both cleared here; each stream's out is zeroed
+// beforehand. After the launch *err is nonzero if a tile's wait for the bit counts before it ran
+// out (the payload is then not valid). With tmp == nullptr, only sets tmp_bytes (no temporary
+// space is used).
 constexpr uint32_t kEncThreads = 256;
 template <class T>
 ASZ_HD constexpr uint32_t enc_tile() { return sizeof(T) == 4 ? 4096u : 2048u; }
@@ -190,8 +192,8 @@ struct EncStream {
     uint32_t *out;          // payload words
 };
 template <class T>
-cudaError_t launch_encode_tiles(const EncStream *streams, uint32_t ns, const uint64_t *toff, uint64_t ntiles, uint64_t *tile_bits,
-                                uint64_t *tile_scan, void *tmp, size_t &tmp_bytes, cudaStream_t st);
+cudaError_t launch_encode_tiles(const EncStream *streams, uint32_t ns, const uint64_t *toff, uint64_t ntiles, uint64_t *tile_state,
+                                uint64_t *err, void *tmp, size_t &tmp_bytes, cudaStream_t st);
 cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st);
 cudaError_t launch_decode_sync(const uint8_t *base, uint64_t chunk_bits, const DecStream *streams, const uint32_t *tile_stream,
                                uint64_t ntiles, uint32_t max_lut_bits, const LutEntry *luts, const uint32_t *childs,
