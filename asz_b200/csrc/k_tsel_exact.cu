@@ -569,20 +569,25 @@ __global__ void __launch_bounds__(kThreads)
                        uint32_t *__restrict__ err_word, uint32_t smem_bytes, uint32_t cap) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ float h1v[kMaxEvals], xv[kMaxEvals];
-    const uint32_t g = blockIdx.x;
+    // Box blockIdx.x, evaluations [5 * blockIdx.y, 5 * blockIdx.y + 5): exact_eval runs five
+    // evaluations side by side, so each CTA rebuilds the box's map and runs one batch of them.
+    const uint32_t g = blockIdx.x, e0 = 5 * blockIdx.y;
+    if (e0 >= n_evals) return;
+    const uint32_t ne = min(5u, n_evals - e0);
     ExactGroup eg;
     eg.box = boxes[g];
     eg.n = eg.box.n;
-    bool ok = exact_eval(eg, orig, orig, n1n2, n2, evals, (int)n_evals, R2, log2arena + eg.box.log2_off, smem, cap, h1v, xv,
-                         m_out + g);
+    uint32_t m = 0;
+    bool ok = exact_eval(eg, orig, orig, n1n2, n2, evals + e0, (int)ne, R2, log2arena + eg.box.log2_off, smem, cap, h1v, xv, &m);
     __syncthreads();
     if (!ok) {
         if (threadIdx.x == 0) atomicOr(err_word, 2u);
         return;
     }
-    for (uint32_t e = threadIdx.x; e < n_evals; e += blockDim.x) {
-        h1_out[g * n_evals + e] = h1v[e];
-        x_out[g * n_evals + e] = xv[e];
+    if (threadIdx.x == 0 && blockIdx.y == 0) m_out[g] = m;
+    for (uint32_t e = threadIdx.x; e < ne; e += blockDim.x) {
+        h1_out[g * n_evals + e0 + e] = h1v[e];
+        x_out[g * n_evals + e0 + e] = xv[e];
     }
 }
 
@@ -696,7 +701,8 @@ cudaError_t launch_slope_exact(const SampleBox *boxes, const ProxyEval *evals, u
     uint32_t smem = exact_smem_bytes(cap);
     cudaError_t e = cudaFuncSetAttribute(slope_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    slope_exact_kernel<<<nboxes, kThreads, smem, st>>>(boxes, evals, n_evals, orig, n1n2, n2, log2arena, R2, h1, x, m_out, err,
+    const dim3 grid(nboxes, (n_evals + 4) / 5);
+    slope_exact_kernel<<<grid, kThreads, smem, st>>>(boxes, evals, n_evals, orig, n1n2, n2, log2arena, R2, h1, x, m_out, err,
                                                   smem, cap);
     count_launch();
     return cudaGetLastError();
