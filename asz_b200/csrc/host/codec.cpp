@@ -241,7 +241,7 @@ struct asz_ctx {
     // Batches (asz_compress_batch): per-field slices of these arenas, the captured round sequence
     // of the last batch, and the launch shapes the autotuner chose per batch shape.
     DevBuf b_in, b_rec, b_qb, b_tval, b_tint, b_ent, b_cls, b_rounds, b_qoff, b_range, b_range0, b_prox, b_amb, b_cnt,
-        b_fields, b_goff, b_poff, b_ioff, b_queue, b_hand, b_spill;
+        b_fields, b_goff, b_poff, b_ioff, b_queue, b_hand, b_spill, b_spill2;
     std::vector<uint64_t> batch_graph_key;
     cudaGraphExec_t batch_graph = nullptr;
     std::map<std::vector<uint64_t>, std::array<uint32_t, 3>> batch_tuned;
@@ -844,7 +844,7 @@ void asz_destroy(asz_ctx *c) {
                       &c->plan_pay, &c->probe_in, &c->probe_pred, &c->rounds_dev, &c->lines_bail,
                       &c->lines_resume, &c->enc, &c->b_in, &c->b_rec, &c->b_qb, &c->b_tval, &c->b_tint, &c->b_ent, &c->b_cls,
                       &c->b_rounds, &c->b_qoff, &c->b_range, &c->b_range0, &c->b_prox, &c->b_amb, &c->b_cnt, &c->b_fields,
-                      &c->b_goff, &c->b_poff, &c->b_ioff, &c->b_queue, &c->b_hand, &c->b_spill})
+                      &c->b_goff, &c->b_poff, &c->b_ioff, &c->b_queue, &c->b_hand, &c->b_spill, &c->b_spill2})
         b->release();
     c->pre_zstd.release();
     c->batch_pre[0].release();
@@ -3574,9 +3574,18 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
     CK(ctx->b_goff.reserve((u64)(nf + 1) * sizeof(u64)));
     CK(ctx->b_poff.reserve((u64)(nf + 1) * sizeof(u64)));
     CK(ctx->b_ioff.reserve((u64)L * (nf + 1) * sizeof(u64)));
-    CK(ctx->b_queue.reserve((u64)L * 4 * sizeof(uint32_t)));
+    CK(ctx->b_queue.reserve((u64)L * 5 * sizeof(uint32_t)));
     CK(ctx->b_hand.reserve(std::max<u64>(nb_total, 1) * sizeof(unsigned long long)));
     CK(ctx->b_spill.reserve(std::max<u64>(nb_total, 1) * sizeof(unsigned long long)));
+    // Groups above the exact kernel's shared-memory capacity: the same replay with global scratch,
+    // a CTA per group (at most 148 CTAs and 512 MiB), then the serial kernel for what is left.
+    const u64 gstride = exact_global_stride(capmax);
+    unsigned ggrid = 0;
+    if (capmax > exact_cap()) {
+        ggrid = (unsigned)std::max<u64>(1, std::min<u64>(148, (512ull << 20) / gstride));
+        CK(ctx->gscratch.reserve(ggrid * gstride));
+        CK(ctx->b_spill2.reserve(std::max<u64>(nb_total, 1) * sizeof(unsigned long long)));
+    }
     uint32_t bcap, tcap;
     u64 sstride;
     scratch_dims(capmax, bcap, tcap, sstride);
@@ -3665,10 +3674,11 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
         CK(cudaMemcpyAsync(ctx->b_range.p, ctx->b_range0.p, (u64)nf * 2 * (L + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
                            st));
         CK(cudaMemsetAsync(ctx->b_cnt.p, 0, (u64)nf * sizeof(BatchCounters), st));
-        CK(cudaMemsetAsync(ctx->b_queue.p, 0, (u64)L * 4 * sizeof(uint32_t), st));
+        CK(cudaMemsetAsync(ctx->b_queue.p, 0, (u64)L * 5 * sizeof(uint32_t), st));
         CK(launch_pivot_compress_batch(dF, ctx->b_poff.as<u64>(), nf, pivots_total, st));
         for (u64 l = 0; l < L; l++) {
-            uint32_t *q = d_queue + 4 * l;
+            // Per round: fast queue, round queue, hand-off count, spill count, second spill count.
+            uint32_t *q = d_queue + 5 * l;
             if (t_tables) {
                 // The caller's t codes replace the coefficient selection.
                 CK(launch_tval_from_codes_batch(dF, d_goff, nf, nb_total, (uint32_t)l, st));
@@ -3679,8 +3689,16 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
                                       148 * sh[0], st));
             CK(launch_tsel_exact_batch(dF, (uint32_t)l, ctx->log2arena.as<float>(), t_default, d_hand, q + 2, d_spill, q + 3,
                                        exact_cap(), 148, st));
+            unsigned long long *d_left = d_spill;
+            uint32_t *d_lcnt = q + 3;
+            if (ggrid) {
+                d_left = ctx->b_spill2.as<unsigned long long>();
+                d_lcnt = q + 4;
+                CK(launch_tsel_exact_global_batch(dF, (uint32_t)l, ctx->log2arena.as<float>(), t_default, d_spill, q + 3, d_left,
+                                                  d_lcnt, ctx->gscratch.as<uint8_t>(), gstride, capmax, ggrid, st));
+            }
             CK(launch_tsel_v0_batch(dF, (uint32_t)l, ctx->log2arena.as<float>(), t_default, ctx->scratch.as<uint8_t>(), sstride,
-                                    capmax, bcap, tcap, d_spill, q + 3, slots, st));
+                                    capmax, bcap, tcap, d_left, d_lcnt, slots, st));
             CK(launch_round_compress_batch(dF, d_ioff + l * (nf + 1), nf, (uint32_t)l, q + 1, 148 * sh[1], st));
         }
         return ASZ_OK;
@@ -3738,7 +3756,7 @@ static int compress_batch_impl(asz_ctx *ctx, uint32_t count, const float *const 
     for (DevBuf *d : {&ctx->b_rec, &ctx->b_qb, &ctx->b_tval, &ctx->b_tint, &ctx->b_ent, &ctx->b_cls, &ctx->b_rounds,
                       &ctx->b_qoff, &ctx->b_range, &ctx->b_range0, &ctx->b_prox, &ctx->b_amb, &ctx->b_cnt, &ctx->b_fields,
                       &ctx->b_goff, &ctx->b_poff, &ctx->b_ioff, &ctx->b_queue, &ctx->b_hand, &ctx->b_spill, &ctx->scratch,
-                      &ctx->log2arena})
+                      &ctx->log2arena, &ctx->b_spill2, &ctx->gscratch})
         graph_key.push_back((uint64_t)(uintptr_t)d->p);
     graph_key.push_back((uint64_t)(uintptr_t)st);
     auto t_rounds = clk::now();

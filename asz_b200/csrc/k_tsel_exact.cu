@@ -562,6 +562,30 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// Batched form of tsel_exact_global_kernel: the entries the batched exact kernel spilled (groups
+// above its shared-memory capacity), a CTA per group in its slice of global scratch; what this
+// cannot take (keys outside int32) goes on to `spill` for the serial kernel.
+__global__ void __launch_bounds__(kThreads)
+    tsel_exact_global_batch_kernel(const BatchField *__restrict__ F, uint32_t l, const float *__restrict__ log2arena,
+                                   float t_default, const unsigned long long *__restrict__ list,
+                                   const uint32_t *__restrict__ list_count, unsigned long long *spill, uint32_t *spill_count,
+                                   uint8_t *scratch, uint64_t stride, uint32_t cap) {
+    uint8_t *mine = scratch + blockIdx.x * stride;
+    const uint32_t items = *list_count;
+    __shared__ float h1v[kMaxEvals], xv[kMaxEvals];
+    __shared__ uint32_t m_sh;
+    for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const unsigned long long e = list[it];
+        const uint32_t f = (uint32_t)(e >> 32);
+        const BatchField &B = F[f];
+        const uint64_t nb = B.fg.block_num[0] * B.fg.block_num[1] * B.fg.block_num[2];
+        const PairSpill sp{spill, spill_count, f};
+        exact_one(B.fg, B.rounds[l], l, B.classes + 27 * l, B.rec, B.in, log2arena, B.R2, t_default, B.tval, B.tint, &B.cnt->fb,
+                  B.amb, B.amb_cap, &B.cnt->amb_count, nullptr, 0, B.proxies ? B.proxies + nb * l * 10 : nullptr,
+                  e & 0xffffffffull, mine, cap, h1v, xv, m_sh, sp);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
     slope_exact_kernel(const SampleBox *__restrict__ boxes, const ProxyEval *__restrict__ evals, uint32_t n_evals,
                        const float *__restrict__ orig, uint64_t n1n2, uint64_t n2, const float *__restrict__ log2arena,
@@ -679,6 +703,17 @@ cudaError_t launch_tsel_exact(const FieldGeom &fg, const RoundGeom &rg, uint32_t
     tsel_exact_kernel<<<grid, kThreads, smem, st>>>(fg, rg, l, classes, rec, orig, log2arena, R2, t_default, tval, t_int,
                                                      fb_count, amb, amb_cap, amb_count, overrides, n_overrides, proxies, list,
                                                      list_count, spill, spill_count, smem, cap);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tsel_exact_global_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default,
+                                           const unsigned long long *list, const uint32_t *list_count,
+                                           unsigned long long *spill, uint32_t *spill_count, uint8_t *scratch, uint64_t stride,
+                                           uint32_t cap, unsigned grid, cudaStream_t st) {
+    if (grid == 0) return cudaSuccess;
+    tsel_exact_global_batch_kernel<<<grid, kThreads, 0, st>>>(F, l, log2arena, t_default, list, list_count, spill, spill_count,
+                                                              scratch, stride, cap);
     count_launch();
     return cudaGetLastError();
 }

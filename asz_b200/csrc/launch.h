@@ -65,6 +65,12 @@ cudaError_t launch_tsel_fast_batch(const BatchField *F, const uint64_t *goff, ui
 cudaError_t launch_tsel_exact_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default,
                                     const unsigned long long *list, const uint32_t *list_count, unsigned long long *spill,
                                     uint32_t *spill_count, uint32_t cap, unsigned grid, cudaStream_t st);
+// Groups the batched exact kernel spilled (above its shared-memory capacity), a CTA each in a
+// `stride`-byte slice of global scratch; what it cannot take goes to `spill`.
+cudaError_t launch_tsel_exact_global_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default,
+                                           const unsigned long long *list, const uint32_t *list_count,
+                                           unsigned long long *spill, uint32_t *spill_count, uint8_t *scratch, uint64_t stride,
+                                           uint32_t cap, unsigned grid, cudaStream_t st);
 cudaError_t launch_tsel_v0_batch(const BatchField *F, uint32_t l, const float *log2arena, float t_default, uint8_t *scratch,
                                  uint64_t scratch_stride, uint32_t cap, uint32_t bcap, uint32_t tcap,
                                  const unsigned long long *list, const uint32_t *list_count, uint64_t slots, cudaStream_t st);
