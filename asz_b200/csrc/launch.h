@@ -95,7 +95,7 @@ cudaError_t launch_pivot_decompress(const PivotGeom &pg, const int32_t *qb, floa
 // Requires tcount[0] * tcount[1] < 2^32 and tcount[2] < 2^32 (checked by the host).
 // hist (optional, kHistWin zeroed 64-bit bins): the QB histogram of the round's stream over
 // [-kHistHalf, kHistHalf), added to hist; a QB outside the window sets *hist_over.
-constexpr uint32_t kHistWin = 4096, kHistHalf = kHistWin / 2;
+constexpr uint32_t kHistWin = 8192, kHistHalf = kHistWin / 2;
 cudaError_t launch_round_compress(const FieldGeom &fg, const RoundGeom &rg, const AxisEntry *ent, const float *tval,
                                   const float *in, float *rec, int32_t *qb, int32_t *qb_range, uint32_t *err, int div_all,
                                   float *pred_out, cudaStream_t st, unsigned long long *hist = nullptr,
