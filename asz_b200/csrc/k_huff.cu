@@ -11,7 +11,6 @@
 
 #include <algorithm>
 
-#include <cub/device/device_scan.cuh>
 
 #include "dev_common.cuh"
 #include "launch.h"
@@ -548,15 +547,96 @@ cudaError_t launch_histogram(const T *s, uint64_t n, int64_t offset, uint64_t ra
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------------
+// Exclusive prefix sums of n 64-bit values (in == out allowed): tiles of kScanTile values, a CTA
+// each, scanned in registers and shared memory; the tiles' totals are scanned the same way (in
+// tmp, a level per kScanTile-fold reduction), then added back to their tiles.
+constexpr uint32_t kScanThreads = 1024, kScanPer = 4, kScanTile = kScanThreads * kScanPer;
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_tiles_kernel(const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *tile_sums) {
+    __shared__ uint64_t wsum[kScanThreads / 32];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t first = (uint64_t)blockIdx.x * kScanTile + (uint64_t)tid * kScanPer;
+    uint64_t v[kScanPer], mine = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kScanPer; k++) {
+        v[k] = first + k < n ? in[first + k] : 0;
+        mine += v[k];
+    }
+    uint64_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint64_t w = wsum[lane];
+        uint64_t wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= (uint32_t)o) wi += t;
+        }
+        wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    uint64_t run = wsum[warp] + incl - mine;
+#pragma unroll
+    for (uint32_t k = 0; k < kScanPer; k++) {
+        if (first + k < n) out[first + k] = run;
+        run += v[k];
+    }
+    if (tile_sums && tid == kScanThreads - 1) tile_sums[blockIdx.x] = run;  // the tile's total
+}
+
+__global__ void scan_add_kernel(uint64_t *out, uint64_t n, const uint64_t *__restrict__ tile_offsets) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] += tile_offsets[i / kScanTile];
+}
+
+static uint64_t scan_tmp_words(uint64_t n) {
+    uint64_t w = 0;
+    while (n > kScanTile) {
+        n = (n + kScanTile - 1) / kScanTile;
+        w += n;
+    }
+    return w;
+}
+
+static cudaError_t scan_u64_levels(const uint64_t *in, uint64_t *out, uint64_t n, uint64_t *tmp, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    uint64_t *sums = tiles > 1 ? tmp : nullptr;
+    scan_tiles_kernel<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, sums);
+    count_launch();
+    if (tiles > 1) {
+        cudaError_t e = scan_u64_levels(sums, sums, tiles, tmp + tiles, st);
+        if (e != cudaSuccess) return e;
+        scan_add_kernel<<<(unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(out, n, sums);
+        count_launch();
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st) {
+    if (tmp == nullptr) {
+        tmp_bytes = std::max<size_t>(scan_tmp_words(n) * sizeof(uint64_t), 16);
+        return cudaSuccess;
+    }
+    if (tmp_bytes < scan_tmp_words(n) * sizeof(uint64_t)) return cudaErrorInvalidValue;
+    return scan_u64_levels(in, out, n, reinterpret_cast<uint64_t *>(tmp), st);
+}
+
 template <class T>
 cudaError_t launch_encode(const T *s, uint64_t n, int64_t offset, const CodeEntry *tab, uint64_t *bitoff, void *tmp,
                           size_t &tmp_bytes, uint32_t *out, cudaStream_t st) {
-    if (tmp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, bitoff, bitoff, (int64_t)n, st);
+    if (tmp == nullptr) return launch_scan_u64(bitoff, bitoff, n, nullptr, tmp_bytes, st);
     if (n == 0) return cudaSuccess;
     uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 16);
     code_len_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(s, n, offset, tab, bitoff);
     count_launch();
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, bitoff, bitoff, (int64_t)n, st);
+    cudaError_t e = launch_scan_u64(bitoff, bitoff, n, tmp, tmp_bytes, st);
     if (e != cudaSuccess) return e;
     encode_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(s, n, offset, tab, bitoff, out);
     count_launch();
@@ -589,11 +669,6 @@ template cudaError_t launch_encode_tiles<int32_t>(const EncStream *, uint32_t, c
                                                   void *, size_t &, cudaStream_t);
 template cudaError_t launch_encode_tiles<int64_t>(const EncStream *, uint32_t, const uint64_t *, uint64_t, uint64_t *, uint64_t *,
                                                   void *, size_t &, cudaStream_t);
-
-cudaError_t launch_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, void *tmp, size_t &tmp_bytes, cudaStream_t st) {
-    if (tmp == nullptr) return cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, in, out, (int64_t)n, st);
-    return cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, (int64_t)n, st);
-}
 
 // Persistent decode grid: up to 6 CTAs of 256 threads per SM (a table takes up to 32 KB).
 static unsigned decode_grid(uint64_t ntiles) { return (unsigned)(ntiles < 148 * 6 ? (ntiles ? ntiles : 1) : 148 * 6); }
