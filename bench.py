@@ -833,7 +833,7 @@ TRAFFIC_PER_LAUNCH = {
 }
 
 
-E2E_WORKERS = 8
+E2E_WORKERS = 12
 
 
 def e2e_pipelined(api, L, local, dims, p, plan_b, xh, yh, blob, steps, barrier):
