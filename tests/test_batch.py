@@ -47,6 +47,31 @@ def test_batch_equals_single_field(gpu_ctx, plan, family):
         assert blob == single
 
 
+def test_batch_groups_beyond_shared_memory(gpu_ctx):
+    """Groups of more samples than the exact kernel's shared memory holds (24^3 blocks sampled
+    2048 at a time, so the finest rounds' groups run to thousands of samples; noisy fields, so
+    many of them reach the exact path): the batched sequence replays those in global scratch, a
+    CTA per group, and every field's bytes equal its single-field compression and the oracle's."""
+    import asz_b200.api as api
+    from asz_b200 import fields
+    rng = np.random.default_rng(43)
+    fs = []
+    for _ in range(3):
+        shape = tuple(int(x) for x in rng.integers(60, 76, size=3))
+        fs.append(fields.grf_field(shape, 4.0, rng).astype(np.float32) + rng.random(shape).astype(np.float32) * 0.5)
+    plan = ",".join(["cubic0_012", "cubic1_012", "cubic2_012"] * 2)
+    p = api.default_params(block_pivot_ratio=6, h1_block_sampling_num=2048)
+    blobs, _, _ = gpu_ctx.compress_batch(fs, 1e-4, plan, "cubic", p)
+    handed_off = 0
+    for f, blob in zip(fs, blobs):
+        single, rep = gpu_ctx.compress(f, 1e-4, plan, "cubic", p)
+        assert blob == single
+        handed_off += rep.exact_groups
+    assert handed_off > 0
+    o = O.compress(fs[0], 1e-4, plan, False, O.default_params(block_pivot_ratio=6, h1_block_sampling_num=2048))
+    assert blobs[0] == o.asz
+
+
 def test_batch_device_inputs_and_errors(gpu_ctx):
     import torch
 
